@@ -1,0 +1,171 @@
+/*
+ * nabla_b200.h — C ABI of the B200 (sm_100a) per-step fluid update.
+ *
+ * The path: WENO-5 advection inside SSP-RK3 stages, each stage followed by a
+ * pressure projection solved with geometric-multigrid-preconditioned CG
+ * (MG-PCG), on a MAC grid stored as 8x8x8-cell bricks in Morton order.
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or torch types
+ * cross this boundary. Host arrays use the reference's lexicographic layouts
+ * (x fastest): u is (nx+1)*ny*nz, v nx*(ny+1)*nz, w nx*ny*(nz+1), cell arrays
+ * nx*ny*nz (core/include/nabla/flow/ns_solver.hpp:94-111).
+ *
+ * Errors: every call returns an nb_status. NB_OK is 0. A failed call leaves a
+ * message retrievable with nb_last_error(ctx). Solver non-convergence is not
+ * an error: it is reported in the report structs (as the reference reports
+ * PoissonSolver::Report::converged, core/include/nabla/flow/poisson.hpp:24-28).
+ */
+#ifndef NABLA_B200_H
+#define NABLA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum nb_status {
+  NB_OK = 0,
+  NB_ERR_BAD_ARG = 1,        /* invalid pointer, size or option */
+  NB_ERR_OOM = 2,            /* device allocation failed / over budget */
+  NB_ERR_NOT_CONVERGED = 3,  /* only returned where a caller asked for strict convergence */
+  NB_ERR_NAN = 4,            /* NaN/Inf detected in a solver input or state */
+  NB_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
+  NB_ERR_CUDA = 6,           /* CUDA runtime error */
+  NB_ERR_UNSUPPORTED = 7     /* configuration outside what this build implements */
+} nb_status;
+
+/* ---- boundary description: mirrors core/include/nabla/flow/grid.hpp:17-26 */
+enum { NB_BC_WALL = 0, NB_BC_INLET = 1, NB_BC_OUTLET = 2, NB_BC_PERIODIC = 3 };
+enum { NB_PROFILE_UNIFORM = 0, NB_PROFILE_PARABOLIC = 1 };
+enum { NB_CONV_CENTRAL = 0, NB_CONV_WENO5 = 1 };
+/* Arithmetic forms of the step. PLAIN is FP64 throughout (the drop-in form).
+ * MIXED runs WENO/RK stage arithmetic and the V-cycle in FP32 with FP64 PCG
+ * dot products, search directions, true residuals, coarsest solve and the
+ * final divergence check. */
+enum { NB_PRECISION_FP64 = 0, NB_PRECISION_MIXED = 1 };
+
+typedef struct nb_face_bc {
+  int32_t type;             /* NB_BC_* (BoundaryType) */
+  int32_t profile;          /* NB_PROFILE_* (InletProfile) */
+  int32_t inlet_axis;       /* velocity component the inlet drives */
+  int32_t reserved;
+  double wall_velocity[3];  /* FaceBC::wallVelocity */
+  double inlet_speed;       /* FaceBC::inletSpeed */
+} nb_face_bc;
+
+/* Uniform Cartesian grid: mirrors UniformGrid (grid.hpp:32-73). Face order
+ * 0=-x 1=+x 2=-y 3=+y 4=-z 5=+z. `solid` is nx*ny*nz bytes (1 = obstacle) in
+ * lexicographic order, or NULL for no obstacle. */
+typedef struct nb_grid_desc {
+  int32_t nx, ny, nz, reserved;
+  double origin[3];
+  double dx, dy, dz;
+  nb_face_bc face[6];
+  const uint8_t* solid;
+} nb_grid_desc;
+
+/* Mirrors FlowConfig (core/include/nabla/flow/ns_solver.hpp:14-32). */
+typedef struct nb_flow_config {
+  double reynolds, ref_length, velocity_scale, density, cfl;
+  double body_force[3];
+  int32_t convection;         /* NB_CONV_* */
+  int32_t poisson_max_iters;
+  double poisson_tol;
+  double tol_continuity, tol_mass;
+  double ref_area;
+} nb_flow_config;
+
+/* Mirrors StepReport (ns_solver.hpp:34-49). */
+typedef struct nb_step_report {
+  int32_t step;
+  int32_t poisson_iters;
+  double t, dt, cfl;
+  double momentum_residual, continuity_residual, divergence_max, mass_error;
+  double poisson_residual, cd, cl;
+  uint64_t cell_count;
+  int32_t accepted;
+  int32_t converged;          /* all three projections converged */
+} nb_step_report;
+
+/* Mirrors PoissonSolver::Report (poisson.hpp:24-28). */
+typedef struct nb_poisson_report {
+  int32_t iterations;
+  int32_t converged;
+  double residual;
+} nb_poisson_report;
+
+typedef struct nb_ctx nb_ctx;
+typedef struct nb_case nb_case;
+
+/* ---- context ------------------------------------------------------------ */
+/* Binds CUDA device `device`. Fails with NB_ERR_CUDA when no sm_100 device is
+ * present: there is no CPU fallback. */
+nb_status nb_ctx_create(int device, nb_ctx** out);
+void nb_ctx_destroy(nb_ctx* ctx);
+const char* nb_last_error(const nb_ctx* ctx);
+const char* nb_status_string(nb_status s);
+/* Kernel launches issued by this context since creation (evidence counter). */
+uint64_t nb_ctx_launch_count(const nb_ctx* ctx);
+nb_status nb_ctx_synchronize(nb_ctx* ctx);
+
+/* ---- cases: one NS problem resident on the device ----------------------- */
+/* Replaces NSSolver::NSSolver(UniformGrid, FlowConfig, shared_ptr<PoissonSolver>)
+ * (core/src/flow/ns_solver.cpp:46-69) with the MG-PCG default solver
+ * (ns_solver.cpp:49-53). The grid, BCs and solid mask are copied. */
+nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_config* cfg,
+                         int precision, nb_case** out);
+void nb_case_destroy(nb_case* c);
+/* Replaces NSSolver::initialize (ns_solver.cpp:95-112). */
+nb_status nb_case_initialize(nb_case* c);
+/* Replaces NSSolver::setState (ns_solver.cpp:826-839): host arrays in the
+ * reference's staggered lexicographic layout. */
+nb_status nb_case_set_state(nb_case* c, const double* u, const double* v, const double* w,
+                            const double* p, int step, double t, double dt_last);
+/* Replaces the uFace()/vFace()/wFace()/pressure() accessors (ns_solver.hpp:76-80).
+ * Any pointer may be NULL to skip that field. */
+nb_status nb_case_get_state(nb_case* c, double* u, double* v, double* w, double* p);
+nb_status nb_case_get_clock(nb_case* c, int* step, double* t, double* dt_last);
+/* Replaces NSSolver::computeDt (ns_solver.cpp:581-603). */
+nb_status nb_case_compute_dt(nb_case* c, double* dt);
+/* Replaces NSSolver::step(double dt) (ns_solver.cpp:767-824); dt <= 0 selects
+ * NSSolver::step() (ns_solver.cpp:765), i.e. dt from computeDt. `rep` may be NULL. */
+nb_status nb_step(nb_case* c, double dt, nb_step_report* rep);
+/* Runs `nsteps` fixed-dt steps without reading any report back (resident
+ * throughput path); the last step's report is written to `rep` if non-NULL. */
+nb_status nb_step_many(nb_case* c, double dt, int nsteps, nb_step_report* rep);
+/* Device bytes held by the case (admission control uses this). */
+uint64_t nb_case_device_bytes(const nb_case* c);
+/* Leaf cells of the case (Mcell-steps/s numerator). */
+uint64_t nb_case_cell_count(const nb_case* c);
+/* The cudaStream_t the case's kernels run on (for caller-side CUDA events). */
+void* nb_case_stream(const nb_case* c);
+
+/* ---- measurement ---------------------------------------------------------
+ * Bracket every launch of one kernel family with CUDA events on its stream
+ * (family names: "rhs_rk", "smooth", "resid_restrict", "coarse_cg",
+ * "pcg_matvec", "pcg_update", "correct", "div", "diag"; NULL disables).
+ * nb_ctx_profile_read returns the summed event time, the launch count and the
+ * algorithmic bytes those launches had to move (each array read or written
+ * once per cell; halos excluded). Reading resets the counters. */
+nb_status nb_ctx_profile(nb_ctx* ctx, const char* family);
+nb_status nb_ctx_profile_read(nb_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes);
+
+/* ---- pressure Poisson: the PoissonSolver seam ---------------------------- */
+/* Replaces MgPoisson::solve (core/src/flow/multigrid.cpp:206-355) behind
+ * PoissonSolver::solve(const UniformGrid&, const std::vector<double>& b,
+ * std::vector<double>& x) (core/include/nabla/flow/poisson.hpp:31-32).
+ * b and x are host arrays of nx*ny*nz doubles. The multigrid hierarchy is
+ * cached on the context keyed by the grid (multigrid.cpp:43-61, :211-266). */
+nb_status nb_poisson_solve(nb_ctx* ctx, const nb_grid_desc* grid, const double* b, double* x,
+                           double tol, int max_cycles, int precision, nb_poisson_report* rep);
+/* Replaces CgPoisson::applyA (core/src/flow/poisson.cpp:102-134). */
+nb_status nb_apply_laplacian(nb_ctx* ctx, const nb_grid_desc* grid, const double* x, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NABLA_B200_H */

@@ -1,0 +1,727 @@
+// nb_api.cu — the extern "C" boundary (include/nabla_b200.h) over the device
+// solver: context, resident cases, the SSP-RK3 step driver and the Poisson
+// seam. Host orchestration only; all arithmetic on the solution runs in the
+// kernels of nb_flow.cu and nb_mg.cu.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "nb_flow.cuh"
+#include "nb_mg.cuh"
+
+using namespace nb;
+
+struct nb_ctx {
+  int device = 0;
+  std::string err;
+  uint64_t launches = 0;
+  Profiler prof;
+  cudaStream_t stream = nullptr;
+  // MgPoisson-style cache for the host-array Poisson seam (multigrid.cpp:211-220)
+  std::map<std::pair<uint64_t, int>, std::unique_ptr<MgSolver>> mg_cache;
+  double* stage_a = nullptr;
+  double* stage_b = nullptr;
+  size_t stage_bytes = 0;
+};
+
+struct nb_case {
+  nb_ctx* ctx = nullptr;
+  nb_grid_desc grid{};
+  std::vector<uint8_t> solid;
+  nb_flow_config cfg{};
+  int precision = NB_PRECISION_FP64;
+  double nu = 0.0;
+  std::unique_ptr<MgSolver> mg;
+  FlowView F{};
+  cudaStream_t stream = nullptr;
+  double* uvw[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int cur = 0;
+  double* uvw0[3] = {nullptr, nullptr, nullptr};
+  double* p = nullptr;
+  double* b = nullptr;
+  double* staging = nullptr;
+  size_t staging_elems = 0;
+  BcOp* bc_out = nullptr;  // applyVelocityBC(enforceOutflow = true), phase 1
+  BcOp* bc_in = nullptr;   // applyVelocityBC(enforceOutflow = false), phase 1
+  BcOp* bc_solid = nullptr;  // phase 2: zero faces touching a solid
+  int n_out = 0, n_in = 0, n_solid = 0, serial_out = 0, serial_in = 0;
+  RedBuf rb{};
+  StepScalars* d_sc = nullptr;
+  StepScalars* h_sc = nullptr;
+  std::vector<void*> allocs;
+  uint64_t bytes = 0;
+  bool has_solid = false;
+  uint64_t nfluid = 0;
+  int step = 0;
+  double t = 0.0, dt_last = 0.0;
+
+  void* alloc(size_t n) {
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, n ? n : 16);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw ApiError{NB_ERR_OOM, "device allocation of " + std::to_string(n) + " bytes failed"};
+    }
+    allocs.push_back(q);
+    bytes += n;
+    return q;
+  }
+  ~nb_case() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* q : allocs) cudaFree(q);
+    if (h_sc) cudaFreeHost(h_sc);
+    mg.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+nb_status fail(nb_ctx* ctx, nb_status s, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return s;
+}
+
+template <class Fn>
+nb_status guarded(nb_ctx* ctx, Fn&& fn) {
+  try {
+    return fn();
+  } catch (const ApiError& e) {
+    return fail(ctx, e.status, e.what);
+  } catch (const CudaError& e) {
+    return fail(ctx, NB_ERR_CUDA, e.what);
+  } catch (const std::exception& e) {
+    return fail(ctx, NB_ERR_BAD_ARG, e.what());
+  }
+}
+
+bool grid_ok(const nb_grid_desc* g, std::string& why) {
+  if (!g) { why = "grid is NULL"; return false; }
+  if (g->nx < 1 || g->ny < 1 || g->nz < 1) { why = "grid dimensions must be >= 1"; return false; }
+  if (!(g->dx > 0.0) || !(g->dy > 0.0) || !(g->dz > 0.0)) { why = "grid spacing must be > 0"; return false; }
+  if (static_cast<long long>(g->nx) * g->ny * g->nz > (1ll << 31) / 2) { why = "grid too large"; return false; }
+  for (int f = 0; f < 6; ++f)
+    if (g->face[f].type < NB_BC_WALL || g->face[f].type > NB_BC_PERIODIC) { why = "bad boundary type"; return false; }
+  for (int a = 0; a < 3; ++a)
+    if ((g->face[2 * a].type == NB_BC_PERIODIC) != (g->face[2 * a + 1].type == NB_BC_PERIODIC)) {
+      why = "periodic faces must come in pairs";
+      return false;
+    }
+  return true;
+}
+
+// Host mirror of the device storage index (brick slot or trailing slab).
+long long h_cell(const HostLevel& L, int i, int j, int k) {
+  const int b = L.lut[((k >> 3) * L.nby + (j >> 3)) * L.nbx + (i >> 3)];
+  return static_cast<long long>(b) * BR3 + (((k & 7) << 6) | ((j & 7) << 3) | (i & 7));
+}
+long long h_face(const HostLevel& L, long long nb, int comp, int i, int j, int k) {
+  if (comp == 0 && i == L.nx) return nb + j + static_cast<long long>(L.ny) * k;
+  if (comp == 1 && j == L.ny) return nb + i + static_cast<long long>(L.nx) * k;
+  if (comp == 2 && k == L.nz) return nb + i + static_cast<long long>(L.nx) * j;
+  return h_cell(L, i, j, k);
+}
+
+// inletVelocityAt (core/src/flow/ns_solver.cpp:71-93)
+double h_inlet(const nb_grid_desc& g, int face, int a, int comp) {
+  const nb_face_bc& fb = g.face[face];
+  double mag = fb.inlet_speed;
+  if (fb.profile == NB_PROFILE_PARABOLIC) {
+    const double H = g.ny * g.dy;
+    const double yc = g.origin[1] + 0.5 * H;
+    const double y = g.origin[1] + (a + 0.5) * g.dy;
+    const double r = (y - yc) / (0.5 * H);
+    mag = 1.5 * fb.inlet_speed * (1.0 - r * r);
+  }
+  return fb.inlet_axis == comp ? mag : 0.0;
+}
+
+bool h_solid(const nb_case& c, int i, int j, int k) {
+  const nb_grid_desc& g = c.grid;
+  if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) return false;
+  return c.solid[static_cast<size_t>(i) + static_cast<size_t>(g.nx) * (j + static_cast<size_t>(g.ny) * k)] != 0;
+}
+
+// applyVelocityBC (core/src/flow/ns_solver.cpp:221-309) as ordered face actions.
+void build_bc(nb_case& c, bool outflow, std::vector<BcOp>& ops, std::vector<BcOp>& solid_ops) {
+  const nb_grid_desc& g = c.grid;
+  const HostLevel& L = c.mg->host0();
+  const long long nb = c.F.nb;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  auto set = [&](int comp, long long idx, double v) { ops.push_back(BcOp{comp, 0, idx, 0, v}); };
+  auto copy = [&](int comp, long long idx, long long src) { ops.push_back(BcOp{comp, 1, idx, src, 0.0}); };
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int side = 0; side < 2; ++side) {
+        const int face = side, i = side == 0 ? 0 : nx;
+        const long long idx = h_face(L, nb, 0, i, j, k);
+        switch (g.face[face].type) {
+          case NB_BC_WALL: set(0, idx, 0.0); break;
+          case NB_BC_INLET: set(0, idx, h_inlet(g, face, j, 0)); break;
+          case NB_BC_OUTLET:
+            if (outflow) copy(0, idx, h_face(L, nb, 0, side == 0 ? 1 : nx - 1, j, k));
+            break;
+          default: break;
+        }
+      }
+  for (int k = 0; k < nz; ++k)
+    for (int i = 0; i < nx; ++i)
+      for (int side = 0; side < 2; ++side) {
+        const int face = 2 + side, j = side == 0 ? 0 : ny;
+        const long long idx = h_face(L, nb, 1, i, j, k);
+        switch (g.face[face].type) {
+          case NB_BC_WALL: set(1, idx, 0.0); break;
+          case NB_BC_INLET: set(1, idx, h_inlet(g, face, i, 1)); break;
+          case NB_BC_OUTLET:
+            if (outflow) copy(1, idx, h_face(L, nb, 1, i, side == 0 ? 1 : ny - 1, k));
+            break;
+          default: break;
+        }
+      }
+  if (nz > 1)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        for (int side = 0; side < 2; ++side) {
+          const int face = 4 + side, k = side == 0 ? 0 : nz;
+          const long long idx = h_face(L, nb, 2, i, j, k);
+          switch (g.face[face].type) {
+            case NB_BC_WALL: set(2, idx, 0.0); break;
+            case NB_BC_INLET: set(2, idx, h_inlet(g, face, i, 2)); break;
+            case NB_BC_OUTLET:
+              if (outflow) copy(2, idx, h_face(L, nb, 2, i, j, side == 0 ? 1 : nz - 1));
+              break;
+            default: break;
+          }
+        }
+  if (c.has_solid) {
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i <= nx; ++i)
+          if (h_solid(c, i - 1, j, k) || h_solid(c, i, j, k))
+            solid_ops.push_back(BcOp{0, 0, h_face(L, nb, 0, i, j, k), 0, 0.0});
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j <= ny; ++j)
+        for (int i = 0; i < nx; ++i)
+          if (h_solid(c, i, j - 1, k) || h_solid(c, i, j, k))
+            solid_ops.push_back(BcOp{1, 0, h_face(L, nb, 1, i, j, k), 0, 0.0});
+    if (nz > 1)
+      for (int k = 0; k <= nz; ++k)
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i < nx; ++i)
+            if (h_solid(c, i, j, k - 1) || h_solid(c, i, j, k))
+              solid_ops.push_back(BcOp{2, 0, h_face(L, nb, 2, i, j, k), 0, 0.0});
+  }
+}
+
+// A copy whose source is also written in the same list must run in order.
+int needs_serial(const std::vector<BcOp>& ops) {
+  std::map<std::pair<int, long long>, int> dst;
+  for (const BcOp& o : ops) dst[{o.comp, o.idx}] = 1;
+  for (const BcOp& o : ops)
+    if (o.action == 1 && dst.count({o.comp, o.src})) return 1;
+  return 0;
+}
+
+BcOp* upload_ops(nb_case& c, const std::vector<BcOp>& ops) {
+  if (ops.empty()) return nullptr;
+  BcOp* d = static_cast<BcOp*>(c.alloc(ops.size() * sizeof(BcOp)));
+  NB_CUDA(cudaMemcpy(d, ops.data(), ops.size() * sizeof(BcOp), cudaMemcpyHostToDevice));
+  return d;
+}
+
+void apply_bc(nb_case& c, double* const* f, bool outflow) {
+  const int n = outflow ? c.n_out : c.n_in;
+  if (n) {
+    launch_bc(c.stream, outflow ? c.bc_out : c.bc_in, n, outflow ? c.serial_out : c.serial_in, f[0],
+              f[1], f[2]);
+    c.ctx->launches++;
+  }
+  if (c.n_solid) {
+    launch_bc(c.stream, c.bc_solid, c.n_solid, 0, f[0], f[1], f[2]);
+    c.ctx->launches++;
+  }
+}
+
+// One flow-kernel launch: counted, and bracketed with events when profiled.
+template <class Fn>
+void flow_launch(nb_case& c, const char* fam, double bytes, Fn&& fn) {
+  Profiler& P = c.ctx->prof;
+  const bool on = P.on(fam);
+  if (on) P.begin(c.stream);
+  fn();
+  if (on) P.end(c.stream, bytes);
+  c.ctx->launches++;
+}
+
+double ncell_of(const nb_case& c) {
+  return static_cast<double>(c.grid.nx) * c.grid.ny * c.grid.nz;
+}
+
+void upload_lex(nb_case& c, int comp, const double* host, double* dst) {
+  const long long n = lex_size(c.F, comp);
+  NB_CUDA(cudaMemcpyAsync(c.staging, host, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  launch_convert(c.stream, c.F, comp, 0, c.staging, dst);
+  c.ctx->launches++;
+}
+
+void download_lex(nb_case& c, int comp, const double* src, double* host) {
+  const long long n = lex_size(c.F, comp);
+  launch_convert(c.stream, c.F, comp, 1, src, c.staging);
+  c.ctx->launches++;
+  NB_CUDA(cudaMemcpyAsync(host, c.staging, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  NB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// NSSolver::project (core/src/flow/ns_solver.cpp:475-579) on the current fields.
+nb_poisson_report project(nb_case& c, double* const* f, double dt) {
+  apply_bc(c, f, true);
+  flow_launch(c, "div", ncell_of(c) * 33, [&] { launch_div(c.stream, c.F, f[0], f[1], f[2], c.b); });
+  c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters);
+  flow_launch(c, "correct", ncell_of(c) * 65,
+              [&] { launch_correct(c.stream, c.F, c.mg->phi(), dt, f[0], f[1], f[2], c.p); });
+  apply_bc(c, f, false);
+  return c.mg->fetch_report(c.stream);
+}
+
+double compute_dt(nb_case& c) {
+  double* const* f = c.uvw[c.cur];
+  const nb_grid_desc& g = c.grid;
+  const bool twoD = g.nz == 1;
+  const double visc = 2.0 * c.nu *
+                      (1.0 / (g.dx * g.dx) + 1.0 / (g.dy * g.dy) + (twoD ? 0.0 : 1.0 / (g.dz * g.dz)));
+  launch_max_inv(c.stream, c.F, f[0], f[1], f[2], visc, c.rb, c.d_sc);
+  c.ctx->launches++;
+  NB_CUDA(cudaMemcpyAsync(c.h_sc, c.d_sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, c.stream));
+  NB_CUDA(cudaStreamSynchronize(c.stream));
+  return c.cfg.cfl / c.h_sc->maxinv;
+}
+
+// NSSolver::step(double) (core/src/flow/ns_solver.cpp:767-824).
+void do_step(nb_case& c, double dt, nb_step_report* rep) {
+  if (dt <= 0.0) dt = compute_dt(c);
+  const size_t fb[3] = {static_cast<size_t>(store_size(c.F, 0)) * 8, static_cast<size_t>(store_size(c.F, 1)) * 8,
+                        static_cast<size_t>(store_size(c.F, 2)) * 8};
+  double** A = c.uvw[c.cur];
+  double** B = c.uvw[1 - c.cur];
+  for (int q = 0; q < 3; ++q)
+    NB_CUDA(cudaMemcpyAsync(c.uvw0[q], A[q], fb[q], cudaMemcpyDeviceToDevice, c.stream));
+  apply_bc(c, A, true);
+  nb_poisson_report pr[3];
+  const int mixed = c.precision == NB_PRECISION_MIXED;
+  for (int stage = 1; stage <= 3; ++stage) {
+    double** in = (stage == 2) ? B : A;
+    double** out = (stage == 2) ? A : B;
+    flow_launch(c, "rhs_rk", ncell_of(c) * 73, [&] {
+      launch_rhs_rk(c.stream, c.F, stage, dt, in[0], in[1], in[2], c.uvw0[0], c.uvw0[1], c.uvw0[2],
+                    out[0], out[1], out[2], mixed);
+    });
+    pr[stage - 1] = project(c, out, dt);
+  }
+  c.cur = 1 - c.cur;  // the stage-3 output (B) is the new state
+  double** S = c.uvw[c.cur];
+  flow_launch(c, "diag", ncell_of(c) * 57, [&] {
+    launch_diag(c.stream, c.F, S[0], S[1], S[2], c.uvw0[0], c.uvw0[1], c.uvw0[2], c.p, c.rb, c.d_sc);
+  });
+  NB_CUDA(cudaMemcpyAsync(c.h_sc, c.d_sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, c.stream));
+  NB_CUDA(cudaStreamSynchronize(c.stream));
+  c.step += 1;
+  c.t += dt;
+  c.dt_last = dt;
+  if (!rep) return;
+  const nb_grid_desc& g = c.grid;
+  const double nfaces = static_cast<double>(lex_size(c.F, 0) + lex_size(c.F, 1) + lex_size(c.F, 2));
+  const StepScalars& sc = *c.h_sc;
+  std::memset(rep, 0, sizeof(*rep));
+  rep->step = c.step;
+  rep->t = c.t;
+  rep->dt = dt;
+  rep->cfl = c.cfg.cfl;
+  rep->momentum_residual = std::sqrt(sc.du2 / nfaces) / (dt * c.cfg.velocity_scale + 1e-300);
+  rep->continuity_residual = c.nfluid ? std::sqrt(sc.div2 / static_cast<double>(c.nfluid)) : 0.0;
+  rep->divergence_max = sc.divmax;
+  const double ay = g.dx * g.dz;
+  rep->mass_error = std::fabs(sc.mass) / (c.cfg.velocity_scale * (g.ny * ay) + 1e-300);
+  rep->poisson_iters = pr[0].iterations + pr[1].iterations + pr[2].iterations;
+  rep->poisson_residual = std::max(pr[0].residual, std::max(pr[1].residual, pr[2].residual));
+  rep->converged = pr[0].converged && pr[1].converged && pr[2].converged;
+  if (c.has_solid) {
+    double aref = c.cfg.ref_area;
+    if (aref <= 0.0) aref = c.cfg.ref_length * c.cfg.ref_length;
+    const double q = 0.5 * c.cfg.density * c.cfg.velocity_scale * c.cfg.velocity_scale * aref + 1e-300;
+    rep->cd = sc.fx / q;
+    rep->cl = sc.fy / q;
+  }
+  rep->cell_count = static_cast<uint64_t>(g.nx) * g.ny * g.nz;
+  rep->accepted = (rep->continuity_residual < c.cfg.tol_continuity && rep->mass_error < c.cfg.tol_mass) ? 1 : 0;
+}
+
+void ensure_staging(nb_ctx* ctx, size_t elems) {
+  if (ctx->stage_bytes >= elems * sizeof(double)) return;
+  if (ctx->stage_a) cudaFree(ctx->stage_a);
+  if (ctx->stage_b) cudaFree(ctx->stage_b);
+  ctx->stage_a = ctx->stage_b = nullptr;
+  ctx->stage_bytes = 0;
+  NB_CUDA(cudaMalloc(&ctx->stage_a, elems * sizeof(double)));
+  NB_CUDA(cudaMalloc(&ctx->stage_b, elems * sizeof(double)));
+  ctx->stage_bytes = elems * sizeof(double);
+}
+
+MgSolver& ctx_solver(nb_ctx* ctx, const nb_grid_desc& g, int precision) {
+  const auto key = std::make_pair(grid_signature(g), precision);
+  auto it = ctx->mg_cache.find(key);
+  if (it == ctx->mg_cache.end()) {
+    auto s = std::make_unique<MgSolver>(g, precision, LaunchCounter{&ctx->launches, &ctx->prof});
+    it = ctx->mg_cache.emplace(key, std::move(s)).first;
+  }
+  return *it->second;
+}
+
+FlowView cell_view(const MgSolver& mg) {
+  FlowView F{};
+  F.L = mg.view0();
+  F.nb = static_cast<long long>(F.L.nbrick) * BR3;
+  return F;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nb_status_string(nb_status s) {
+  switch (s) {
+    case NB_OK: return "ok";
+    case NB_ERR_BAD_ARG: return "bad argument";
+    case NB_ERR_OOM: return "out of device memory";
+    case NB_ERR_NOT_CONVERGED: return "not converged";
+    case NB_ERR_NAN: return "NaN detected";
+    case NB_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+    case NB_ERR_CUDA: return "CUDA error";
+    case NB_ERR_UNSUPPORTED: return "unsupported configuration";
+  }
+  return "unknown status";
+}
+
+nb_status nb_ctx_create(int device, nb_ctx** out) {
+  if (!out) return NB_ERR_BAD_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    (void)cudaGetLastError();
+    return NB_ERR_CUDA;
+  }
+  if (device < 0 || device >= n) return NB_ERR_BAD_ARG;
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return NB_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return NB_ERR_CUDA;
+  auto* ctx = new nb_ctx();
+  ctx->device = device;
+  const nb_status s = guarded(ctx, [&] {
+    NB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    flow_kernel_setup();
+    return NB_OK;
+  });
+  if (s != NB_OK) {
+    delete ctx;
+    return s;
+  }
+  *out = ctx;
+  return NB_OK;
+}
+
+void nb_ctx_destroy(nb_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->mg_cache.clear();
+  if (ctx->stage_a) cudaFree(ctx->stage_a);
+  if (ctx->stage_b) cudaFree(ctx->stage_b);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* nb_last_error(const nb_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+uint64_t nb_ctx_launch_count(const nb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+nb_status nb_ctx_synchronize(nb_ctx* ctx) {
+  if (!ctx) return NB_ERR_BAD_ARG;
+  return guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    NB_CUDA(cudaDeviceSynchronize());
+    return NB_OK;
+  });
+}
+
+nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_config* cfg,
+                         int precision, nb_case** out) {
+  if (!ctx || !out || !cfg) return NB_ERR_BAD_ARG;
+  *out = nullptr;
+  std::string why;
+  if (!grid_ok(grid, why)) return fail(ctx, NB_ERR_BAD_ARG, why);
+  if (precision != NB_PRECISION_FP64 && precision != NB_PRECISION_MIXED)
+    return fail(ctx, NB_ERR_BAD_ARG, "precision must be NB_PRECISION_FP64 or NB_PRECISION_MIXED");
+  if (!(cfg->reynolds > 0.0)) return fail(ctx, NB_ERR_BAD_ARG, "reynolds must be > 0");
+  auto c = std::make_unique<nb_case>();
+  c->ctx = ctx;
+  const nb_status s = guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    NB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->grid = *grid;
+    const size_t ncell = static_cast<size_t>(grid->nx) * grid->ny * grid->nz;
+    c->solid.assign(ncell, 0);
+    if (grid->solid) std::memcpy(c->solid.data(), grid->solid, ncell);
+    c->grid.solid = c->solid.data();
+    c->cfg = *cfg;
+    c->precision = precision;
+    c->nu = cfg->velocity_scale * cfg->ref_length / cfg->reynolds;  // ns_solver.cpp:54
+    for (uint8_t v : c->solid)
+      if (v) { c->has_solid = true; break; }
+    c->mg = std::make_unique<MgSolver>(c->grid, precision, LaunchCounter{&ctx->launches, &ctx->prof});
+    c->nfluid = c->mg->host0().nfluid;
+    FlowView& F = c->F;
+    F.L = c->mg->view0();
+    F.nb = static_cast<long long>(F.L.nbrick) * BR3;
+    for (int a = 0; a < 3; ++a) F.origin[a] = grid->origin[a];
+    for (int f = 0; f < 6; ++f) {
+      for (int a = 0; a < 3; ++a) F.wallv[f][a] = grid->face[f].wall_velocity[a];
+      F.inlet_speed[f] = grid->face[f].inlet_speed;
+      F.profile[f] = grid->face[f].profile;
+      F.inlet_axis[f] = grid->face[f].inlet_axis;
+    }
+    for (int a = 0; a < 3; ++a) F.per[a] = grid->face[2 * a].type == NB_BC_PERIODIC;
+    F.weno = cfg->convection == NB_CONV_WENO5;
+    F.has_solid = c->has_solid;
+    F.nu = c->nu;
+    for (int a = 0; a < 3; ++a) F.bf[a] = cfg->body_force[a];
+    F.density = cfg->density;
+    F.velocity_scale = cfg->velocity_scale;
+    for (int h = 0; h < 2; ++h)
+      for (int q = 0; q < 3; ++q) {
+        const size_t nb = static_cast<size_t>(store_size(F, q)) * sizeof(double);
+        c->uvw[h][q] = static_cast<double*>(c->alloc(nb));
+        NB_CUDA(cudaMemset(c->uvw[h][q], 0, nb));
+      }
+    for (int q = 0; q < 3; ++q) {
+      const size_t nb = static_cast<size_t>(store_size(F, q)) * sizeof(double);
+      c->uvw0[q] = static_cast<double*>(c->alloc(nb));
+      NB_CUDA(cudaMemset(c->uvw0[q], 0, nb));
+    }
+    const size_t ncs = static_cast<size_t>(F.nb);
+    c->p = static_cast<double*>(c->alloc(ncs * sizeof(double)));
+    c->b = static_cast<double*>(c->alloc(ncs * sizeof(double)));
+    NB_CUDA(cudaMemset(c->p, 0, ncs * sizeof(double)));
+    NB_CUDA(cudaMemset(c->b, 0, ncs * sizeof(double)));
+    c->staging_elems = static_cast<size_t>(std::max({lex_size(F, 0), lex_size(F, 1), lex_size(F, 2)}));
+    c->staging = static_cast<double*>(c->alloc(c->staging_elems * sizeof(double)));
+    std::vector<BcOp> out_ops, in_ops, solid_ops, dummy;
+    build_bc(*c, true, out_ops, solid_ops);
+    build_bc(*c, false, in_ops, dummy);
+    c->n_out = static_cast<int>(out_ops.size());
+    c->n_in = static_cast<int>(in_ops.size());
+    c->n_solid = static_cast<int>(solid_ops.size());
+    c->serial_out = needs_serial(out_ops);
+    c->serial_in = needs_serial(in_ops);
+    c->bc_out = upload_ops(*c, out_ops);
+    c->bc_in = upload_ops(*c, in_ops);
+    c->bc_solid = upload_ops(*c, solid_ops);
+    c->rb.max_blocks = 148 * 4;
+    c->rb.partials = static_cast<double*>(c->alloc(RED_KMAX * c->rb.max_blocks * sizeof(double)));
+    c->rb.counter = static_cast<unsigned*>(c->alloc(sizeof(unsigned)));
+    NB_CUDA(cudaMemset(c->rb.counter, 0, sizeof(unsigned)));
+    c->d_sc = static_cast<StepScalars*>(c->alloc(sizeof(StepScalars)));
+    NB_CUDA(cudaMallocHost(&c->h_sc, sizeof(StepScalars)));
+    NB_CUDA(cudaDeviceSynchronize());
+    return NB_OK;
+  });
+  if (s != NB_OK) return s;
+  *out = c.release();
+  return NB_OK;
+}
+
+void nb_case_destroy(nb_case* c) {
+  if (!c) return;
+  cudaSetDevice(c->ctx->device);
+  delete c;
+}
+
+uint64_t nb_case_device_bytes(const nb_case* c) {
+  return c ? c->bytes + c->mg->device_bytes() : 0;
+}
+
+void* nb_case_stream(const nb_case* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+nb_status nb_ctx_profile(nb_ctx* ctx, const char* family) {
+  if (!ctx) return NB_ERR_BAD_ARG;
+  ctx->prof.family = family ? family : "";
+  return NB_OK;
+}
+
+nb_status nb_ctx_profile_read(nb_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes) {
+  if (!ctx) return NB_ERR_BAD_ARG;
+  return guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    const double ms = ctx->prof.drain(launches, bytes);
+    if (total_ms) *total_ms = ms;
+    return NB_OK;
+  });
+}
+
+uint64_t nb_case_cell_count(const nb_case* c) {
+  return c ? static_cast<uint64_t>(c->grid.nx) * c->grid.ny * c->grid.nz : 0;
+}
+
+nb_status nb_case_set_state(nb_case* c, const double* u, const double* v, const double* w,
+                            const double* p, int step, double t, double dt_last) {
+  if (!c || !u || !v || !w || !p) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    double** f = c->uvw[c->cur];
+    upload_lex(*c, 0, u, f[0]);
+    upload_lex(*c, 1, v, f[1]);
+    upload_lex(*c, 2, w, f[2]);
+    upload_lex(*c, 3, p, c->p);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    c->step = step;
+    c->t = t;
+    c->dt_last = dt_last;
+    return NB_OK;
+  });
+}
+
+nb_status nb_case_get_state(nb_case* c, double* u, double* v, double* w, double* p) {
+  if (!c) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    double** f = c->uvw[c->cur];
+    if (u) download_lex(*c, 0, f[0], u);
+    if (v) download_lex(*c, 1, f[1], v);
+    if (w) download_lex(*c, 2, f[2], w);
+    if (p) download_lex(*c, 3, c->p, p);
+    return NB_OK;
+  });
+}
+
+nb_status nb_case_get_clock(nb_case* c, int* step, double* t, double* dt_last) {
+  if (!c) return NB_ERR_BAD_ARG;
+  if (step) *step = c->step;
+  if (t) *t = c->t;
+  if (dt_last) *dt_last = c->dt_last;
+  return NB_OK;
+}
+
+// NSSolver::initialize (core/src/flow/ns_solver.cpp:95-112)
+nb_status nb_case_initialize(nb_case* c) {
+  if (!c) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    const long long nu = lex_size(c->F, 0), nv = lex_size(c->F, 1), nw = lex_size(c->F, 2),
+                    np = lex_size(c->F, 3);
+    std::vector<double> U(nu, 0.0), V(nv, 0.0), W(nw, 0.0), P(np, 0.0);
+    for (int f = 0; f < 6; ++f)
+      if (c->grid.face[f].type == NB_BC_INLET && c->grid.face[f].inlet_axis == 0) {
+        std::fill(U.begin(), U.end(), c->grid.face[f].inlet_speed);
+        break;
+      }
+    double** fl = c->uvw[c->cur];
+    upload_lex(*c, 0, U.data(), fl[0]);
+    upload_lex(*c, 1, V.data(), fl[1]);
+    upload_lex(*c, 2, W.data(), fl[2]);
+    upload_lex(*c, 3, P.data(), c->p);
+    apply_bc(*c, fl, true);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    c->step = 0;
+    c->t = 0.0;
+    c->dt_last = 0.0;
+    return NB_OK;
+  });
+}
+
+nb_status nb_case_compute_dt(nb_case* c, double* dt) {
+  if (!c || !dt) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    *dt = compute_dt(*c);
+    return NB_OK;
+  });
+}
+
+nb_status nb_step(nb_case* c, double dt, nb_step_report* rep) {
+  if (!c) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    nb_step_report r{};
+    do_step(*c, dt, &r);
+    if (rep) *rep = r;
+    if (std::isnan(r.momentum_residual) || std::isnan(r.continuity_residual))
+      return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");
+    return NB_OK;
+  });
+}
+
+nb_status nb_step_many(nb_case* c, double dt, int nsteps, nb_step_report* rep) {
+  if (!c || nsteps < 0) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    nb_step_report r{};
+    for (int i = 0; i < nsteps; ++i) do_step(*c, dt, &r);
+    if (rep) *rep = r;
+    if (std::isnan(r.momentum_residual)) return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");
+    return NB_OK;
+  });
+}
+
+nb_status nb_poisson_solve(nb_ctx* ctx, const nb_grid_desc* grid, const double* b, double* x,
+                           double tol, int max_cycles, int precision, nb_poisson_report* rep) {
+  if (!ctx || !b || !x || max_cycles < 0) return NB_ERR_BAD_ARG;
+  std::string why;
+  if (!grid_ok(grid, why)) return fail(ctx, NB_ERR_BAD_ARG, why);
+  return guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    MgSolver& mg = ctx_solver(ctx, *grid, precision);
+    const FlowView F = cell_view(mg);
+    const size_t n = static_cast<size_t>(grid->nx) * grid->ny * grid->nz;
+    ensure_staging(ctx, std::max(n, static_cast<size_t>(F.nb)));
+    NB_CUDA(cudaMemcpyAsync(ctx->stage_a, b, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    NB_CUDA(cudaMemsetAsync(ctx->stage_b, 0, F.nb * sizeof(double), ctx->stream));
+    launch_convert(ctx->stream, F, 3, 0, ctx->stage_a, ctx->stage_b);
+    ctx->launches++;
+    mg.solve_async(ctx->stream, ctx->stage_b, tol, max_cycles);
+    const nb_poisson_report r = mg.fetch_report(ctx->stream);
+    launch_convert(ctx->stream, F, 3, 1, mg.phi(), ctx->stage_a);
+    ctx->launches++;
+    NB_CUDA(cudaMemcpyAsync(x, ctx->stage_a, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    NB_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (rep) *rep = r;
+    return NB_OK;
+  });
+}
+
+nb_status nb_apply_laplacian(nb_ctx* ctx, const nb_grid_desc* grid, const double* x, double* out) {
+  if (!ctx || !x || !out) return NB_ERR_BAD_ARG;
+  std::string why;
+  if (!grid_ok(grid, why)) return fail(ctx, NB_ERR_BAD_ARG, why);
+  return guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    MgSolver& mg = ctx_solver(ctx, *grid, NB_PRECISION_FP64);
+    const FlowView F = cell_view(mg);
+    const size_t n = static_cast<size_t>(grid->nx) * grid->ny * grid->nz;
+    ensure_staging(ctx, std::max(n, static_cast<size_t>(F.nb)) * 2);
+    double* xa = ctx->stage_b;
+    double* xo = ctx->stage_b + F.nb;
+    NB_CUDA(cudaMemcpyAsync(ctx->stage_a, x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    NB_CUDA(cudaMemsetAsync(xa, 0, F.nb * sizeof(double), ctx->stream));
+    launch_convert(ctx->stream, F, 3, 0, ctx->stage_a, xa);
+    mg.apply_a(ctx->stream, xa, xo);
+    launch_convert(ctx->stream, F, 3, 1, xo, ctx->stage_a);
+    ctx->launches += 2;
+    NB_CUDA(cudaMemcpyAsync(out, ctx->stage_a, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    NB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return NB_OK;
+  });
+}
+
+}  // extern "C"

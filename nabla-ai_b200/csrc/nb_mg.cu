@@ -1,0 +1,949 @@
+// nb_mg.cu — sm_100a kernels and host driver of the MG-PCG pressure solve.
+//
+// Bandwidth-bound stencils on bricks: one 512-thread CTA walks bricks
+// (grid-stride), thread t owns cell t of the brick. No tensor cores (the
+// operator is a 7-point stencil, not a dense contraction).
+//
+// Reference arithmetic followed (paths within the reference project):
+//   stencil / diagonal     core/src/flow/poisson.cpp:18-134
+//   smooth / removeMean    core/src/flow/multigrid.cpp:81-114
+//   residual + restrict    core/src/flow/multigrid.cpp:116-154
+//   prolongAdd             core/src/flow/multigrid.cpp:158-173
+//   vcycle                 core/src/flow/multigrid.cpp:175-194
+//   coarsest CgPoisson     core/src/flow/poisson.cpp:136-252
+//   flexible PCG           core/src/flow/multigrid.cpp:268-355
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "nb_mg.cuh"
+#include "nb_reduce.cuh"
+
+namespace nb {
+
+namespace {
+
+constexpr int NT = 512;          // threads per CTA = cells per brick
+constexpr int MAX_GRID = 148 * 4;  // grid-stride CTA cap (4 CTAs of 512 per SM)
+constexpr double kOmega = 0.8;   // multigrid.cpp:38
+constexpr int COARSE_MAX_CELLS = 4096;
+
+inline int grid_for(int nbrick) { return nbrick < MAX_GRID ? nbrick : MAX_GRID; }
+
+__device__ __forceinline__ bool stopped(const SolveFlags* f, int maxit) {
+  return f != nullptr && (f->stop != 0 || f->iters >= maxit);
+}
+
+// Value of a level vector at an (in-grid, fluid) cell after the operations
+// still pending on it: the lazy removeMean (x - mean) and the lazy
+// prolongAdd (+ e[parent], itself with the coarse level's pending mean).
+template <typename T>
+struct XFetch {
+  const T* x;            // nullptr => the vector is identically zero
+  const double* xmean;   // pending mean (nullptr => none)
+  const T* ec;           // pending prolongation source (nullptr => none)
+  const double* ecmean;  // pending mean of ec
+  LevelView C;           // coarse level (for parent lookup)
+  int fx, fy, fz;
+  __device__ __forceinline__ T operator()(int n, int gi, int gj, int gk) const {
+    T v = x ? x[n] : T(0);
+    if (xmean) v = v - static_cast<T>(*xmean);
+    if (ec) {
+      T e = ec[cell_index(C, gi / fx, gj / fy, gk / fz)];
+      if (ecmean) e = e - static_cast<T>(*ecmean);
+      v = v + e;
+    }
+    return v;
+  }
+};
+
+// Row of the -Laplacian at fluid cell (gi,gj,gk): returns diag (raw sum of
+// face coefficients) and off = sum coeff * x[n] in the reference's order
+// (axis 0 side -1, +1, axis 1, axis 2).
+template <typename T, class F>
+__device__ __forceinline__ void stencil_row(const LevelView& L, int gi, int gj, int gk, const F& fx,
+                                            T& diag, T& off) {
+  diag = T(0);
+  off = T(0);
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    if (axis == 2 && L.twoD) continue;
+    const T h2 = static_cast<T>(L.h2[axis]);
+#pragma unroll
+    for (int side = -1; side <= 1; side += 2) {
+      int n = 0;
+      const int kind = resolve_face(L, gi, gj, gk, axis, side, n);
+      if (kind == 1) {
+        int c[3] = {gi, gj, gk};
+        const int dims[3] = {L.nx, L.ny, L.nz};
+        c[axis] = wrapi(c[axis] + side, dims[axis]);
+        diag += h2;
+        off += h2 * fx(n, c[0], c[1], c[2]);
+      } else if (kind == 2) {
+        diag += T(2) * h2;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Damped-Jacobi sweep (multigrid.cpp:102-114), one sweep per launch.
+//   xout = fluid ? x' + omega (b' - A x') / D : 0
+// where x' / b' include pending mean / prolongation. Optionally reduces the
+// fluid sum of xout into `mean_out` (= sum / nfluid) for the next removeMean.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict__ b,
+                                               const double* bmean, XFetch<T> X, T* __restrict__ xout,
+                                               RedBuf rb, double* mean_out, double inv_nfluid,
+                                               const SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const uint8_t ty = L.type[c];
+    T out = T(0);
+    if (ty == CELL_FLUID) {
+      int gi, gj, gk;
+      cell_coords(L, c, gi, gj, gk);
+      T diag, off;
+      stencil_row<T>(L, gi, gj, gk, X, diag, off);
+      const T xc = X(c, gi, gj, gk);
+      T bc = b[c];
+      if (bmean) bc = bc - static_cast<T>(*bmean);
+      const T Ax = diag * xc - off;
+      const T dM = diag > T(0) ? diag : T(1);
+      out = xc + static_cast<T>(kOmega) * (bc - Ax) / dM;
+      part[0] += static_cast<double>(out);
+    }
+    xout[c] = out;
+  }
+  if (mean_out) {
+    grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Residual + full-weighting restriction (multigrid.cpp:116-154): one CTA per
+// fine brick computes r = fluid ? b' - A x' : 0 into shared memory, then each
+// coarse cell covered by the brick averages its fluid children, summed in the
+// reference's lexicographic child order (k, then j, then i).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __restrict__ b,
+                                                       const double* bmean, XFetch<T> X, LevelView C,
+                                                       int fx, int fy, int fz, T* __restrict__ rc,
+                                                       RedBuf rb, double* mean_out, double inv_nfluid_c,
+                                                       const SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;
+  __shared__ T rs[BR3];
+  __shared__ uint8_t fl[BR3];
+  double part[1] = {0.0};
+  const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
+  for (int brick = blockIdx.x; brick < F.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const uint8_t ty = F.type[c];
+    T r = T(0);
+    if (ty == CELL_FLUID) {
+      int gi, gj, gk;
+      cell_coords(F, c, gi, gj, gk);
+      T diag, off;
+      stencil_row<T>(F, gi, gj, gk, X, diag, off);
+      T bc = b[c];
+      if (bmean) bc = bc - static_cast<T>(*bmean);
+      r = bc - (diag * X(c, gi, gj, gk) - off);
+    }
+    rs[threadIdx.x] = r;
+    fl[threadIdx.x] = (ty == CELL_FLUID);
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < cx * cy * cz) {
+      const int lci = t % cx, lcj = (t / cx) % cy, lck = t / (cx * cy);
+      const int gci = F.bcoord[3 * brick] * cx + lci;
+      const int gcj = F.bcoord[3 * brick + 1] * cy + lcj;
+      const int gck = F.bcoord[3 * brick + 2] * cz + lck;
+      if (gci < C.nx && gcj < C.ny && gck < C.nz) {
+        T sum = T(0);
+        int count = 0;
+        for (int dk = 0; dk < fz; ++dk)
+          for (int dj = 0; dj < fy; ++dj)
+            for (int di = 0; di < fx; ++di) {
+              const int l = ((lck * fz + dk) << 6) | ((lcj * fy + dj) << 3) | (lci * fx + di);
+              if (fl[l]) {
+                sum += rs[l];
+                ++count;
+              }
+            }
+        const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
+        rc[cell_index(C, gci, gcj, gck)] = val;
+        part[0] += static_cast<double>(val);
+      }
+    }
+    __syncthreads();
+  }
+  if (mean_out) {
+    grid_reduce<1>(part, rb, [=] __device__(const double* tt) { *mean_out = tt[0] * inv_nfluid_c; });
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest-level solve: CgPoisson(1e-6, 500)::solve (poisson.cpp:136-252) in
+// one CTA with every vector in shared memory (FP64 in both forms). The level
+// is held lexicographically in shared memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double bsum_bcast(double v, double* sh) {
+  double a[1] = {v};
+  block_reduce<1>(a, sh);
+  if (threadIdx.x == 0) sh[64] = a[0];
+  __syncthreads();
+  return sh[64];
+}
+__device__ __forceinline__ void bsum2_bcast(double& v0, double& v1, double* sh) {
+  double a[2] = {v0, v1};
+  block_reduce<2>(a, sh);
+  if (threadIdx.x == 0) {
+    sh[64] = a[0];
+    sh[65] = a[1];
+  }
+  __syncthreads();
+  v0 = sh[64];
+  v1 = sh[65];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restrict__ b,
+                                                  const double* bmean, T* __restrict__ xout,
+                                                  int singular, double tol, int maxit_cg,
+                                                  const SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;
+  extern __shared__ double sm[];
+  const int n = C.nx * C.ny * C.nz;
+  double* xs = sm;
+  double* rs = xs + n;
+  double* ps = rs + n;
+  double* zs = ps + n;  // z, then Ap
+  double* ds = zs + n;  // preconditioner diagonal
+  double* rh = ds + n;  // rhs
+  uint8_t* fl = reinterpret_cast<uint8_t*>(rh + n);
+  __shared__ double red[128];
+  const int tid = threadIdx.x;
+  auto lex_coords = [&](int m, int& i, int& j, int& k) {
+    i = m % C.nx;
+    j = (m / C.nx) % C.ny;
+    k = m / (C.nx * C.ny);
+  };
+  // Row of A at lexicographic cell m (fluid), on shared-memory vector v.
+  auto rowA = [&](int m, const double* v, double& diag, double& off) {
+    int i, j, k;
+    lex_coords(m, i, j, k);
+    diag = 0.0;
+    off = 0.0;
+    for (int axis = 0; axis < 3; ++axis) {
+      if (axis == 2 && C.twoD) continue;
+      const double h2 = C.h2[axis];
+      for (int side = -1; side <= 1; side += 2) {
+        int c[3] = {i, j, k};
+        const int dims[3] = {C.nx, C.ny, C.nz};
+        c[axis] += side;
+        int kind;
+        if (c[axis] < 0 || c[axis] >= dims[axis]) {
+          const int bt = C.bc[2 * axis + (side > 0 ? 1 : 0)];
+          if (bt == NB_BC_PERIODIC) {
+            c[axis] = (c[axis] + dims[axis]) % dims[axis];
+            kind = 1;
+          } else {
+            kind = (bt == NB_BC_OUTLET) ? 2 : 0;
+          }
+        } else {
+          kind = 1;
+        }
+        if (kind == 1) {
+          const int nn = c[0] + C.nx * (c[1] + C.ny * c[2]);
+          if (!fl[nn]) continue;  // solid neighbour: Neumann
+          diag += h2;
+          off += h2 * v[nn];
+        } else if (kind == 2) {
+          diag += 2.0 * h2;
+        }
+      }
+    }
+  };
+  // load
+  double bm = bmean ? *bmean : 0.0;
+  int nf_local = 0;
+  for (int m = tid; m < n; m += blockDim.x) {
+    int i, j, k;
+    lex_coords(m, i, j, k);
+    const int gidx = cell_index(C, i, j, k);
+    const bool f = C.type[gidx] == CELL_FLUID;
+    fl[m] = f;
+    nf_local += f;
+    rh[m] = f ? static_cast<double>(b[gidx]) - (bmean ? bm : 0.0) : 0.0;
+    xs[m] = 0.0;
+  }
+  __syncthreads();
+  for (int m = tid; m < n; m += blockDim.x) {
+    double d = 1.0;
+    if (fl[m]) {
+      double dg, off;
+      rowA(m, xs, dg, off);
+      d = dg > 0.0 ? dg : 1.0;
+    }
+    ds[m] = d;
+  }
+  const double nfluid = bsum_bcast(static_cast<double>(nf_local), red);
+  if (singular && nfluid > 0.0) {  // poisson.cpp:160-178
+    double s = 0.0;
+    for (int m = tid; m < n; m += blockDim.x)
+      if (fl[m]) s += rh[m];
+    const double mean = bsum_bcast(s, red) / nfluid;
+    for (int m = tid; m < n; m += blockDim.x) rh[m] = fl[m] ? rh[m] - mean : 0.0;
+    __syncthreads();
+  }
+  double rz_l = 0.0, bb_l = 0.0;
+  for (int m = tid; m < n; m += blockDim.x) {
+    rs[m] = rh[m];
+    zs[m] = rs[m] / ds[m];
+    ps[m] = zs[m];
+    rz_l += rs[m] * zs[m];
+    bb_l += rh[m] * rh[m];
+  }
+  bsum2_bcast(rz_l, bb_l, red);
+  double rz = rz_l;
+  const double bnorm = sqrt(bb_l) + 1e-300;
+  for (int it = 0; it < maxit_cg; ++it) {
+    double pap_l = 0.0;
+    for (int m = tid; m < n; m += blockDim.x) {
+      double ap;
+      if (!fl[m]) {
+        ap = ps[m];
+      } else {
+        double dg, off;
+        rowA(m, ps, dg, off);
+        ap = dg * ps[m] - off;
+      }
+      zs[m] = ap;
+      pap_l += ps[m] * ap;
+    }
+    const double pAp = bsum_bcast(pap_l, red);
+    if (fabs(pAp) < 1e-300) break;
+    const double alpha = rz / pAp;
+    double rr_l = 0.0;
+    for (int m = tid; m < n; m += blockDim.x) {
+      xs[m] += alpha * ps[m];
+      rs[m] -= alpha * zs[m];
+      rr_l += rs[m] * rs[m];
+    }
+    const double rnorm = sqrt(bsum_bcast(rr_l, red));
+    if (rnorm <= tol * bnorm) break;
+    double rzn_l = 0.0;
+    for (int m = tid; m < n; m += blockDim.x) {
+      zs[m] = rs[m] / ds[m];
+      rzn_l += rs[m] * zs[m];
+    }
+    const double rzNew = bsum_bcast(rzn_l, red);
+    const double beta = rzNew / rz;
+    for (int m = tid; m < n; m += blockDim.x) ps[m] = zs[m] + beta * ps[m];
+    rz = rzNew;
+    __syncthreads();
+  }
+  __syncthreads();
+  double mean = 0.0;
+  if (singular && nfluid > 0.0) {
+    double s = 0.0;
+    for (int m = tid; m < n; m += blockDim.x)
+      if (fl[m]) s += xs[m];
+    mean = bsum_bcast(s, red) / nfluid;
+  }
+  for (int m = tid; m < n; m += blockDim.x) {
+    int i, j, k;
+    lex_coords(m, i, j, k);
+    const double v = (singular && fl[m]) ? xs[m] - mean : xs[m];
+    xout[cell_index(C, i, j, k)] = static_cast<T>(v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PCG vector kernels on level 0 (FP64).
+// ---------------------------------------------------------------------------
+struct DFetch {
+  const double* x;
+  const double* xmean;
+  __device__ __forceinline__ double operator()(int n, int, int, int) const {
+    return xmean ? x[n] - *xmean : x[n];
+  }
+};
+
+// out = A x, identity rows on solid cells (poisson.cpp:102-134); void cells 0.
+__global__ void __launch_bounds__(NT) k_apply_a(LevelView L, const double* __restrict__ x,
+                                                double* __restrict__ out) {
+  DFetch X{x, nullptr};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const uint8_t ty = L.type[c];
+    double o = 0.0;
+    if (ty == CELL_SOLID) {
+      o = x[c];
+    } else if (ty == CELL_FLUID) {
+      int gi, gj, gk;
+      cell_coords(L, c, gi, gj, gk);
+      double diag, off;
+      stencil_row<double>(L, gi, gj, gk, X, diag, off);
+      o = diag * x[c] - off;
+    }
+    out[c] = o;
+  }
+}
+
+// Sum of b over fluid cells -> S[S_BSUM] = mean (singular rhs projection).
+__global__ void __launch_bounds__(NT) k_fluid_mean(LevelView L, const double* __restrict__ v,
+                                                   const double* vmean, RedBuf rb, double* mean_out,
+                                                   double inv_nfluid, const SolveFlags* flags,
+                                                   int maxit) {
+  if (stopped(flags, maxit)) return;
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    if (L.type[c] == CELL_FLUID) part[0] += vmean ? v[c] - *vmean : v[c];
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
+}
+
+// Float variant (mixed form: the V-cycle output z is FP32).
+__global__ void __launch_bounds__(NT) k_fluid_mean_f(LevelView L, const float* __restrict__ v,
+                                                     const double* vmean, RedBuf rb, double* mean_out,
+                                                     double inv_nfluid, const SolveFlags* flags,
+                                                     int maxit) {
+  if (stopped(flags, maxit)) return;
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    if (L.type[c] == CELL_FLUID) {
+      const double z = static_cast<double>(v[c]);
+      part[0] += vmean ? z - *vmean : z;
+    }
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
+}
+
+// rhs = fluid ? b - mean : 0 ; r = rhs ; S_BNORM2 = rhs.rhs ; early-exit test
+// (multigrid.cpp:279-298).
+__global__ void __launch_bounds__(NT) k_pcg_setup(LevelView L, const double* __restrict__ b,
+                                                  const double* bmean, double* __restrict__ rhs,
+                                                  double* __restrict__ r, double* __restrict__ x,
+                                                  float* __restrict__ r_f, RedBuf rb, double* S,
+                                                  SolveFlags* flags, double tol) {
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    double v = 0.0;
+    if (L.type[c] == CELL_FLUID) v = bmean ? b[c] - *bmean : b[c];
+    rhs[c] = v;
+    r[c] = v;
+    x[c] = 0.0;
+    if (r_f) r_f[c] = static_cast<float>(v);
+    part[0] += v * v;
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) {
+    S[S_BNORM2] = t[0];
+    const double bnorm = sqrt(t[0]) + 1e-300;
+    flags->iters = 0;
+    flags->nan = isnan(t[0]) ? 1 : 0;
+    if (sqrt(t[0]) <= tol * bnorm || isnan(t[0])) {
+      flags->stop = 1;
+      flags->early = 1;
+    } else {
+      flags->stop = 0;
+      flags->early = 0;
+    }
+  });
+}
+
+// z' = fluid ? (z - m1) - m2 : 0 (the smoother's last removeMean, then Minv's,
+// multigrid.cpp:283-288); written to zo (FP64). With `first`, p = z' and
+// S_RZ = r.z'; otherwise S_RNEWZ = z'.rnew, S_RZCROSS = z'.r and the finaliser
+// forms the flexible beta (multigrid.cpp:330-338).
+template <typename TZ>
+__global__ void __launch_bounds__(NT) k_pcg_dots(LevelView L, const TZ* __restrict__ z,
+                                                 const double* m1, const double* m2,
+                                                 double* __restrict__ zo, double* __restrict__ p,
+                                                 const double* __restrict__ rnew,
+                                                 const double* __restrict__ r, int first, RedBuf rb,
+                                                 double* S, SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;
+  double part[2] = {0.0, 0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    double v = 0.0;
+    if (L.type[c] == CELL_FLUID) {
+      v = static_cast<double>(z[c]);
+      if (m1) v = v - *m1;
+      if (m2) v = v - *m2;
+    }
+    zo[c] = v;
+    if (first) {
+      p[c] = v;
+      part[0] += r[c] * v;
+    } else {
+      part[0] += v * rnew[c];
+      part[1] += v * r[c];
+    }
+  }
+  grid_reduce<2>(part, rb, [=] __device__(const double* t) {
+    if (first) {
+      S[S_RZ] = t[0];
+    } else {
+      S[S_RNEWZ] = t[0];
+      S[S_RZCROSS] = t[1];
+      S[S_BETA] = (t[0] - t[1]) / S[S_RZ];
+      S[S_RZ] = t[0];
+      flags->iters += 1;
+    }
+  });
+}
+
+// p = z' + beta p (multigrid.cpp:335-337).
+__global__ void __launch_bounds__(NT) k_pcg_dir(LevelView L, const double* __restrict__ z,
+                                                double* __restrict__ p, const double* S,
+                                                const SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;
+  const double beta = S[S_BETA];
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    p[c] = z[c] + beta * p[c];
+  }
+}
+
+// Ap = A p ; S_PAP = p.Ap ; alpha = rz / pAp or breakdown (multigrid.cpp:303-308).
+__global__ void __launch_bounds__(NT) k_pcg_matvec(LevelView L, const double* __restrict__ p,
+                                                   double* __restrict__ Ap, RedBuf rb, double* S,
+                                                   SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;
+  DFetch X{p, nullptr};
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const uint8_t ty = L.type[c];
+    double o = 0.0;
+    if (ty == CELL_SOLID) {
+      o = p[c];
+    } else if (ty == CELL_FLUID) {
+      int gi, gj, gk;
+      cell_coords(L, c, gi, gj, gk);
+      double diag, off;
+      stencil_row<double>(L, gi, gj, gk, X, diag, off);
+      o = diag * p[c] - off;
+    }
+    Ap[c] = o;
+    part[0] += p[c] * o;
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) {
+    S[S_PAP] = t[0];
+    if (fabs(t[0]) < 1e-300 || isnan(t[0])) {
+      flags->stop = 2;
+      if (isnan(t[0])) flags->nan = 1;
+    } else {
+      S[S_ALPHA] = S[S_RZ] / t[0];
+    }
+  });
+}
+
+__device__ __forceinline__ void conv_check(double rnorm2, double* S, SolveFlags* flags, double tol) {
+  S[S_RNORM2] = rnorm2;
+  const double bnorm = sqrt(S[S_BNORM2]) + 1e-300;
+  if (isnan(rnorm2)) {
+    flags->nan = 1;
+    flags->stop = 2;
+  } else if (sqrt(rnorm2) <= tol * bnorm) {
+    flags->stop = 1;
+    flags->iters += 1;
+  }
+}
+
+// x += alpha p ; rnew = r - alpha Ap (multigrid.cpp:309-316). Non-singular:
+// reduces rnew.rnew and tests convergence; singular: reduces the fluid sum of
+// rnew for removeMean (then k_pcg_center finishes).
+__global__ void __launch_bounds__(NT) k_pcg_update(LevelView L, double* __restrict__ x,
+                                                   const double* __restrict__ p,
+                                                   const double* __restrict__ r,
+                                                   const double* __restrict__ Ap,
+                                                   double* __restrict__ rnew, float* __restrict__ rnew_f,
+                                                   int singular, double inv_nfluid, RedBuf rb,
+                                                   double* S, SolveFlags* flags, int maxit,
+                                                   double tol) {
+  if (stopped(flags, maxit)) return;
+  const double alpha = S[S_ALPHA];
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    x[c] += alpha * p[c];
+    const double rn = r[c] - alpha * Ap[c];
+    rnew[c] = rn;
+    if (singular) {
+      if (L.type[c] == CELL_FLUID) part[0] += rn;
+    } else {
+      part[0] += rn * rn;
+      if (rnew_f) rnew_f[c] = static_cast<float>(rn);
+    }
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) {
+    if (singular) S[S_RMEAN] = t[0] * inv_nfluid;
+    else conv_check(t[0], S, flags, tol);
+  });
+}
+
+// rnew = fluid ? rnew - mean : 0 ; rnew.rnew ; convergence (multigrid.cpp:317-325).
+__global__ void __launch_bounds__(NT) k_pcg_center(LevelView L, double* __restrict__ rnew,
+                                                   float* __restrict__ rnew_f, RedBuf rb, double* S,
+                                                   SolveFlags* flags, int maxit, double tol) {
+  if (stopped(flags, maxit)) return;
+  const double mean = S[S_RMEAN];
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const double v = L.type[c] == CELL_FLUID ? rnew[c] - mean : 0.0;
+    rnew[c] = v;
+    if (rnew_f) rnew_f[c] = static_cast<float>(v);
+    part[0] += v * v;
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) { conv_check(t[0], S, flags, tol); });
+}
+
+// Final removeMean(x) + true residual (multigrid.cpp:341-353):
+//   xf = fluid ? x - mean : x ; S_TRUERES2 = |rhs - A xf|^2
+__global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double* __restrict__ x,
+                                                      const double* xmean,
+                                                      const double* __restrict__ rhs,
+                                                      double* __restrict__ xf, RedBuf rb, double* S) {
+  DFetch X{x, xmean};
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const uint8_t ty = L.type[c];
+    double ax = 0.0, xv = x[c];
+    if (ty == CELL_FLUID) {
+      int gi, gj, gk;
+      cell_coords(L, c, gi, gj, gk);
+      double diag, off;
+      stencil_row<double>(L, gi, gj, gk, X, diag, off);
+      xv = X(c, gi, gj, gk);
+      ax = diag * xv - off;
+    } else if (ty == CELL_SOLID) {
+      ax = xv;
+    }
+    xf[c] = xv;
+    const double e = rhs[c] - ax;
+    part[0] += e * e;
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) { S[S_TRUERES2] = t[0]; });
+}
+
+}  // namespace
+
+// ===========================================================================
+// host driver
+// ===========================================================================
+void* MgSolver::alloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  const cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw ApiError{NB_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed"};
+  }
+  allocs_.push_back(p);
+  bytes_ += bytes;
+  return p;
+}
+
+MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
+    : precision_(precision), lc_(lc) {
+  std::vector<HostLevel> H = build_hierarchy(g);
+  singular_ = true;
+  for (int f = 0; f < 6; ++f)
+    if (g.face[f].type == NB_BC_OUTLET) singular_ = false;  // hasDirichlet, poisson.cpp:93-100
+  const HostLevel& last = H.back();
+  if (static_cast<size_t>(last.nx) * last.ny * last.nz > COARSE_MAX_CELLS)
+    throw ApiError{NB_ERR_UNSUPPORTED, "coarsest multigrid level exceeds 4096 cells"};
+  const size_t tsz = precision == NB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
+  lv_.resize(H.size());
+  for (size_t l = 0; l < H.size(); ++l) {
+    DevLevel& D = lv_[l];
+    D.h = std::move(H[l]);
+    const HostLevel& h = D.h;
+    const size_t ncs = static_cast<size_t>(h.nbrick) * BR3;
+    D.d_lut = static_cast<int*>(alloc(h.lut.size() * sizeof(int)));
+    D.d_bcoord = static_cast<int*>(alloc(h.bcoord.size() * sizeof(int)));
+    D.d_type = static_cast<uint8_t*>(alloc(ncs));
+    NB_CUDA(cudaMemcpy(D.d_lut, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice));
+    NB_CUDA(cudaMemcpy(D.d_bcoord, h.bcoord.data(), h.bcoord.size() * sizeof(int), cudaMemcpyHostToDevice));
+    NB_CUDA(cudaMemcpy(D.d_type, h.type.data(), ncs, cudaMemcpyHostToDevice));
+    D.b = alloc(ncs * tsz);
+    D.x0 = alloc(ncs * tsz);
+    D.x1 = alloc(ncs * tsz);
+    NB_CUDA(cudaMemset(D.b, 0, ncs * tsz));
+    NB_CUDA(cudaMemset(D.x0, 0, ncs * tsz));
+    NB_CUDA(cudaMemset(D.x1, 0, ncs * tsz));
+    LevelView& v = D.v;
+    v.nx = h.nx;
+    v.ny = h.ny;
+    v.nz = h.nz;
+    v.nbx = h.nbx;
+    v.nby = h.nby;
+    v.nbz = h.nbz;
+    v.nbrick = h.nbrick;
+    for (int f = 0; f < 6; ++f) v.bc[f] = g.face[f].type;
+    v.dxyz[0] = h.dx;
+    v.dxyz[1] = h.dy;
+    v.dxyz[2] = h.dz;
+    v.h2[0] = 1.0 / (h.dx * h.dx);
+    v.h2[1] = 1.0 / (h.dy * h.dy);
+    v.h2[2] = 1.0 / (h.dz * h.dz);
+    v.twoD = h.nz == 1;
+    v.lut = D.d_lut;
+    v.bcoord = D.d_bcoord;
+    v.type = D.d_type;
+  }
+  n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
+  double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
+  for (double** v : vecs) {
+    *v = static_cast<double*>(alloc(n0_ * sizeof(double)));
+    NB_CUDA(cudaMemset(*v, 0, n0_ * sizeof(double)));
+  }
+  if (precision_ == NB_PRECISION_MIXED) {
+    rnew_f_ = static_cast<float*>(alloc(n0_ * sizeof(float)));
+    NB_CUDA(cudaMemset(rnew_f_, 0, n0_ * sizeof(float)));
+  }
+  S_ = static_cast<double*>(alloc(S_COUNT * sizeof(double)));
+  NB_CUDA(cudaMemset(S_, 0, S_COUNT * sizeof(double)));
+  flags_ = static_cast<SolveFlags*>(alloc(sizeof(SolveFlags)));
+  NB_CUDA(cudaMemset(flags_, 0, sizeof(SolveFlags)));
+  rb_.max_blocks = MAX_GRID;
+  rb_.partials = static_cast<double*>(alloc(RED_KMAX * MAX_GRID * sizeof(double)));
+  rb_.counter = static_cast<unsigned*>(alloc(sizeof(unsigned)));
+  NB_CUDA(cudaMemset(rb_.counter, 0, sizeof(unsigned)));
+  NB_CUDA(cudaMallocHost(&h_flags_, sizeof(SolveFlags)));
+  NB_CUDA(cudaMallocHost(&h_S_, S_COUNT * sizeof(double)));
+  // The coarsest-level CTA keeps 6 FP64 vectors + flags in shared memory.
+  const int smem_max = COARSE_MAX_CELLS * static_cast<int>(6 * sizeof(double) + 1);
+  NB_CUDA(cudaFuncSetAttribute(k_coarse_cg<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+  NB_CUDA(cudaFuncSetAttribute(k_coarse_cg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+}
+
+MgSolver::~MgSolver() {
+  for (void* p : allocs_) cudaFree(p);
+  if (h_flags_) cudaFreeHost(h_flags_);
+  if (h_S_) cudaFreeHost(h_S_);
+}
+
+void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
+  const LevelView& L = lv_[0].v;
+  NB_LAUNCH(lc_, "apply_a", s, static_cast<double>(L.nx) * L.ny * L.nz * 17,
+            (k_apply_a<<<grid_for(L.nbrick), NT, 0, s>>>(L, x, out)));
+  NB_CUDA(cudaGetLastError());
+}
+
+// One V-cycle at level `lvl` on rhs b (pending mean slot bmean_slot or -1).
+// Returns the level's x buffer and the slot of its pending mean (-1 if none).
+template <typename T>
+void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, void* /*unused*/,
+                      int* out_mean_slot, void** out_x) {
+  DevLevel& D = lv_[lvl];
+  const LevelView& L = D.v;
+  const T* b = static_cast<const T*>(bv);
+  const double* bmean = (singular_ && bmean_slot >= 0) ? S_ + bmean_slot : nullptr;
+  const int grid = grid_for(L.nbrick);
+  const double tsz = sizeof(T);
+  const double ncell = static_cast<double>(L.nx) * L.ny * L.nz;
+  if (lvl + 1 == static_cast<int>(lv_.size())) {
+    const size_t smem = static_cast<size_t>(L.nx) * L.ny * L.nz * (6 * sizeof(double) + 1);
+    NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
+              (k_coarse_cg<T><<<1, NT, smem, s>>>(L, b, bmean, static_cast<T*>(D.x0), singular_ ? 1 : 0,
+                                                  1e-6, 500, flags_, maxit_)));
+    *out_x = D.x0;
+    *out_mean_slot = -1;
+    return;
+  }
+  const double inv_nf = D.h.nfluid ? 1.0 / static_cast<double>(D.h.nfluid) : 0.0;
+  const bool sing = singular_ && D.h.nfluid > 0;
+  T* xa = static_cast<T*>(D.x0);
+  T* xb = static_cast<T*>(D.x1);
+  double* mA = sing ? S_ + lvl_slot(lvl, 0) : nullptr;
+  double* mB = sing ? S_ + lvl_slot(lvl, 1) : nullptr;
+  const LevelView dummy = L;
+  DevLevel& Cd = lv_[lvl + 1];
+  const LevelView& C = Cd.v;
+  const double ncoarse = static_cast<double>(C.nx) * C.ny * C.nz;
+  // pre-smoothing (2 sweeps), first from x = 0
+  NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
+            (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean,
+                                             XFetch<T>{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1}, xa,
+                                             rb_, mA, inv_nf, flags_, maxit_)));
+  NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
+            (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
+                                             xb, rb_, mB, inv_nf, flags_, maxit_)));
+  // residual + restriction
+  const double inv_nfc = Cd.h.nfluid ? 1.0 / static_cast<double>(Cd.h.nfluid) : 0.0;
+  const int cb_slot = lvl_slot(lvl + 1, 2);
+  double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
+  NB_LAUNCH(lc_, "resid_restrict", s, ncell * (2 * tsz + 1) + ncoarse * tsz,
+            (k_resid_restrict<T><<<grid, NT, 0, s>>>(L, b, bmean,
+                                                     XFetch<T>{xb, mB, nullptr, nullptr, dummy, 1, 1, 1}, C,
+                                                     Cd.h.fx, Cd.h.fy, Cd.h.fz, static_cast<T*>(Cd.b), rb_,
+                                                     cmean, inv_nfc, flags_, maxit_)));
+  void* ec = nullptr;
+  int ec_slot = -1;
+  vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec);
+  const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
+  // post-smoothing: first sweep folds in the prolongation x += P e
+  NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
+            (k_smooth<T><<<grid, NT, 0, s>>>(
+                L, b, bmean,
+                XFetch<T>{xb, mB, static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy, Cd.h.fz}, xa, rb_,
+                mA, inv_nf, flags_, maxit_)));
+  NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
+            (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
+                                             xb, rb_, mB, inv_nf, flags_, maxit_)));
+  *out_x = xb;
+  *out_mean_slot = sing ? lvl_slot(lvl, 1) : -1;
+}
+
+// Minv: z = V-cycle(r) (+ Minv's removeMean), then either p = z, rz = r.z
+// (first) or the flexible-beta dots, then p = z + beta p.
+void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
+  const LevelView& L = lv_[0].v;
+  const int grid = grid_for(L.nbrick);
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / static_cast<double>(lv_[0].h.nfluid) : 0.0;
+  const bool sing = singular_ && lv_[0].h.nfluid > 0;
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  const double n = static_cast<double>(L.nx) * L.ny * L.nz;
+  const double zsz = mixed ? 4.0 : 8.0;
+  for (int k = 0; k < count; ++k) {
+    NB_LAUNCH(lc_, "pcg_matvec", s, n * 17,
+              (k_pcg_matvec<<<grid, NT, 0, s>>>(L, p_, Ap_, rb_, S_, flags_, maxit)));
+    NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0)),
+              (k_pcg_update<<<grid, NT, 0, s>>>(L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
+                                                sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol)));
+    if (sing) {
+      NB_LAUNCH(lc_, "pcg_center", s, n * (17 + (mixed ? 4 : 0)),
+                (k_pcg_center<<<grid, NT, 0, s>>>(L, rnew_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, maxit,
+                                                  tol)));
+    }
+    void* zx = nullptr;
+    int zslot = -1;
+    if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
+    else vcycle<double>(s, 0, rnew_, -1, nullptr, &zslot, &zx);
+    const double* m1 = (sing && zslot >= 0) ? S_ + zslot : nullptr;
+    const double* m2 = sing ? S_ + S_ZMEAN2 : nullptr;
+    if (sing) {
+      if (mixed)
+        NB_LAUNCH(lc_, "pcg_mean", s, n * (zsz + 1),
+                  (k_fluid_mean_f<<<grid, NT, 0, s>>>(L, static_cast<const float*>(zx), m1, rb_, S_ + S_ZMEAN2,
+                                                      inv_nf, flags_, maxit)));
+      else
+        NB_LAUNCH(lc_, "pcg_mean", s, n * (zsz + 1),
+                  (k_fluid_mean<<<grid, NT, 0, s>>>(L, static_cast<const double*>(zx), m1, rb_, S_ + S_ZMEAN2,
+                                                    inv_nf, flags_, maxit)));
+    }
+    if (mixed)
+      NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
+                (k_pcg_dots<float><<<grid, NT, 0, s>>>(L, static_cast<const float*>(zx), m1, m2, z_, p_, rnew_,
+                                                       r_, 0, rb_, S_, flags_, maxit)));
+    else
+      NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
+                (k_pcg_dots<double><<<grid, NT, 0, s>>>(L, static_cast<const double*>(zx), m1, m2, z_, p_,
+                                                        rnew_, r_, 0, rb_, S_, flags_, maxit)));
+    NB_LAUNCH(lc_, "pcg_dir", s, n * 24, (k_pcg_dir<<<grid, NT, 0, s>>>(L, z_, p_, S_, flags_, maxit)));
+    std::swap(r_, rnew_);
+  }
+  NB_CUDA(cudaGetLastError());
+}
+
+void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxit) {
+  tol_ = tol;
+  maxit_ = maxit;
+  const LevelView& L = lv_[0].v;
+  const int grid = grid_for(L.nbrick);
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / static_cast<double>(lv_[0].h.nfluid) : 0.0;
+  const bool sing = singular_ && lv_[0].h.nfluid > 0;
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  // rhs = b masked (+ mean removal), r = rhs, x = 0, bnorm, early exit
+  if (sing) {
+    k_fluid_mean<<<grid, NT, 0, s>>>(L, b, nullptr, rb_, S_ + S_BSUM, inv_nf, nullptr, maxit);
+    lc_.add();
+  }
+  k_pcg_setup<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, rhs_, r_, x_,
+                                  mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);
+  lc_.add();
+  // z = Minv(r) ; p = z ; rz = r.z
+  void* zx = nullptr;
+  int zslot = -1;
+  if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
+  else vcycle<double>(s, 0, r_, -1, nullptr, &zslot, &zx);
+  const double* m1 = (sing && zslot >= 0) ? S_ + zslot : nullptr;
+  const double* m2 = sing ? S_ + S_ZMEAN2 : nullptr;
+  if (sing) {
+    if (mixed)
+      k_fluid_mean_f<<<grid, NT, 0, s>>>(L, static_cast<const float*>(zx), m1, rb_, S_ + S_ZMEAN2, inv_nf,
+                                         flags_, maxit);
+    else
+      k_fluid_mean<<<grid, NT, 0, s>>>(L, static_cast<const double*>(zx), m1, rb_, S_ + S_ZMEAN2, inv_nf,
+                                       flags_, maxit);
+    lc_.add();
+  }
+  if (mixed)
+    k_pcg_dots<float><<<grid, NT, 0, s>>>(L, static_cast<const float*>(zx), m1, m2, z_, p_, r_, r_, 1, rb_,
+                                          S_, flags_, maxit);
+  else
+    k_pcg_dots<double><<<grid, NT, 0, s>>>(L, static_cast<const double*>(zx), m1, m2, z_, p_, r_, r_, 1,
+                                           rb_, S_, flags_, maxit);
+  lc_.add();
+  NB_CUDA(cudaGetLastError());
+  // Iterate in batches; every kernel returns at once after convergence, so
+  // over-issuing costs only launch latency. The batch grows geometrically.
+  int issued = 0, batch = 4;
+  while (issued < maxit) {
+    const int cnt = std::min(batch, maxit - issued);
+    iterate(s, tol, maxit, cnt);
+    issued += cnt;
+    NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaStreamSynchronize(s));
+    if (h_flags_->stop != 0 || h_flags_->iters >= maxit) break;
+    batch = std::min(batch * 2, 16);
+  }
+  // final removeMean(x) + true residual
+  if (sing) {
+    k_fluid_mean<<<grid, NT, 0, s>>>(L, x_, nullptr, rb_, S_ + S_XMEAN, inv_nf, nullptr, maxit);
+    lc_.add();
+  }
+  k_true_residual<<<grid, NT, 0, s>>>(L, x_, sing ? S_ + S_XMEAN : nullptr, rhs_, xfin_, rb_, S_);
+  lc_.add();
+  NB_CUDA(cudaGetLastError());
+}
+
+nb_poisson_report MgSolver::fetch_report(cudaStream_t s) {
+  NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
+  NB_CUDA(cudaMemcpyAsync(h_S_, S_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s));
+  NB_CUDA(cudaStreamSynchronize(s));
+  nb_poisson_report rep{};
+  const double bnorm = std::sqrt(h_S_[S_BNORM2]) + 1e-300;
+  if (h_flags_->early) {
+    rep.iterations = 0;
+    rep.residual = std::sqrt(h_S_[S_BNORM2]) / bnorm;
+    rep.converged = 1;
+    return rep;
+  }
+  rep.iterations = h_flags_->iters;
+  rep.residual = std::sqrt(h_S_[S_TRUERES2]) / bnorm;
+  rep.converged = (h_flags_->stop == 1 || rep.residual <= tol_) ? 1 : 0;
+  return rep;
+}
+
+void MgSolver::solve(cudaStream_t s, const double* b, double tol, int maxit) {
+  solve_async(s, b, tol, maxit);
+}
+
+template void MgSolver::vcycle<double>(cudaStream_t, int, const void*, int, void*, int*, void**);
+template void MgSolver::vcycle<float>(cudaStream_t, int, const void*, int, void*, int*, void**);
+
+}  // namespace nb

@@ -1,0 +1,91 @@
+// nb_mg.cuh — MG-PCG pressure solver on brick levels (host interface).
+//
+// Device restatement of MgPoisson (core/src/flow/multigrid.cpp:22-355) and its
+// coarsest-level CgPoisson (core/src/flow/poisson.cpp:136-252):
+//   * V(2,2) cycle, damped Jacobi (omega 0.8), restriction = average of fluid
+//     children, piecewise-constant prolongation, removeMean after every sweep
+//     on singular systems (applied lazily by the next kernel that reads the
+//     vector, so it costs no extra pass);
+//   * coarsest level: Jacobi-PCG to 1e-6 / 500 in one CTA (shared memory);
+//   * flexible (Polak-Ribiere) PCG outer loop, FP64 in both forms.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "nb_internal.h"
+
+namespace nb {
+
+struct DevLevel {
+  HostLevel h;
+  LevelView v{};
+  int* d_lut = nullptr;
+  int* d_bcoord = nullptr;
+  uint8_t* d_type = nullptr;
+  // V-cycle vectors in the level's arithmetic type (double or float):
+  // b (restricted residual), x ping, x pong.
+  void* b = nullptr;
+  void* x0 = nullptr;
+  void* x1 = nullptr;
+};
+
+class MgSolver {
+ public:
+  MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc);
+  ~MgSolver();
+  MgSolver(const MgSolver&) = delete;
+  MgSolver& operator=(const MgSolver&) = delete;
+
+  // Solve A x = b for device vector b (fluid rhs, brick layout). The solution
+  // (mean-removed when singular) is left in phi(). Reads back only the small
+  // report (one device->host copy of the flags + 3 scalars).
+  void solve(cudaStream_t s, const double* b_dev, double tol, int maxit);
+  // Same but leaves the report on the device (no host synchronisation);
+  // read it later with fetch_report().
+  void solve_async(cudaStream_t s, const double* b_dev, double tol, int maxit);
+  nb_poisson_report fetch_report(cudaStream_t s);
+
+  // out = A x (CgPoisson::applyA on level 0), brick layout.
+  void apply_a(cudaStream_t s, const double* x, double* out);
+
+  const double* phi() const { return xfin_; }
+  const LevelView& view0() const { return lv_[0].v; }
+  const HostLevel& host0() const { return lv_[0].h; }
+  bool singular() const { return singular_; }
+  uint64_t device_bytes() const { return bytes_; }
+  int levels() const { return static_cast<int>(lv_.size()); }
+  double* scalars() const { return S_; }
+  SolveFlags* flags() const { return flags_; }
+
+  // Scratch reduction buffer shared with the flow kernels of the same stream.
+  RedBuf red() const { return rb_; }
+
+ private:
+  template <typename T>
+  void vcycle(cudaStream_t s, int lvl, const void* b, int bmean_slot, void* xout_final,
+              int* out_mean_slot, void** out_x);
+  void iterate(cudaStream_t s, double tol, int maxit, int count);
+  void* alloc(size_t bytes);
+
+  std::vector<DevLevel> lv_;
+  bool singular_ = false;
+  int precision_ = NB_PRECISION_FP64;
+  double tol_ = 1e-9;
+  int maxit_ = 100;
+  size_t n0_ = 0;  // level-0 slots (nbrick * 512)
+  // level-0 PCG vectors (FP64)
+  double *rhs_ = nullptr, *x_ = nullptr, *r_ = nullptr, *rnew_ = nullptr, *z_ = nullptr,
+         *p_ = nullptr, *Ap_ = nullptr, *xfin_ = nullptr;
+  float* rnew_f_ = nullptr;  // mixed form: FP32 copy of the V-cycle input
+  float* z_f_ = nullptr;     // mixed form: FP32 V-cycle output
+  double* S_ = nullptr;
+  SolveFlags* flags_ = nullptr;
+  SolveFlags* h_flags_ = nullptr;  // pinned
+  double* h_S_ = nullptr;          // pinned
+  RedBuf rb_;
+  std::vector<void*> allocs_;
+  uint64_t bytes_ = 0;
+  LaunchCounter lc_;
+};
+
+}  // namespace nb

@@ -1,0 +1,180 @@
+"""Host-side mirror of the reference's solver seams over the C ABI.
+
+Same names, argument meaning and error behaviour as the reference:
+
+* ``MgPoisson(tol, max_cycles).solve(grid, b) -> (x, Report)`` —
+  ``nabla::flow::MgPoisson`` / ``PoissonSolver::solve``
+  (core/include/nabla/flow/poisson.hpp:20-33, :77-91).
+* ``apply_a(grid, x)`` — ``CgPoisson::applyA`` (core/src/flow/poisson.cpp:102-134).
+* ``NSSolver(grid, config)`` with ``initialize / step / set_state / u_face ...``
+  — ``nabla::flow::NSSolver`` (core/include/nabla/flow/ns_solver.hpp:58-156).
+
+Errors raise ``NablaError`` (the reference throws std::runtime_error); solver
+non-convergence is reported in ``Report.converged`` and is not an error.
+Every call runs on the CUDA library; nothing here computes the solution.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .cases import Grid
+
+
+class NablaError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+@dataclass
+class Report:
+    iterations: int
+    residual: float
+    converged: bool
+
+
+class Context:
+    """One CUDA device. ``Context(device)`` fails loudly without an sm_100 GPU."""
+
+    def __init__(self, device: int = 0):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        st = self.lib.nb_ctx_create(device, C.byref(h))
+        if st != abi.NB_OK:
+            raise NablaError(st, "nb_ctx_create failed: " + self.lib.nb_status_string(st).decode())
+        self.h = h
+
+    def check(self, st: int, what: str):
+        if st != abi.NB_OK:
+            raise NablaError(st, f"{what}: {self.lib.nb_last_error(self.h).decode()}")
+
+    @property
+    def launches(self) -> int:
+        return self.lib.nb_ctx_launch_count(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def apply_a(grid: Grid, x: np.ndarray, ctx: Context | None = None) -> np.ndarray:
+    ctx = ctx or default_context()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(grid.ncell)
+    ctx.check(ctx.lib.nb_apply_laplacian(ctx.h, C.byref(grid.desc()), abi.dptr(x), abi.dptr(out)),
+              "nb_apply_laplacian")
+    return out
+
+
+class MgPoisson:
+    """Geometric-multigrid-preconditioned flexible CG on the GPU."""
+
+    def __init__(self, tol: float = 1e-9, max_cycles: int = 100, precision: int = abi.PRECISION_FP64,
+                 ctx: Context | None = None):
+        self.tol, self.max_cycles, self.precision = tol, max_cycles, precision
+        self.ctx = ctx or default_context()
+
+    def name(self) -> str:
+        return "mg-pcg" if self.precision == abi.PRECISION_FP64 else "mg-pcg-mixed"
+
+    def solve(self, grid: Grid, b: np.ndarray):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(grid.ncell)
+        rep = abi.PoissonReport()
+        self.ctx.check(self.ctx.lib.nb_poisson_solve(self.ctx.h, C.byref(grid.desc()), abi.dptr(b),
+                                                     abi.dptr(x), self.tol, self.max_cycles,
+                                                     self.precision, C.byref(rep)),
+                       "nb_poisson_solve")
+        return x, Report(rep.iterations, rep.residual, bool(rep.converged))
+
+
+class NSSolver:
+    """Staggered SSP-RK3 / WENO-5 / MG-PCG step, state resident on the device."""
+
+    def __init__(self, grid: Grid, config: abi.FlowConfig, precision: int = abi.PRECISION_FP64,
+                 ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.grid, self.config = grid, config
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.nb_case_create(self.ctx.h, C.byref(grid.desc()), C.byref(config),
+                                                   precision, C.byref(h)), "nb_case_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.nb_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def initialize(self):
+        self.ctx.check(self.ctx.lib.nb_case_initialize(self.h), "initialize")
+
+    def set_state(self, u, v, w, p, step=0, t=0.0, dt_last=0.0):
+        nu, nv, nw, np_ = self.grid.sizes()
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, p)]
+        if [a.size for a in arrs] != [nu, nv, nw, np_]:
+            raise NablaError(abi.NB_ERR_BAD_ARG, "NSSolver::setState: size mismatch")
+        self.ctx.check(self.ctx.lib.nb_case_set_state(self.h, *[abi.dptr(a) for a in arrs], step, t,
+                                                      dt_last), "setState")
+
+    def get_state(self):
+        nu, nv, nw, np_ = self.grid.sizes()
+        u, v, w, p = np.zeros(nu), np.zeros(nv), np.zeros(nw), np.zeros(np_)
+        self.ctx.check(self.ctx.lib.nb_case_get_state(self.h, abi.dptr(u), abi.dptr(v), abi.dptr(w),
+                                                      abi.dptr(p)), "get_state")
+        return u, v, w, p
+
+    def u_face(self):
+        return self.get_state()[0]
+
+    def pressure(self):
+        return self.get_state()[3]
+
+    def clock(self):
+        st, t, dt = C.c_int(), C.c_double(), C.c_double()
+        self.ctx.check(self.ctx.lib.nb_case_get_clock(self.h, C.byref(st), C.byref(t), C.byref(dt)),
+                       "clock")
+        return st.value, t.value, dt.value
+
+    def compute_dt(self) -> float:
+        dt = C.c_double()
+        self.ctx.check(self.ctx.lib.nb_case_compute_dt(self.h, C.byref(dt)), "computeDt")
+        return dt.value
+
+    def step(self, dt: float = 0.0) -> abi.StepReport:
+        rep = abi.StepReport()
+        self.ctx.check(self.ctx.lib.nb_step(self.h, dt, C.byref(rep)), "step")
+        return rep
+
+    def step_many(self, dt: float, n: int) -> abi.StepReport:
+        rep = abi.StepReport()
+        self.ctx.check(self.ctx.lib.nb_step_many(self.h, dt, n, C.byref(rep)), "step_many")
+        return rep
+
+    @property
+    def device_bytes(self) -> int:
+        return self.ctx.lib.nb_case_device_bytes(self.h)
+
+    @property
+    def cell_count(self) -> int:
+        return self.ctx.lib.nb_case_cell_count(self.h)
