@@ -129,7 +129,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     # share of each kernel family (one profiled step per family, untimed)
     shares = {}
-    for fam in FAMILIES:
+    for fam in (FAMILIES if args.shares else ["smooth"]):
         ctx.lib.nb_ctx_profile(ctx.h, fam.encode())
         one_step()
         ms, nl, nb = C.c_double(), C.c_uint64(), C.c_double()
@@ -284,6 +284,8 @@ def main():
     ap.add_argument("--workload", default="tgv64")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--shares", type=int, default=1,
+                    help="1: time each kernel family once before the timed region")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
