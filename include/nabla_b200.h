@@ -164,6 +164,23 @@ nb_status nb_poisson_solve(nb_ctx* ctx, const nb_grid_desc* grid, const double* 
 /* Replaces CgPoisson::applyA (core/src/flow/poisson.cpp:102-134). */
 nb_status nb_apply_laplacian(nb_ctx* ctx, const nb_grid_desc* grid, const double* x, double* out);
 
+/* ---- allocation-free operator ---------------------------------------------
+ * No counterpart in the reference. The same -Laplacian as nb_apply_laplacian,
+ * for callers that cannot call cudaMalloc: code issuing work while a stream is
+ * captured into a CUDA graph, and hosts that own all device memory through
+ * their own arena or budget. `x` and `out` are the caller's DEVICE arrays of
+ * nx*ny*nz doubles in lexicographic order; `stream` is a cudaStream_t (NULL =
+ * legacy default stream) on the current device. No context is needed and
+ * nothing is allocated: the solid mask (grid->solid, host memory, or NULL) is
+ * staged into a static device array of NB_NOALLOC_MAX_CELLS bytes that every
+ * GPU loading this library holds until exit. Grids with more cells are
+ * rejected with NB_ERR_UNSUPPORTED. The first call on a device looks up that
+ * array's device address; make it before any stream capture. All calls share
+ * the array: calls that overlap on the GPU race and must be serialised. */
+#define NB_NOALLOC_MAX_CELLS (16u * 1024u * 1024u)
+nb_status nb_apply_laplacian_noalloc(const nb_grid_desc* grid, const double* x, double* out,
+                                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif

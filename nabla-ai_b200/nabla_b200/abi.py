@@ -138,6 +138,7 @@ PROTOTYPES = [
     ("nb_poisson_solve", C.c_int, [VP, C.POINTER(GridDesc), DP, DP, C.c_double, C.c_int, C.c_int,
                                    C.POINTER(PoissonReport)]),
     ("nb_apply_laplacian", C.c_int, [VP, C.POINTER(GridDesc), DP, DP]),
+    ("nb_apply_laplacian_noalloc", C.c_int, [C.POINTER(GridDesc), VP, VP, VP]),
 ]
 
 
