@@ -51,7 +51,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
         if verbose and out.strip():
             print(out)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
     return LIB
 
 

@@ -28,6 +28,21 @@ struct nb_ctx {
   size_t stage_bytes = 0;
 };
 
+// Results of one step, written by the step's kernels.
+struct StepBlock {
+  StepScalars sc;
+  double rep[3][6];  // per projection: MgSolver report
+  double dt;
+  unsigned long long execs;  // MG loop-body executions so far
+};
+
+struct GraphSlot {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t fixed_kernels = 0;
+  uint64_t body_kernels = 0;
+};
+
 struct nb_case {
   nb_ctx* ctx = nullptr;
   nb_grid_desc grid{};
@@ -50,8 +65,12 @@ struct nb_case {
   BcOp* bc_solid = nullptr;  // phase 2: zero faces touching a solid
   int n_out = 0, n_in = 0, n_solid = 0, serial_out = 0, serial_in = 0;
   RedBuf rb{};
-  StepScalars* d_sc = nullptr;
-  StepScalars* h_sc = nullptr;
+  StepBlock* d_blk = nullptr;  // per-step results (device)
+  StepBlock* h_blk = nullptr;  // pinned host copy
+  double* h_dt = nullptr;      // pinned dt staging
+  GraphSlot graphs[2][2];      // [state parity][cfl dt]
+  uint64_t body_kernels = 0;
+  unsigned long long last_execs = 0;
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   bool has_solid = false;
@@ -72,8 +91,14 @@ struct nb_case {
   }
   ~nb_case() {
     if (stream) cudaStreamSynchronize(stream);
+    for (auto& row : graphs)
+      for (GraphSlot& g : row) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+      }
     for (void* q : allocs) cudaFree(q);
-    if (h_sc) cudaFreeHost(h_sc);
+    if (h_blk) cudaFreeHost(h_blk);
+    if (h_dt) cudaFreeHost(h_dt);
     mg.reset();
     if (stream) cudaStreamDestroy(stream);
   }
@@ -277,64 +302,123 @@ void download_lex(nb_case& c, int comp, const double* src, double* host) {
 }
 
 // NSSolver::project (core/src/flow/ns_solver.cpp:475-579) on the current fields.
-nb_poisson_report project(nb_case& c, double* const* f, double dt) {
+// Graph form: the MG-PCG cycle loop is a device-side conditional node.
+void project(nb_case& c, double* const* f, int stage, bool direct) {
+  StepBlock* blk = c.d_blk;
   apply_bc(c, f, true);
   flow_launch(c, "div", ncell_of(c) * 33, [&] { launch_div(c.stream, c.F, f[0], f[1], f[2], c.b); });
-  c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters);
+  if (direct) {
+    c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage]);
+  } else {
+    uint64_t nbody = 0;
+    c.mg->capture_solve(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage],
+                        &nbody);
+    c.body_kernels = nbody;
+  }
   flow_launch(c, "correct", ncell_of(c) * 65,
-              [&] { launch_correct(c.stream, c.F, c.mg->phi(), dt, f[0], f[1], f[2], c.p); });
+              [&] { launch_correct(c.stream, c.F, c.mg->phi(), &blk->dt, f[0], f[1], f[2], c.p); });
   apply_bc(c, f, false);
-  return c.mg->fetch_report(c.stream);
+}
+
+double visc_of(const nb_case& c) {
+  const nb_grid_desc& g = c.grid;
+  const bool twoD = g.nz == 1;
+  return 2.0 * c.nu * (1.0 / (g.dx * g.dx) + 1.0 / (g.dy * g.dy) + (twoD ? 0.0 : 1.0 / (g.dz * g.dz)));
 }
 
 double compute_dt(nb_case& c) {
   double* const* f = c.uvw[c.cur];
-  const nb_grid_desc& g = c.grid;
-  const bool twoD = g.nz == 1;
-  const double visc = 2.0 * c.nu *
-                      (1.0 / (g.dx * g.dx) + 1.0 / (g.dy * g.dy) + (twoD ? 0.0 : 1.0 / (g.dz * g.dz)));
-  launch_max_inv(c.stream, c.F, f[0], f[1], f[2], visc, c.rb, c.d_sc);
-  c.ctx->launches++;
-  NB_CUDA(cudaMemcpyAsync(c.h_sc, c.d_sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, c.stream));
+  flow_launch(c, "max_inv", ncell_of(c) * 25, [&] {
+    launch_max_inv(c.stream, c.F, f[0], f[1], f[2], visc_of(c), c.cfg.cfl, nullptr, c.rb, &c.d_blk->sc);
+  });
+  NB_CUDA(cudaMemcpyAsync(c.h_blk, c.d_blk, sizeof(StepBlock), cudaMemcpyDeviceToHost, c.stream));
   NB_CUDA(cudaStreamSynchronize(c.stream));
-  return c.cfg.cfl / c.h_sc->maxinv;
+  return c.cfg.cfl / c.h_blk->sc.maxinv;
 }
 
-// NSSolver::step(double) (core/src/flow/ns_solver.cpp:767-824).
-void do_step(nb_case& c, double dt, nb_step_report* rep) {
-  if (dt <= 0.0) dt = compute_dt(c);
-  const size_t fb[3] = {static_cast<size_t>(store_size(c.F, 0)) * 8, static_cast<size_t>(store_size(c.F, 1)) * 8,
-                        static_cast<size_t>(store_size(c.F, 2)) * 8};
-  double** A = c.uvw[c.cur];
-  double** B = c.uvw[1 - c.cur];
+// Issues one SSP-RK3 step (NSSolver::step, core/src/flow/ns_solver.cpp:765-824)
+// starting from state parity `cur`. cfl_dt: dt = computeDt() on the device.
+void issue_step(nb_case& c, int cur, bool cfl_dt, bool direct) {
+  StepBlock* blk = c.d_blk;
+  double** A = c.uvw[cur];
+  double** B = c.uvw[1 - cur];
+  if (cfl_dt)
+    flow_launch(c, "max_inv", ncell_of(c) * 25, [&] {
+      launch_max_inv(c.stream, c.F, A[0], A[1], A[2], visc_of(c), c.cfg.cfl, &blk->dt, c.rb, &blk->sc);
+    });
   for (int q = 0; q < 3; ++q)
-    NB_CUDA(cudaMemcpyAsync(c.uvw0[q], A[q], fb[q], cudaMemcpyDeviceToDevice, c.stream));
+    NB_CUDA(cudaMemcpyAsync(c.uvw0[q], A[q], static_cast<size_t>(store_size(c.F, q)) * 8,
+                            cudaMemcpyDeviceToDevice, c.stream));
   apply_bc(c, A, true);
-  nb_poisson_report pr[3];
   const int mixed = c.precision == NB_PRECISION_MIXED;
   for (int stage = 1; stage <= 3; ++stage) {
     double** in = (stage == 2) ? B : A;
     double** out = (stage == 2) ? A : B;
     flow_launch(c, "rhs_rk", ncell_of(c) * 73, [&] {
-      launch_rhs_rk(c.stream, c.F, stage, dt, in[0], in[1], in[2], c.uvw0[0], c.uvw0[1], c.uvw0[2],
+      launch_rhs_rk(c.stream, c.F, stage, &blk->dt, in[0], in[1], in[2], c.uvw0[0], c.uvw0[1], c.uvw0[2],
                     out[0], out[1], out[2], mixed);
     });
-    pr[stage - 1] = project(c, out, dt);
+    project(c, out, stage - 1, direct);
   }
-  c.cur = 1 - c.cur;  // the stage-3 output (B) is the new state
-  double** S = c.uvw[c.cur];
   flow_launch(c, "diag", ncell_of(c) * 57, [&] {
-    launch_diag(c.stream, c.F, S[0], S[1], S[2], c.uvw0[0], c.uvw0[1], c.uvw0[2], c.p, c.rb, c.d_sc);
+    launch_diag(c.stream, c.F, B[0], B[1], B[2], c.uvw0[0], c.uvw0[1], c.uvw0[2], c.p, c.rb, &blk->sc);
   });
-  NB_CUDA(cudaMemcpyAsync(c.h_sc, c.d_sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, c.stream));
+  NB_CUDA(cudaMemcpyAsync(&blk->execs, c.mg->body_execs(), sizeof(unsigned long long),
+                          cudaMemcpyDeviceToDevice, c.stream));
+}
+
+// One step. Without profiling the step runs as one CUDA graph (built on first
+// use per state parity and dt mode): one launch and one small read-back per step.
+void do_step(nb_case& c, double dt, nb_step_report* rep) {
+  const bool cfl_dt = dt <= 0.0;
+  if (!cfl_dt) {
+    c.h_dt[0] = dt;
+    NB_CUDA(cudaMemcpyAsync(&c.d_blk->dt, c.h_dt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  }
+  const bool direct = !c.ctx->prof.family.empty();
+  if (direct) {
+    issue_step(c, c.cur, cfl_dt, true);
+  } else {
+    GraphSlot& gs = c.graphs[c.cur][cfl_dt ? 1 : 0];
+    if (!gs.exec) {
+      const uint64_t before = c.ctx->launches;
+      NB_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        issue_step(c, c.cur, cfl_dt, false);
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        c.ctx->launches = before;
+        throw;
+      }
+      NB_CUDA(cudaStreamEndCapture(c.stream, &gs.graph));
+      NB_CUDA(cudaGraphInstantiate(&gs.exec, gs.graph, 0));
+      gs.fixed_kernels = c.ctx->launches - before;
+      gs.body_kernels = c.body_kernels;
+      c.ctx->launches = before;
+    }
+    NB_CUDA(cudaGraphLaunch(gs.exec, c.stream));
+  }
+  NB_CUDA(cudaMemcpyAsync(c.h_blk, c.d_blk, sizeof(StepBlock), cudaMemcpyDeviceToHost, c.stream));
   NB_CUDA(cudaStreamSynchronize(c.stream));
+  const StepBlock& hb = *c.h_blk;
+  if (!direct) {
+    const GraphSlot& gs = c.graphs[c.cur][cfl_dt ? 1 : 0];
+    c.ctx->launches += gs.fixed_kernels + (hb.execs - c.last_execs) * gs.body_kernels;
+  }
+  c.last_execs = hb.execs;
+  dt = hb.dt;
+  c.cur = 1 - c.cur;  // the stage-3 output is the new state
   c.step += 1;
   c.t += dt;
   c.dt_last = dt;
   if (!rep) return;
+  nb_poisson_report pr[3];
+  for (int s = 0; s < 3; ++s) pr[s] = MgSolver::report_from(hb.rep[s], c.cfg.poisson_tol);
   const nb_grid_desc& g = c.grid;
   const double nfaces = static_cast<double>(lex_size(c.F, 0) + lex_size(c.F, 1) + lex_size(c.F, 2));
-  const StepScalars& sc = *c.h_sc;
+  const StepScalars& sc = hb.sc;
   std::memset(rep, 0, sizeof(*rep));
   rep->step = c.step;
   rep->t = c.t;
@@ -532,8 +616,10 @@ nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_co
     c->rb.partials = static_cast<double*>(c->alloc(RED_KMAX * c->rb.max_blocks * sizeof(double)));
     c->rb.counter = static_cast<unsigned*>(c->alloc(sizeof(unsigned)));
     NB_CUDA(cudaMemset(c->rb.counter, 0, sizeof(unsigned)));
-    c->d_sc = static_cast<StepScalars*>(c->alloc(sizeof(StepScalars)));
-    NB_CUDA(cudaMallocHost(&c->h_sc, sizeof(StepScalars)));
+    c->d_blk = static_cast<StepBlock*>(c->alloc(sizeof(StepBlock)));
+    NB_CUDA(cudaMemset(c->d_blk, 0, sizeof(StepBlock)));
+    NB_CUDA(cudaMallocHost(&c->h_blk, sizeof(StepBlock)));
+    NB_CUDA(cudaMallocHost(&c->h_dt, sizeof(double)));
     NB_CUDA(cudaDeviceSynchronize());
     return NB_OK;
   });

@@ -61,6 +61,41 @@ void build_level(HostLevel& L, int nx, int ny, int nz, double dx, double dy, dou
       }
 }
 
+void build_codes(HostLevel& L, const int bc[6]) {
+  L.code.assign(L.type.size(), static_cast<uint16_t>(CELL_VOID << CODE_TYPE));
+  const int dims[3] = {L.nx, L.ny, L.nz};
+  auto lex = [&](int i, int j, int k) {
+    return static_cast<size_t>(i) + static_cast<size_t>(L.nx) * (j + static_cast<size_t>(L.ny) * k);
+  };
+  for (int k = 0; k < L.nz; ++k)
+    for (int j = 0; j < L.ny; ++j)
+      for (int i = 0; i < L.nx; ++i) {
+        const int b = L.lut[((k / BR) * L.nby + j / BR) * L.nbx + i / BR];
+        const size_t idx = static_cast<size_t>(b) * BR3 + ((k & 7) << 6) + ((j & 7) << 3) + (i & 7);
+        const bool solid = L.solid[lex(i, j, k)] != 0;
+        uint16_t code = static_cast<uint16_t>((solid ? CELL_SOLID : CELL_FLUID) << CODE_TYPE);
+        for (int axis = 0; axis < 3 && !solid; ++axis) {
+          if (axis == 2 && L.nz == 1) continue;  // 2-D: no z coupling
+          for (int side = 0; side < 2; ++side) {
+            int c[3] = {i, j, k};
+            c[axis] += side ? 1 : -1;
+            const int f = 2 * axis + side;
+            if (c[axis] < 0 || c[axis] >= dims[axis]) {
+              const int bt = bc[f];
+              if (bt == NB_BC_OUTLET) {
+                code |= static_cast<uint16_t>(1u << (CODE_DIRICHLET + f));
+                continue;
+              }
+              if (bt != NB_BC_PERIODIC) continue;  // wall / inlet: Neumann
+              c[axis] = (c[axis] + dims[axis]) % dims[axis];
+            }
+            if (!L.solid[lex(c[0], c[1], c[2])]) code |= static_cast<uint16_t>(1u << f);
+          }
+        }
+        L.code[idx] = code;
+      }
+}
+
 // MgPoisson hierarchy construction (core/src/flow/multigrid.cpp:211-266):
 // halve an axis only if its length is >= 4, stop at <= 2048 cells or 8 levels;
 // a coarse cell is fluid if any child is fluid.

@@ -226,7 +226,7 @@ __device__ __forceinline__ int tix(int a, int b, int c) { return ((c + 3) * TW +
 // (domain-boundary faces, faces touching a solid) get R = 0.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(RHS_NT) k_rhs_rk(FlowView F, int stage, double dt,
+__global__ void __launch_bounds__(RHS_NT) k_rhs_rk(FlowView F, int stage, const double* __restrict__ dtp,
                                                    const double* __restrict__ u,
                                                    const double* __restrict__ v,
                                                    const double* __restrict__ w,
@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(RHS_NT) k_rhs_rk(FlowView F, int stage, double
   const T nu = T(F.nu);
   const T h = T(0.5);
   const double c1 = 1.0 / 3.0, c2 = 2.0 / 3.0;
+  const double dt = *dtp;
   auto comb = [&](double a0, double a, double r) -> double {
     if (stage == 1) return a0 + dt * r;
     if (stage == 2) return 0.75 * a0 + 0.25 * (a + dt * r);
@@ -466,11 +467,13 @@ __device__ __forceinline__ double phi_at(const FlowView& F, const double* __rest
 
 // u -= d(phi)/dn on every face not touching a solid, incl. boundary faces
 // (ns_solver.cpp:528-562); p = phi / dt (ns_solver.cpp:575-578).
-__global__ void __launch_bounds__(NT) k_correct(FlowView F, const double* __restrict__ phi, double dt,
+__global__ void __launch_bounds__(NT) k_correct(FlowView F, const double* __restrict__ phi,
+                                                const double* __restrict__ dtp,
                                                 double* __restrict__ u, double* __restrict__ v,
                                                 double* __restrict__ w, double* __restrict__ p) {
   const LevelView& L = F.L;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const double dt = *dtp;
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
     const int c = brick * BR3 + threadIdx.x;
     const uint8_t ty = L.type[c];
@@ -581,7 +584,8 @@ __global__ void __launch_bounds__(NT) k_diag(FlowView F, const double* __restric
 // computeDt reduction (ns_solver.cpp:581-603).
 __global__ void __launch_bounds__(NT) k_max_inv(FlowView F, const double* __restrict__ u,
                                                 const double* __restrict__ v,
-                                                const double* __restrict__ w, double visc, RedBuf rb,
+                                                const double* __restrict__ w, double visc, double cfl,
+                                                double* dt_out, RedBuf rb,
                                                 StepScalars* out) {
   const LevelView& L = F.L;
   const int twoD = L.twoD;
@@ -597,7 +601,10 @@ __global__ void __launch_bounds__(NT) k_max_inv(FlowView F, const double* __rest
     const double inv = uc / L.dxyz[0] + vc / L.dxyz[1] + (twoD ? 0.0 : wc / L.dxyz[2]) + visc;
     m[0] = fmax(m[0], inv);
   }
-  grid_reduce<1, 1u>(m, rb, [=] __device__(const double* t) { out->maxinv = t[0]; });
+  grid_reduce<1, 1u>(m, rb, [=] __device__(const double* t) {
+    out->maxinv = t[0];
+    if (dt_out) *dt_out = cfl / t[0];  // ns_solver.cpp:602
+  });
 }
 
 // lexicographic <-> brick conversion (one thread per lexicographic element)
@@ -656,15 +663,15 @@ void launch_bc(cudaStream_t s, const BcOp* ops, int n, int serial, double* u, do
   NB_CUDA(cudaGetLastError());
 }
 
-void launch_rhs_rk(cudaStream_t s, const FlowView& F, int stage, double dt, const double* u,
+void launch_rhs_rk(cudaStream_t s, const FlowView& F, int stage, const double* dtp, const double* u,
                    const double* v, const double* w, const double* u0, const double* v0,
                    const double* w0, double* uo, double* vo, double* wo, int mixed) {
   const int grid = std::min(F.L.nbrick, 148 * 2);
   if (mixed)
-    k_rhs_rk<float><<<grid, RHS_NT, 3 * TN * sizeof(float), s>>>(F, stage, dt, u, v, w, u0, v0, w0, uo,
+    k_rhs_rk<float><<<grid, RHS_NT, 3 * TN * sizeof(float), s>>>(F, stage, dtp, u, v, w, u0, v0, w0, uo,
                                                                  vo, wo);
   else
-    k_rhs_rk<double><<<grid, RHS_NT, 3 * TN * sizeof(double), s>>>(F, stage, dt, u, v, w, u0, v0, w0,
+    k_rhs_rk<double><<<grid, RHS_NT, 3 * TN * sizeof(double), s>>>(F, stage, dtp, u, v, w, u0, v0, w0,
                                                                    uo, vo, wo);
   NB_CUDA(cudaGetLastError());
 }
@@ -675,9 +682,9 @@ void launch_div(cudaStream_t s, const FlowView& F, const double* u, const double
   NB_CUDA(cudaGetLastError());
 }
 
-void launch_correct(cudaStream_t s, const FlowView& F, const double* phi, double dt, double* u,
+void launch_correct(cudaStream_t s, const FlowView& F, const double* phi, const double* dtp, double* u,
                     double* v, double* w, double* p) {
-  k_correct<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, phi, dt, u, v, w, p);
+  k_correct<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, phi, dtp, u, v, w, p);
   NB_CUDA(cudaGetLastError());
 }
 
@@ -689,8 +696,9 @@ void launch_diag(cudaStream_t s, const FlowView& F, const double* u, const doubl
 }
 
 void launch_max_inv(cudaStream_t s, const FlowView& F, const double* u, const double* v,
-                    const double* w, double visc, RedBuf rb, StepScalars* out) {
-  k_max_inv<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, visc, rb, out);
+                    const double* w, double visc, double cfl, double* dt_out, RedBuf rb,
+                    StepScalars* out) {
+  k_max_inv<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, visc, cfl, dt_out, rb, out);
   NB_CUDA(cudaGetLastError());
 }
 

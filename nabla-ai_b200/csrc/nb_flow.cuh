@@ -36,18 +36,19 @@ struct StepScalars {  // per-step diagnostics (device), ns_solver.cpp:797-823
 
 // host wrappers (nb_flow.cu)
 void launch_bc(cudaStream_t s, const BcOp* ops, int n, int serial, double* u, double* v, double* w);
-void launch_rhs_rk(cudaStream_t s, const FlowView& F, int stage, double dt, const double* u,
+void launch_rhs_rk(cudaStream_t s, const FlowView& F, int stage, const double* dtp, const double* u,
                    const double* v, const double* w, const double* u0, const double* v0,
                    const double* w0, double* uo, double* vo, double* wo, int mixed);
 void launch_div(cudaStream_t s, const FlowView& F, const double* u, const double* v, const double* w,
                 double* b);
-void launch_correct(cudaStream_t s, const FlowView& F, const double* phi, double dt, double* u,
+void launch_correct(cudaStream_t s, const FlowView& F, const double* phi, const double* dtp, double* u,
                     double* v, double* w, double* p);
 void launch_diag(cudaStream_t s, const FlowView& F, const double* u, const double* v,
                  const double* w, const double* u0, const double* v0, const double* w0,
                  const double* p, RedBuf rb, StepScalars* out);
 void launch_max_inv(cudaStream_t s, const FlowView& F, const double* u, const double* v,
-                    const double* w, double visc, RedBuf rb, StepScalars* out);
+                    const double* w, double visc, double cfl, double* dt_out, RedBuf rb,
+                    StepScalars* out);
 // Layout conversion between the reference's lexicographic arrays and bricks.
 // comp: 0 u, 1 v, 2 w, 3 cell. dir 0: lex -> brick, 1: brick -> lex.
 void launch_convert(cudaStream_t s, const FlowView& F, int comp, int dir, const double* src,

@@ -41,7 +41,13 @@ struct LevelView {
   const int* lut;     // [nbz][nby][nbx] -> brick rank
   const int* bcoord;  // [nbrick][3] brick coordinates
   const uint8_t* type;  // [nbrick*512] CELL_*
+  // Per-cell stencil code (built on the host from the BCs and solids):
+  // bit f (f = 2*axis + side, side 0 low / 1 high): face f couples to a fluid
+  // neighbour; bit 6+f: face f is a Dirichlet outlet face; bits 12-13: CELL_*.
+  const uint16_t* code;
 };
+constexpr int CODE_DIRICHLET = 6;
+constexpr int CODE_TYPE = 12;
 
 __host__ __device__ inline int wrapi(int a, int n) { return (a % n + n) % n; }
 
@@ -131,9 +137,14 @@ struct HostLevel {
   double dx, dy, dz;
   std::vector<int> lut, bcoord;
   std::vector<uint8_t> type;   // brick layout
+  std::vector<uint16_t> code;  // brick layout, see LevelView::code
   std::vector<uint8_t> solid;  // lexicographic (for hierarchy construction)
   uint64_t nfluid = 0;
 };
+
+// Fills L.code from the cell types and the domain BCs (the face resolution of
+// core/src/flow/poisson.cpp:18-52, precomputed once per level).
+void build_codes(HostLevel& L, const int bc[6]);
 
 // Builds the brick layout of an nx*ny*nz grid with the given lexicographic
 // solid mask (NULL = none).

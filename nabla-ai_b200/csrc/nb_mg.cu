@@ -87,6 +87,67 @@ __device__ __forceinline__ void stencil_row(const LevelView& L, int gi, int gj, 
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory halo staging. A CTA works on one brick at a time: it stages
+// the brick's 8^3 values plus the one-cell face halo from the six neighbour
+// bricks (10^3 positions minus edges and corners, which a 7-point stencil
+// never reads), applying the vector's pending operations on the way in, then
+// every cell evaluates its row from shared memory with its precomputed code.
+// ---------------------------------------------------------------------------
+constexpr int TS = 10;
+constexpr int TSN = TS * TS * TS;
+
+__device__ __forceinline__ int tpos(int i, int j, int k) { return ((k + 1) * TS + (j + 1)) * TS + (i + 1); }
+__device__ __forceinline__ int tpos_local(int l) { return tpos(l & 7, (l >> 3) & 7, l >> 6); }
+__device__ __forceinline__ int code_type(uint32_t code) { return (code >> CODE_TYPE) & 3; }
+
+template <typename T, class F>
+__device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile, const F& fx) {
+  const int ox = L.bcoord[3 * brick] * BR, oy = L.bcoord[3 * brick + 1] * BR,
+            oz = L.bcoord[3 * brick + 2] * BR;
+  const int dims[3] = {L.nx, L.ny, L.nz};
+  for (int p = threadIdx.x; p < TSN; p += blockDim.x) {
+    const int ti = p % TS - 1, tj = (p / TS) % TS - 1, tk = p / (TS * TS) - 1;
+    const int outc = (ti < 0 || ti > 7) + (tj < 0 || tj > 7) + (tk < 0 || tk > 7);
+    if (outc > 1) continue;
+    int g[3] = {ox + ti, oy + tj, oz + tk};
+    T v = T(0);
+    if (outc == 0 && g[0] < dims[0] && g[1] < dims[1] && g[2] < dims[2]) {
+      v = fx(brick * BR3 + ((tk << 6) | (tj << 3) | ti), g[0], g[1], g[2]);
+    } else {
+      bool ok = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (g[a] < 0 || g[a] >= dims[a]) {
+          if (L.bc[2 * a] == NB_BC_PERIODIC) g[a] = wrapi(g[a], dims[a]);
+          else ok = false;
+        }
+      if (ok) v = fx(cell_index(L, g[0], g[1], g[2]), g[0], g[1], g[2]);
+    }
+    tile[p] = v;
+  }
+}
+
+// Row of the -Laplacian from the staged tile: diag = sum of face coefficients,
+// off = sum coeff * neighbour, faces in the reference's order (poisson.cpp:114-129).
+template <typename T>
+__device__ __forceinline__ void row_from_tile(const LevelView& L, uint32_t code, const T* tile, int ctr,
+                                              T& diag, T& off) {
+  diag = T(0);
+  off = T(0);
+  const int step[6] = {-1, 1, -TS, TS, -TS * TS, TS * TS};
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const T h2 = static_cast<T>(L.h2[f >> 1]);
+    if (code & (1u << f)) {
+      diag += h2;
+      off += h2 * tile[ctr + step[f]];
+    } else if (code & (1u << (CODE_DIRICHLET + f))) {
+      diag += T(2) * h2;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Damped-Jacobi sweep (multigrid.cpp:102-114), one sweep per launch.
 //   xout = fluid ? x' + omega (b' - A x') / D : 0
 // where x' / b' include pending mean / prolongation. Optionally reduces the
@@ -98,17 +159,31 @@ __global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict_
                                                RedBuf rb, double* mean_out, double inv_nfluid,
                                                const SolveFlags* flags, int maxit) {
   if (stopped(flags, maxit)) return;
+  __shared__ T tile[TSN];
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    if (X.x || X.ec) fill_halo<T>(L, brick, tile, X);
+    __syncthreads();
     const int c = brick * BR3 + threadIdx.x;
-    const uint8_t ty = L.type[c];
+    const uint32_t code = L.code[c];
     T out = T(0);
-    if (ty == CELL_FLUID) {
-      int gi, gj, gk;
-      cell_coords(L, c, gi, gj, gk);
-      T diag, off;
-      stencil_row<T>(L, gi, gj, gk, X, diag, off);
-      const T xc = X(c, gi, gj, gk);
+    if (code_type(code) == CELL_FLUID) {
+      const int ctr = tpos_local(threadIdx.x);
+      T diag, off, xc;
+      if (X.x || X.ec) {
+        row_from_tile<T>(L, code, tile, ctr, diag, off);
+        xc = tile[ctr];
+      } else {  // first sweep from x = 0: A x = 0
+        diag = T(0);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+          const T h2 = static_cast<T>(L.h2[f >> 1]);
+          if (code & (1u << f)) diag += h2;
+          else if (code & (1u << (CODE_DIRICHLET + f))) diag += T(2) * h2;
+        }
+        off = T(0);
+        xc = T(0);
+      }
       T bc = b[c];
       if (bmean) bc = bc - static_cast<T>(*bmean);
       const T Ax = diag * xc - off;
@@ -117,6 +192,7 @@ __global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict_
       part[0] += static_cast<double>(out);
     }
     xout[c] = out;
+    __syncthreads();
   }
   if (mean_out) {
     grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
@@ -136,25 +212,28 @@ __global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __r
                                                        RedBuf rb, double* mean_out, double inv_nfluid_c,
                                                        const SolveFlags* flags, int maxit) {
   if (stopped(flags, maxit)) return;
+  __shared__ T tile[TSN];
   __shared__ T rs[BR3];
   __shared__ uint8_t fl[BR3];
   double part[1] = {0.0};
   const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
   for (int brick = blockIdx.x; brick < F.nbrick; brick += gridDim.x) {
+    fill_halo<T>(F, brick, tile, X);
+    __syncthreads();
     const int c = brick * BR3 + threadIdx.x;
-    const uint8_t ty = F.type[c];
+    const uint32_t code = F.code[c];
+    const bool fluid = code_type(code) == CELL_FLUID;
     T r = T(0);
-    if (ty == CELL_FLUID) {
-      int gi, gj, gk;
-      cell_coords(F, c, gi, gj, gk);
+    if (fluid) {
+      const int ctr = tpos_local(threadIdx.x);
       T diag, off;
-      stencil_row<T>(F, gi, gj, gk, X, diag, off);
+      row_from_tile<T>(F, code, tile, ctr, diag, off);
       T bc = b[c];
       if (bmean) bc = bc - static_cast<T>(*bmean);
-      r = bc - (diag * X(c, gi, gj, gk) - off);
+      r = bc - (diag * tile[ctr] - off);
     }
     rs[threadIdx.x] = r;
-    fl[threadIdx.x] = (ty == CELL_FLUID);
+    fl[threadIdx.x] = fluid;
     __syncthreads();
     const int t = threadIdx.x;
     if (t < cx * cy * cz) {
@@ -378,20 +457,24 @@ struct DFetch {
 __global__ void __launch_bounds__(NT) k_apply_a(LevelView L, const double* __restrict__ x,
                                                 double* __restrict__ out) {
   DFetch X{x, nullptr};
+  __shared__ double tile[TSN];
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    fill_halo<double>(L, brick, tile, X);
+    __syncthreads();
     const int c = brick * BR3 + threadIdx.x;
-    const uint8_t ty = L.type[c];
+    const uint32_t code = L.code[c];
+    const int ty = code_type(code);
     double o = 0.0;
     if (ty == CELL_SOLID) {
       o = x[c];
     } else if (ty == CELL_FLUID) {
-      int gi, gj, gk;
-      cell_coords(L, c, gi, gj, gk);
+      const int ctr = tpos_local(threadIdx.x);
       double diag, off;
-      stencil_row<double>(L, gi, gj, gk, X, diag, off);
-      o = diag * x[c] - off;
+      row_from_tile<double>(L, code, tile, ctr, diag, off);
+      o = diag * tile[ctr] - off;
     }
     out[c] = o;
+    __syncthreads();
   }
 }
 
@@ -520,22 +603,26 @@ __global__ void __launch_bounds__(NT) k_pcg_matvec(LevelView L, const double* __
                                                    SolveFlags* flags, int maxit) {
   if (stopped(flags, maxit)) return;
   DFetch X{p, nullptr};
+  __shared__ double tile[TSN];
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    fill_halo<double>(L, brick, tile, X);
+    __syncthreads();
     const int c = brick * BR3 + threadIdx.x;
-    const uint8_t ty = L.type[c];
+    const uint32_t code = L.code[c];
+    const int ty = code_type(code);
+    const double pc = p[c];
     double o = 0.0;
     if (ty == CELL_SOLID) {
-      o = p[c];
+      o = pc;
     } else if (ty == CELL_FLUID) {
-      int gi, gj, gk;
-      cell_coords(L, c, gi, gj, gk);
       double diag, off;
-      stencil_row<double>(L, gi, gj, gk, X, diag, off);
-      o = diag * p[c] - off;
+      row_from_tile<double>(L, code, tile, tpos_local(threadIdx.x), diag, off);
+      o = diag * pc - off;
     }
     Ap[c] = o;
-    part[0] += p[c] * o;
+    part[0] += pc * o;
+    __syncthreads();
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) {
     S[S_PAP] = t[0];
@@ -616,17 +703,20 @@ __global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double*
                                                       const double* __restrict__ rhs,
                                                       double* __restrict__ xf, RedBuf rb, double* S) {
   DFetch X{x, xmean};
+  __shared__ double tile[TSN];
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    fill_halo<double>(L, brick, tile, X);
+    __syncthreads();
     const int c = brick * BR3 + threadIdx.x;
-    const uint8_t ty = L.type[c];
+    const uint32_t code = L.code[c];
+    const int ty = code_type(code);
     double ax = 0.0, xv = x[c];
     if (ty == CELL_FLUID) {
-      int gi, gj, gk;
-      cell_coords(L, c, gi, gj, gk);
+      const int ctr = tpos_local(threadIdx.x);
       double diag, off;
-      stencil_row<double>(L, gi, gj, gk, X, diag, off);
-      xv = X(c, gi, gj, gk);
+      row_from_tile<double>(L, code, tile, ctr, diag, off);
+      xv = tile[ctr];
       ax = diag * xv - off;
     } else if (ty == CELL_SOLID) {
       ax = xv;
@@ -634,8 +724,27 @@ __global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double*
     xf[c] = xv;
     const double e = rhs[c] - ax;
     part[0] += e * e;
+    __syncthreads();
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) { S[S_TRUERES2] = t[0]; });
+}
+
+// Loop condition of the graph form: keep cycling while not converged, not
+// broken down and under the cycle cap.
+__global__ void k_set_cond(cudaGraphConditionalHandle h, const SolveFlags* f, int maxit,
+                           unsigned long long* execs) {
+  cudaGraphSetConditional(h, (f->stop == 0 && f->iters < maxit) ? 1u : 0u);
+  if (execs) *execs += 1ull;
+}
+
+// Per-solve report: iterations, stop code, early exit, |rhs|^2, |true residual|^2, NaN.
+__global__ void k_report(const SolveFlags* f, const double* S, double* out) {
+  out[0] = static_cast<double>(f->iters);
+  out[1] = static_cast<double>(f->stop);
+  out[2] = static_cast<double>(f->early);
+  out[3] = S[S_BNORM2];
+  out[4] = S[S_TRUERES2];
+  out[5] = static_cast<double>(f->nan);
 }
 
 }  // namespace
@@ -670,14 +779,19 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
   for (size_t l = 0; l < H.size(); ++l) {
     DevLevel& D = lv_[l];
     D.h = std::move(H[l]);
+    int bcs[6];
+    for (int f = 0; f < 6; ++f) bcs[f] = g.face[f].type;
+    build_codes(D.h, bcs);
     const HostLevel& h = D.h;
     const size_t ncs = static_cast<size_t>(h.nbrick) * BR3;
     D.d_lut = static_cast<int*>(alloc(h.lut.size() * sizeof(int)));
     D.d_bcoord = static_cast<int*>(alloc(h.bcoord.size() * sizeof(int)));
     D.d_type = static_cast<uint8_t*>(alloc(ncs));
+    D.d_code = static_cast<uint16_t*>(alloc(ncs * sizeof(uint16_t)));
     NB_CUDA(cudaMemcpy(D.d_lut, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice));
     NB_CUDA(cudaMemcpy(D.d_bcoord, h.bcoord.data(), h.bcoord.size() * sizeof(int), cudaMemcpyHostToDevice));
     NB_CUDA(cudaMemcpy(D.d_type, h.type.data(), ncs, cudaMemcpyHostToDevice));
+    NB_CUDA(cudaMemcpy(D.d_code, h.code.data(), ncs * sizeof(uint16_t), cudaMemcpyHostToDevice));
     D.b = alloc(ncs * tsz);
     D.x0 = alloc(ncs * tsz);
     D.x1 = alloc(ncs * tsz);
@@ -703,6 +817,7 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
     v.lut = D.d_lut;
     v.bcoord = D.d_bcoord;
     v.type = D.d_type;
+    v.code = D.d_code;
   }
   n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
   double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
@@ -718,6 +833,8 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
   NB_CUDA(cudaMemset(S_, 0, S_COUNT * sizeof(double)));
   flags_ = static_cast<SolveFlags*>(alloc(sizeof(SolveFlags)));
   NB_CUDA(cudaMemset(flags_, 0, sizeof(SolveFlags)));
+  body_execs_ = static_cast<unsigned long long*>(alloc(sizeof(unsigned long long)));
+  NB_CUDA(cudaMemset(body_execs_, 0, sizeof(unsigned long long)));
   rb_.max_blocks = MAX_GRID;
   rb_.partials = static_cast<double*>(alloc(RED_KMAX * MAX_GRID * sizeof(double)));
   rb_.counter = static_cast<unsigned*>(alloc(sizeof(unsigned)));
@@ -734,6 +851,7 @@ MgSolver::~MgSolver() {
   for (void* p : allocs_) cudaFree(p);
   if (h_flags_) cudaFreeHost(h_flags_);
   if (h_S_) cudaFreeHost(h_S_);
+  if (side_) cudaStreamDestroy(side_);
 }
 
 void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
@@ -859,7 +977,96 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   NB_CUDA(cudaGetLastError());
 }
 
-void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxit) {
+void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxit, double* report) {
+  setup(s, b, tol, maxit);
+  // Iterate in batches; every kernel returns at once after convergence, so
+  // over-issuing costs only launch latency. The batch grows geometrically.
+  int issued = 0, batch = 4;
+  while (issued < maxit) {
+    const int cnt = std::min(batch, maxit - issued + (maxit - issued) % 2);
+    iterate(s, tol, maxit, cnt);
+    issued += cnt;
+    NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaStreamSynchronize(s));
+    if (h_flags_->stop != 0 || h_flags_->iters >= maxit) break;
+    batch = std::min(batch * 2, 16);
+  }
+  finish(s, report);
+}
+
+// Graph form: the cycle loop is a conditional WHILE node whose body runs two
+// cycles (so the r/rnew buffers return to their captured roles) and then sets
+// the loop condition on the device. Must be called while `s` is capturing.
+void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int maxit, double* report,
+                             uint64_t* body_kernels) {
+  setup(s, b, tol, maxit);
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  NB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphConditionalHandle h;
+  NB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  NB_LAUNCH(lc_, "set_cond", s, 0, (k_set_cond<<<1, 1, 0, s>>>(h, flags_, maxit, nullptr)));
+  NB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  NB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  if (!side_) NB_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+  uint64_t* saved = lc_.count;
+  uint64_t nbody = 0;
+  lc_.count = &nbody;
+  NB_CUDA(cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  iterate(side_, tol, maxit, 2);
+  NB_LAUNCH(lc_, "set_cond", side_, 0, (k_set_cond<<<1, 1, 0, side_>>>(h, flags_, maxit, body_execs_)));
+  cudaGraph_t body_out = nullptr;
+  NB_CUDA(cudaStreamEndCapture(side_, &body_out));
+  lc_.count = saved;
+  if (body_kernels) *body_kernels = nbody;
+  NB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  finish(s, report);
+}
+
+void MgSolver::finish(cudaStream_t s, double* report) {
+  const LevelView& L = lv_[0].v;
+  const int grid = grid_for(L.nbrick);
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / static_cast<double>(lv_[0].h.nfluid) : 0.0;
+  const bool sing = singular_ && lv_[0].h.nfluid > 0;
+  // final removeMean(x) + true residual (multigrid.cpp:341-353)
+  if (sing) {
+    k_fluid_mean<<<grid, NT, 0, s>>>(L, x_, nullptr, rb_, S_ + S_XMEAN, inv_nf, nullptr, maxit_);
+    lc_.add();
+  }
+  k_true_residual<<<grid, NT, 0, s>>>(L, x_, sing ? S_ + S_XMEAN : nullptr, rhs_, xfin_, rb_, S_);
+  lc_.add();
+  if (report) {
+    k_report<<<1, 1, 0, s>>>(flags_, S_, report);
+    lc_.add();
+  }
+  NB_CUDA(cudaGetLastError());
+}
+
+nb_poisson_report MgSolver::report_from(const double* r, double tol) {
+  nb_poisson_report rep{};
+  const double bnorm = std::sqrt(r[3]) + 1e-300;
+  if (r[2] != 0.0) {  // early exit: rhs already below tolerance
+    rep.iterations = 0;
+    rep.residual = std::sqrt(r[3]) / bnorm;
+    rep.converged = 1;
+    return rep;
+  }
+  rep.iterations = static_cast<int>(r[0]);
+  rep.residual = std::sqrt(r[4]) / bnorm;
+  rep.converged = (r[1] == 1.0 || rep.residual <= tol) ? 1 : 0;
+  return rep;
+}
+
+void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit) {
   tol_ = tol;
   maxit_ = maxit;
   const LevelView& L = lv_[0].v;
@@ -899,44 +1106,16 @@ void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxi
                                            rb_, S_, flags_, maxit);
   lc_.add();
   NB_CUDA(cudaGetLastError());
-  // Iterate in batches; every kernel returns at once after convergence, so
-  // over-issuing costs only launch latency. The batch grows geometrically.
-  int issued = 0, batch = 4;
-  while (issued < maxit) {
-    const int cnt = std::min(batch, maxit - issued);
-    iterate(s, tol, maxit, cnt);
-    issued += cnt;
-    NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
-    NB_CUDA(cudaStreamSynchronize(s));
-    if (h_flags_->stop != 0 || h_flags_->iters >= maxit) break;
-    batch = std::min(batch * 2, 16);
-  }
-  // final removeMean(x) + true residual
-  if (sing) {
-    k_fluid_mean<<<grid, NT, 0, s>>>(L, x_, nullptr, rb_, S_ + S_XMEAN, inv_nf, nullptr, maxit);
-    lc_.add();
-  }
-  k_true_residual<<<grid, NT, 0, s>>>(L, x_, sing ? S_ + S_XMEAN : nullptr, rhs_, xfin_, rb_, S_);
-  lc_.add();
-  NB_CUDA(cudaGetLastError());
 }
 
 nb_poisson_report MgSolver::fetch_report(cudaStream_t s) {
   NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
   NB_CUDA(cudaMemcpyAsync(h_S_, S_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s));
   NB_CUDA(cudaStreamSynchronize(s));
-  nb_poisson_report rep{};
-  const double bnorm = std::sqrt(h_S_[S_BNORM2]) + 1e-300;
-  if (h_flags_->early) {
-    rep.iterations = 0;
-    rep.residual = std::sqrt(h_S_[S_BNORM2]) / bnorm;
-    rep.converged = 1;
-    return rep;
-  }
-  rep.iterations = h_flags_->iters;
-  rep.residual = std::sqrt(h_S_[S_TRUERES2]) / bnorm;
-  rep.converged = (h_flags_->stop == 1 || rep.residual <= tol_) ? 1 : 0;
-  return rep;
+  const double r[6] = {static_cast<double>(h_flags_->iters), static_cast<double>(h_flags_->stop),
+                       static_cast<double>(h_flags_->early), h_S_[S_BNORM2], h_S_[S_TRUERES2],
+                       static_cast<double>(h_flags_->nan)};
+  return report_from(r, tol_);
 }
 
 void MgSolver::solve(cudaStream_t s, const double* b, double tol, int maxit) {

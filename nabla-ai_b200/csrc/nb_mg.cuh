@@ -22,6 +22,7 @@ struct DevLevel {
   int* d_lut = nullptr;
   int* d_bcoord = nullptr;
   uint8_t* d_type = nullptr;
+  uint16_t* d_code = nullptr;
   // V-cycle vectors in the level's arithmetic type (double or float):
   // b (restricted residual), x ping, x pong.
   void* b = nullptr;
@@ -42,8 +43,21 @@ class MgSolver {
   void solve(cudaStream_t s, const double* b_dev, double tol, int maxit);
   // Same but leaves the report on the device (no host synchronisation);
   // read it later with fetch_report().
-  void solve_async(cudaStream_t s, const double* b_dev, double tol, int maxit);
+  void solve_async(cudaStream_t s, const double* b_dev, double tol, int maxit,
+                   double* report = nullptr);
   nb_poisson_report fetch_report(cudaStream_t s);
+  // Issues the whole solve into stream `s`, which must be capturing a graph:
+  // the cycle loop becomes a conditional WHILE node (no host round trip).
+  // `report` (6 doubles, device) receives iterations, stop code, early-exit
+  // flag, |rhs|^2, |true residual|^2 and the NaN flag. `body_kernels`
+  // receives the kernel count of one loop-body execution.
+  void capture_solve(cudaStream_t s, const double* b_dev, double tol, int maxit, double* report,
+                     uint64_t* body_kernels);
+  static nb_poisson_report report_from(const double* r, double tol);
+  // Number of loop-body executions so far (device counter).
+  unsigned long long* body_execs() const { return body_execs_; }
+  void set_counter(uint64_t* c) { lc_.count = c; }
+  uint64_t* counter() const { return lc_.count; }
 
   // out = A x (CgPoisson::applyA on level 0), brick layout.
   void apply_a(cudaStream_t s, const double* x, double* out);
@@ -65,7 +79,11 @@ class MgSolver {
   void vcycle(cudaStream_t s, int lvl, const void* b, int bmean_slot, void* xout_final,
               int* out_mean_slot, void** out_x);
   void iterate(cudaStream_t s, double tol, int maxit, int count);
+  void setup(cudaStream_t s, const double* b, double tol, int maxit);
+  void finish(cudaStream_t s, double* report);
   void* alloc(size_t bytes);
+  cudaStream_t side_ = nullptr;               // capture stream of the loop body
+  unsigned long long* body_execs_ = nullptr;  // device counter
 
   std::vector<DevLevel> lv_;
   bool singular_ = false;
