@@ -164,6 +164,53 @@ nb_status nb_poisson_solve(nb_ctx* ctx, const nb_grid_desc* grid, const double* 
 /* Replaces CgPoisson::applyA (core/src/flow/poisson.cpp:102-134). */
 nb_status nb_apply_laplacian(nb_ctx* ctx, const nb_grid_desc* grid, const double* x, double* out);
 
+/* ---- octree-AMR brick meshes ------------------------------------------------
+ * A mesh is a set of leaf bricks of 8x8x8 cells at octree levels 0..lmax over
+ * a base grid of nb0 bricks per axis at level 0 (cell size h0 / 2^level),
+ * 2:1 balanced across faces, edges and corners. A leaf is 4 int32 values:
+ * (level, bx, by, bz) in level-`level` brick coordinates. Cell arrays over a
+ * mesh are nleaf*512 doubles: leaves in the mesh's rank order (Morton order
+ * of the leaf anchors on the finest level, the key of
+ * core/include/nabla/mesh/morton.hpp:19-48), cells x-fastest inside a brick.
+ * Replaces the reference's leaves-only linear Octree (core/src/mesh/octree.cpp)
+ * for the flow path; its face rule follows OctreePoisson
+ * (core/src/flow/octree_poisson.cpp:24-105). */
+typedef struct nb_amr_geom {
+  int32_t nb0[3];
+  int32_t lmax;
+  double h0[3];
+  double origin[3];
+  nb_face_bc face[6];
+} nb_amr_geom;
+
+typedef struct nb_amr_mesh nb_amr_mesh;
+
+/* Splits the flagged leaves (flags[i] != 0) and restores 2:1 balance
+ * (Octree::refineByMorton's balance, core/src/mesh/octree.cpp:325-356, at
+ * brick granularity and over all 26 neighbours). `out` receives the new leaf
+ * list (4 int32 each, any order) when `cap` is large enough; `n_out` always
+ * receives the required count (NB_ERR_BAD_ARG if cap is too small). */
+nb_status nb_amr_refine(const nb_amr_geom* g, const int32_t* leaves, int64_t n, const uint8_t* flags,
+                        int32_t* out, int64_t cap, int64_t* n_out);
+/* Builds a mesh from a leaf list (validated: coverage, no overlap, balance).
+ * `solid` (optional) holds 512 bytes per leaf in the INPUT order. */
+nb_status nb_amr_mesh_create(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* leaves, int64_t n,
+                             const uint8_t* solid, nb_amr_mesh** out);
+void nb_amr_mesh_destroy(nb_amr_mesh* m);
+int64_t nb_amr_mesh_leaf_count(const nb_amr_mesh* m);
+/* Leaves in rank order (4 int32 each). */
+nb_status nb_amr_mesh_leaves(const nb_amr_mesh* m, int32_t* out);
+/* Composite -Laplacian per unit volume, (A x)_i = (1/V_i) sum_f area_f/dist_f
+ * (x_i - x_n): OctreePoisson::applyA (core/src/flow/octree_poisson.cpp:64-85)
+ * divided by the cell volume, plus the uniform operator's outlet (Dirichlet)
+ * and periodic closures (core/src/flow/poisson.cpp:18-52). Solid rows identity. */
+nb_status nb_amr_apply_laplacian(nb_ctx* ctx, nb_amr_mesh* m, const double* x, double* out);
+/* MG-PCG on the composite operator (volume-weighted inner products and means;
+ * composite V-cycle merging the finest octree level per MG level, then the
+ * uniform coarsening of core/src/flow/multigrid.cpp:211-266). */
+nb_status nb_amr_poisson_solve(nb_ctx* ctx, nb_amr_mesh* m, const double* b, double* x, double tol,
+                               int max_cycles, int precision, nb_poisson_report* rep);
+
 /* ---- allocation-free operator ---------------------------------------------
  * No counterpart in the reference. The same -Laplacian as nb_apply_laplacian,
  * for callers that cannot call cudaMalloc: code issuing work while a stream is

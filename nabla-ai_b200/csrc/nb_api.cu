@@ -10,23 +10,11 @@
 #include <string>
 #include <vector>
 
+#include "nb_ctx.h"
 #include "nb_flow.cuh"
 #include "nb_mg.cuh"
 
 using namespace nb;
-
-struct nb_ctx {
-  int device = 0;
-  std::string err;
-  uint64_t launches = 0;
-  Profiler prof;
-  cudaStream_t stream = nullptr;
-  // MgPoisson-style cache for the host-array Poisson seam (multigrid.cpp:211-220)
-  std::map<std::pair<uint64_t, int>, std::unique_ptr<MgSolver>> mg_cache;
-  double* stage_a = nullptr;
-  double* stage_b = nullptr;
-  size_t stage_bytes = 0;
-};
 
 // Results of one step, written by the step's kernels.
 struct StepBlock {
@@ -104,25 +92,18 @@ struct nb_case {
   }
 };
 
+void nb::ensure_staging(nb_ctx* ctx, size_t elems) {
+  if (ctx->stage_bytes >= elems * sizeof(double)) return;
+  if (ctx->stage_a) cudaFree(ctx->stage_a);
+  if (ctx->stage_b) cudaFree(ctx->stage_b);
+  ctx->stage_a = ctx->stage_b = nullptr;
+  ctx->stage_bytes = 0;
+  NB_CUDA(cudaMalloc(&ctx->stage_a, elems * sizeof(double)));
+  NB_CUDA(cudaMalloc(&ctx->stage_b, elems * sizeof(double)));
+  ctx->stage_bytes = elems * sizeof(double);
+}
+
 namespace {
-
-nb_status fail(nb_ctx* ctx, nb_status s, const std::string& msg) {
-  if (ctx) ctx->err = msg;
-  return s;
-}
-
-template <class Fn>
-nb_status guarded(nb_ctx* ctx, Fn&& fn) {
-  try {
-    return fn();
-  } catch (const ApiError& e) {
-    return fail(ctx, e.status, e.what);
-  } catch (const CudaError& e) {
-    return fail(ctx, NB_ERR_CUDA, e.what);
-  } catch (const std::exception& e) {
-    return fail(ctx, NB_ERR_BAD_ARG, e.what());
-  }
-}
 
 bool grid_ok(const nb_grid_desc* g, std::string& why) {
   if (!g) { why = "grid is NULL"; return false; }
@@ -441,17 +422,6 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
   }
   rep->cell_count = static_cast<uint64_t>(g.nx) * g.ny * g.nz;
   rep->accepted = (rep->continuity_residual < c.cfg.tol_continuity && rep->mass_error < c.cfg.tol_mass) ? 1 : 0;
-}
-
-void ensure_staging(nb_ctx* ctx, size_t elems) {
-  if (ctx->stage_bytes >= elems * sizeof(double)) return;
-  if (ctx->stage_a) cudaFree(ctx->stage_a);
-  if (ctx->stage_b) cudaFree(ctx->stage_b);
-  ctx->stage_a = ctx->stage_b = nullptr;
-  ctx->stage_bytes = 0;
-  NB_CUDA(cudaMalloc(&ctx->stage_a, elems * sizeof(double)));
-  NB_CUDA(cudaMalloc(&ctx->stage_b, elems * sizeof(double)));
-  ctx->stage_bytes = elems * sizeof(double);
 }
 
 MgSolver& ctx_solver(nb_ctx* ctx, const nb_grid_desc& g, int precision) {

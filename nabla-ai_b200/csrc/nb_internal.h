@@ -26,6 +26,7 @@ namespace nb {
 
 constexpr int BR = 8;       // brick edge (cells)
 constexpr int BR3 = 512;    // cells per brick
+constexpr int AMR_MAXLEV = 6;  // octree levels of a composite mesh
 enum : uint8_t { CELL_FLUID = 0, CELL_SOLID = 1, CELL_VOID = 2 };
 
 // ---------------------------------------------------------------------------
@@ -45,9 +46,29 @@ struct LevelView {
   // bit f (f = 2*axis + side, side 0 low / 1 high): face f couples to a fluid
   // neighbour; bit 6+f: face f is a Dirichlet outlet face; bits 12-13: CELL_*.
   const uint16_t* code;
+  // ---- composite (multi-level) levels only: amr != 0 ----
+  // Bricks carry their own octree level; `lut` holds one dense table per
+  // octree level (offset lut_off[L], lnb[L] bricks per axis, -1 = no leaf);
+  // bit f of `code` couples to the same-level neighbour only, coarse-fine
+  // couplings are the CSR list cf_off/cf_nbr/cf_coef (CODE_HASCF cells).
+  int amr;
+  int nlev;
+  int lut_off[AMR_MAXLEV];
+  int lnb[AMR_MAXLEV][3];
+  int lcells[AMR_MAXLEV][3];
+  double lh2[AMR_MAXLEV][3];
+  const int8_t* blevel;
+  const double* bweight;  // cell volume / finest cell volume (exact powers of 8)
+  const int* cf_off;
+  const int* cf_nbr;
+  const double* cf_coef;
+  // transfer to the next coarser MG level: coarse brick, octant (-1 kept)
+  const int* xf_brick;
+  const int* xf_oct;
 };
 constexpr int CODE_DIRICHLET = 6;
 constexpr int CODE_TYPE = 12;
+constexpr int CODE_HASCF = 14;  // composite levels: the cell has coarse-fine couplings
 
 __host__ __device__ inline int wrapi(int a, int n) { return (a % n + n) % n; }
 

@@ -45,17 +45,33 @@ struct XFetch {
   const double* ecmean;  // pending mean of ec
   LevelView C;           // coarse level (for parent lookup)
   int fx, fy, fz;
+  const int* xfb = nullptr;  // composite fine level: parent brick per brick
+  const int* xfo = nullptr;  // composite fine level: octant in the parent (-1 kept)
+  __device__ __forceinline__ int parent(int n, int gi, int gj, int gk) const {
+    if (xfb) {
+      const int b = n >> 9, l = n & 511, oct = xfo[b];
+      if (oct < 0) return xfb[b] * BR3 + l;
+      const int ci = (oct & 1) * 4 + ((l & 7) >> 1), cj = ((oct >> 1) & 1) * 4 + (((l >> 3) & 7) >> 1),
+                ck = (oct >> 2) * 4 + ((l >> 6) >> 1);
+      return xfb[b] * BR3 + ((ck << 6) | (cj << 3) | ci);
+    }
+    return cell_index(C, gi / fx, gj / fy, gk / fz);
+  }
   __device__ __forceinline__ T operator()(int n, int gi, int gj, int gk) const {
     T v = x ? x[n] : T(0);
     if (xmean) v = v - static_cast<T>(*xmean);
     if (ec) {
-      T e = ec[cell_index(C, gi / fx, gj / fy, gk / fz)];
+      T e = ec[parent(n, gi, gj, gk)];
       if (ecmean) e = e - static_cast<T>(*ecmean);
       v = v + e;
     }
     return v;
   }
 };
+
+__device__ __forceinline__ double cell_weight(const LevelView& L, int brick) {
+  return L.amr ? L.bweight[brick] : 1.0;
+}
 
 // Row of the -Laplacian at fluid cell (gi,gj,gk): returns diag (raw sum of
 // face coefficients) and off = sum coeff * x[n] in the reference's order
@@ -101,7 +117,44 @@ __device__ __forceinline__ int tpos_local(int l) { return tpos(l & 7, (l >> 3) &
 __device__ __forceinline__ int code_type(uint32_t code) { return (code >> CODE_TYPE) & 3; }
 
 template <typename T, class F>
+__device__ __forceinline__ void fill_halo_amr(const LevelView& L, int brick, T* tile, const F& fx) {
+  const int lev = L.blevel[brick];
+  const int ox = L.bcoord[3 * brick] * BR, oy = L.bcoord[3 * brick + 1] * BR,
+            oz = L.bcoord[3 * brick + 2] * BR;
+  const int dims[3] = {L.lcells[lev][0], L.lcells[lev][1], L.lcells[lev][2]};
+  for (int p = threadIdx.x; p < TSN; p += blockDim.x) {
+    const int ti = p % TS - 1, tj = (p / TS) % TS - 1, tk = p / (TS * TS) - 1;
+    const int outc = (ti < 0 || ti > 7) + (tj < 0 || tj > 7) + (tk < 0 || tk > 7);
+    if (outc > 1) continue;
+    int g[3] = {ox + ti, oy + tj, oz + tk};
+    T v = T(0);
+    if (outc == 0) {
+      v = fx(brick * BR3 + ((tk << 6) | (tj << 3) | ti), g[0], g[1], g[2]);
+    } else {
+      bool ok = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (g[a] < 0 || g[a] >= dims[a]) {
+          if (L.bc[2 * a] == NB_BC_PERIODIC) g[a] = wrapi(g[a], dims[a]);
+          else ok = false;
+        }
+      if (ok) {
+        // same-level neighbour only; other halo cells are never read
+        const int nb = L.lut[L.lut_off[lev] + ((g[2] >> 3) * L.lnb[lev][1] + (g[1] >> 3)) * L.lnb[lev][0] +
+                             (g[0] >> 3)];
+        if (nb >= 0) v = fx(nb * BR3 + (((g[2] & 7) << 6) | ((g[1] & 7) << 3) | (g[0] & 7)), g[0], g[1], g[2]);
+      }
+    }
+    tile[p] = v;
+  }
+}
+
+template <typename T, class F>
 __device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile, const F& fx) {
+  if (L.amr) {
+    fill_halo_amr<T>(L, brick, tile, fx);
+    return;
+  }
   const int ox = L.bcoord[3 * brick] * BR, oy = L.bcoord[3 * brick + 1] * BR,
             oz = L.bcoord[3 * brick + 2] * BR;
   const int dims[3] = {L.nx, L.ny, L.nz};
@@ -131,13 +184,13 @@ __device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile
 // off = sum coeff * neighbour, faces in the reference's order (poisson.cpp:114-129).
 template <typename T>
 __device__ __forceinline__ void row_from_tile(const LevelView& L, uint32_t code, const T* tile, int ctr,
-                                              T& diag, T& off) {
+                                              T& diag, T& off, int lev = 0) {
   diag = T(0);
   off = T(0);
   const int step[6] = {-1, 1, -TS, TS, -TS * TS, TS * TS};
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
-    const T h2 = static_cast<T>(L.h2[f >> 1]);
+    const T h2 = static_cast<T>(L.amr ? L.lh2[lev][f >> 1] : L.h2[f >> 1]);
     if (code & (1u << f)) {
       diag += h2;
       off += h2 * tile[ctr + step[f]];
@@ -145,6 +198,27 @@ __device__ __forceinline__ void row_from_tile(const LevelView& L, uint32_t code,
       diag += T(2) * h2;
     }
   }
+}
+
+// Coarse-fine couplings of a composite-level cell (added after the six
+// same-level faces): coefficient c with neighbour value x_n.
+template <typename T, class F>
+__device__ __forceinline__ void add_cf(const LevelView& L, uint32_t code, int c, const F& fx, T& diag, T& off) {
+  if (!(code & (1u << CODE_HASCF))) return;
+  for (int q = L.cf_off[c]; q < L.cf_off[c + 1]; ++q) {
+    const T coef = static_cast<T>(L.cf_coef[q]);
+    diag += coef;
+    off += coef * fx(L.cf_nbr[q], 0, 0, 0);
+  }
+}
+
+// Full row: same-level faces from the tile, then coarse-fine couplings.
+template <typename T, class F>
+__device__ __forceinline__ void full_row(const LevelView& L, uint32_t code, const T* tile, int brick, int c,
+                                         const F& fx, T& diag, T& off) {
+  const int lev = L.amr ? L.blevel[brick] : 0;
+  row_from_tile<T>(L, code, tile, tpos_local(c & 511), diag, off, lev);
+  if (L.amr) add_cf<T>(L, code, c, fx, diag, off);
 }
 
 // ---------------------------------------------------------------------------
@@ -171,16 +245,19 @@ __global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict_
       const int ctr = tpos_local(threadIdx.x);
       T diag, off, xc;
       if (X.x || X.ec) {
-        row_from_tile<T>(L, code, tile, ctr, diag, off);
+        full_row<T>(L, code, tile, brick, c, X, diag, off);
         xc = tile[ctr];
       } else {  // first sweep from x = 0: A x = 0
+        const int lev = L.amr ? L.blevel[brick] : 0;
         diag = T(0);
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
-          const T h2 = static_cast<T>(L.h2[f >> 1]);
+          const T h2 = static_cast<T>(L.amr ? L.lh2[lev][f >> 1] : L.h2[f >> 1]);
           if (code & (1u << f)) diag += h2;
           else if (code & (1u << (CODE_DIRICHLET + f))) diag += T(2) * h2;
         }
+        if (L.amr && (code & (1u << CODE_HASCF)))
+          for (int q = L.cf_off[c]; q < L.cf_off[c + 1]; ++q) diag += static_cast<T>(L.cf_coef[q]);
         off = T(0);
         xc = T(0);
       }
@@ -189,7 +266,7 @@ __global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict_
       const T Ax = diag * xc - off;
       const T dM = diag > T(0) ? diag : T(1);
       out = xc + static_cast<T>(kOmega) * (bc - Ax) / dM;
-      part[0] += static_cast<double>(out);
+      part[0] += cell_weight(L, brick) * static_cast<double>(out);
     }
     xout[c] = out;
     __syncthreads();
@@ -227,7 +304,7 @@ __global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __r
     if (fluid) {
       const int ctr = tpos_local(threadIdx.x);
       T diag, off;
-      row_from_tile<T>(F, code, tile, ctr, diag, off);
+      full_row<T>(F, code, tile, brick, c, X, diag, off);
       T bc = b[c];
       if (bmean) bc = bc - static_cast<T>(*bmean);
       r = bc - (diag * tile[ctr] - off);
@@ -236,7 +313,34 @@ __global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __r
     fl[threadIdx.x] = fluid;
     __syncthreads();
     const int t = threadIdx.x;
-    if (t < cx * cy * cz) {
+    if (F.amr) {
+      // composite transfer: a kept brick maps cell-for-cell; a merged brick
+      // fills one octant (4^3 cells) of its parent with child averages.
+      const int cb = F.xf_brick[brick], oct = F.xf_oct[brick];
+      const double wc = cell_weight(C, cb);
+      if (oct < 0) {
+        const T val = fl[t] ? rs[t] : T(0);
+        rc[cb * BR3 + t] = val;
+        part[0] += wc * static_cast<double>(val);
+      } else if (t < 64) {
+        const int lci = t & 3, lcj = (t >> 2) & 3, lck = t >> 4;
+        T sum = T(0);
+        int count = 0;
+        for (int dk = 0; dk < 2; ++dk)
+          for (int dj = 0; dj < 2; ++dj)
+            for (int di = 0; di < 2; ++di) {
+              const int l = ((2 * lck + dk) << 6) | ((2 * lcj + dj) << 3) | (2 * lci + di);
+              if (fl[l]) {
+                sum += rs[l];
+                ++count;
+              }
+            }
+        const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
+        const int ci = (oct & 1) * 4 + lci, cj = ((oct >> 1) & 1) * 4 + lcj, ck = (oct >> 2) * 4 + lck;
+        rc[cb * BR3 + ((ck << 6) | (cj << 3) | ci)] = val;
+        part[0] += wc * static_cast<double>(val);
+      }
+    } else if (t < cx * cy * cz) {
       const int lci = t % cx, lcj = (t / cx) % cy, lck = t / (cx * cy);
       const int gci = F.bcoord[3 * brick] * cx + lci;
       const int gcj = F.bcoord[3 * brick + 1] * cy + lcj;
@@ -470,7 +574,7 @@ __global__ void __launch_bounds__(NT) k_apply_a(LevelView L, const double* __res
     } else if (ty == CELL_FLUID) {
       const int ctr = tpos_local(threadIdx.x);
       double diag, off;
-      row_from_tile<double>(L, code, tile, ctr, diag, off);
+      full_row<double>(L, code, tile, brick, c, X, diag, off);
       o = diag * tile[ctr] - off;
     }
     out[c] = o;
@@ -487,7 +591,7 @@ __global__ void __launch_bounds__(NT) k_fluid_mean(LevelView L, const double* __
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
     const int c = brick * BR3 + threadIdx.x;
-    if (L.type[c] == CELL_FLUID) part[0] += vmean ? v[c] - *vmean : v[c];
+    if (L.type[c] == CELL_FLUID) part[0] += cell_weight(L, brick) * (vmean ? v[c] - *vmean : v[c]);
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
 }
@@ -503,7 +607,7 @@ __global__ void __launch_bounds__(NT) k_fluid_mean_f(LevelView L, const float* _
     const int c = brick * BR3 + threadIdx.x;
     if (L.type[c] == CELL_FLUID) {
       const double z = static_cast<double>(v[c]);
-      part[0] += vmean ? z - *vmean : z;
+      part[0] += cell_weight(L, brick) * (vmean ? z - *vmean : z);
     }
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
@@ -525,7 +629,7 @@ __global__ void __launch_bounds__(NT) k_pcg_setup(LevelView L, const double* __r
     r[c] = v;
     x[c] = 0.0;
     if (r_f) r_f[c] = static_cast<float>(v);
-    part[0] += v * v;
+    part[0] += cell_weight(L, brick) * (v * v);
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) {
     S[S_BNORM2] = t[0];
@@ -566,10 +670,10 @@ __global__ void __launch_bounds__(NT) k_pcg_dots(LevelView L, const TZ* __restri
     zo[c] = v;
     if (first) {
       p[c] = v;
-      part[0] += r[c] * v;
+      part[0] += cell_weight(L, brick) * (r[c] * v);
     } else {
-      part[0] += v * rnew[c];
-      part[1] += v * r[c];
+      part[0] += cell_weight(L, brick) * (v * rnew[c]);
+      part[1] += cell_weight(L, brick) * (v * r[c]);
     }
   }
   grid_reduce<2>(part, rb, [=] __device__(const double* t) {
@@ -617,11 +721,11 @@ __global__ void __launch_bounds__(NT) k_pcg_matvec(LevelView L, const double* __
       o = pc;
     } else if (ty == CELL_FLUID) {
       double diag, off;
-      row_from_tile<double>(L, code, tile, tpos_local(threadIdx.x), diag, off);
+      full_row<double>(L, code, tile, brick, c, X, diag, off);
       o = diag * pc - off;
     }
     Ap[c] = o;
-    part[0] += pc * o;
+    part[0] += cell_weight(L, brick) * (pc * o);
     __syncthreads();
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) {
@@ -667,9 +771,9 @@ __global__ void __launch_bounds__(NT) k_pcg_update(LevelView L, double* __restri
     const double rn = r[c] - alpha * Ap[c];
     rnew[c] = rn;
     if (singular) {
-      if (L.type[c] == CELL_FLUID) part[0] += rn;
+      if (L.type[c] == CELL_FLUID) part[0] += cell_weight(L, brick) * rn;
     } else {
-      part[0] += rn * rn;
+      part[0] += cell_weight(L, brick) * (rn * rn);
       if (rnew_f) rnew_f[c] = static_cast<float>(rn);
     }
   }
@@ -691,7 +795,7 @@ __global__ void __launch_bounds__(NT) k_pcg_center(LevelView L, double* __restri
     const double v = L.type[c] == CELL_FLUID ? rnew[c] - mean : 0.0;
     rnew[c] = v;
     if (rnew_f) rnew_f[c] = static_cast<float>(v);
-    part[0] += v * v;
+    part[0] += cell_weight(L, brick) * (v * v);
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) { conv_check(t[0], S, flags, tol); });
 }
@@ -715,7 +819,7 @@ __global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double*
     if (ty == CELL_FLUID) {
       const int ctr = tpos_local(threadIdx.x);
       double diag, off;
-      row_from_tile<double>(L, code, tile, ctr, diag, off);
+      full_row<double>(L, code, tile, brick, c, X, diag, off);
       xv = tile[ctr];
       ax = diag * xv - off;
     } else if (ty == CELL_SOLID) {
@@ -723,7 +827,7 @@ __global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double*
     }
     xf[c] = xv;
     const double e = rhs[c] - ax;
-    part[0] += e * e;
+    part[0] += cell_weight(L, brick) * (e * e);
     __syncthreads();
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) { S[S_TRUERES2] = t[0]; });
@@ -765,60 +869,117 @@ void* MgSolver::alloc(size_t bytes) {
   return p;
 }
 
-MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
-    : precision_(precision), lc_(lc) {
-  std::vector<HostLevel> H = build_hierarchy(g);
-  singular_ = true;
-  for (int f = 0; f < 6; ++f)
-    if (g.face[f].type == NB_BC_OUTLET) singular_ = false;  // hasDirichlet, poisson.cpp:93-100
-  const HostLevel& last = H.back();
-  if (static_cast<size_t>(last.nx) * last.ny * last.nz > COARSE_MAX_CELLS)
-    throw ApiError{NB_ERR_UNSUPPORTED, "coarsest multigrid level exceeds 4096 cells"};
-  const size_t tsz = precision == NB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
-  lv_.resize(H.size());
-  for (size_t l = 0; l < H.size(); ++l) {
-    DevLevel& D = lv_[l];
-    D.h = std::move(H[l]);
-    int bcs[6];
-    for (int f = 0; f < 6; ++f) bcs[f] = g.face[f].type;
-    build_codes(D.h, bcs);
-    const HostLevel& h = D.h;
-    const size_t ncs = static_cast<size_t>(h.nbrick) * BR3;
-    D.d_lut = static_cast<int*>(alloc(h.lut.size() * sizeof(int)));
-    D.d_bcoord = static_cast<int*>(alloc(h.bcoord.size() * sizeof(int)));
-    D.d_type = static_cast<uint8_t*>(alloc(ncs));
-    D.d_code = static_cast<uint16_t*>(alloc(ncs * sizeof(uint16_t)));
-    NB_CUDA(cudaMemcpy(D.d_lut, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice));
-    NB_CUDA(cudaMemcpy(D.d_bcoord, h.bcoord.data(), h.bcoord.size() * sizeof(int), cudaMemcpyHostToDevice));
-    NB_CUDA(cudaMemcpy(D.d_type, h.type.data(), ncs, cudaMemcpyHostToDevice));
-    NB_CUDA(cudaMemcpy(D.d_code, h.code.data(), ncs * sizeof(uint16_t), cudaMemcpyHostToDevice));
-    D.b = alloc(ncs * tsz);
-    D.x0 = alloc(ncs * tsz);
-    D.x1 = alloc(ncs * tsz);
-    NB_CUDA(cudaMemset(D.b, 0, ncs * tsz));
-    NB_CUDA(cudaMemset(D.x0, 0, ncs * tsz));
-    NB_CUDA(cudaMemset(D.x1, 0, ncs * tsz));
-    LevelView& v = D.v;
-    v.nx = h.nx;
-    v.ny = h.ny;
-    v.nz = h.nz;
-    v.nbx = h.nbx;
-    v.nby = h.nby;
-    v.nbz = h.nbz;
-    v.nbrick = h.nbrick;
-    for (int f = 0; f < 6; ++f) v.bc[f] = g.face[f].type;
-    v.dxyz[0] = h.dx;
-    v.dxyz[1] = h.dy;
-    v.dxyz[2] = h.dz;
-    v.h2[0] = 1.0 / (h.dx * h.dx);
-    v.h2[1] = 1.0 / (h.dy * h.dy);
-    v.h2[2] = 1.0 / (h.dz * h.dz);
-    v.twoD = h.nz == 1;
-    v.lut = D.d_lut;
-    v.bcoord = D.d_bcoord;
-    v.type = D.d_type;
-    v.code = D.d_code;
+void MgSolver::upload_uniform(DevLevel& D, const int bcs[6]) {
+  build_codes(D.h, bcs);
+  const HostLevel& h = D.h;
+  const size_t tsz = precision_ == NB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
+  const size_t ncs = static_cast<size_t>(h.nbrick) * BR3;
+  D.d_lut = static_cast<int*>(alloc(h.lut.size() * sizeof(int)));
+  D.d_bcoord = static_cast<int*>(alloc(h.bcoord.size() * sizeof(int)));
+  D.d_type = static_cast<uint8_t*>(alloc(ncs));
+  D.d_code = static_cast<uint16_t*>(alloc(ncs * sizeof(uint16_t)));
+  NB_CUDA(cudaMemcpy(D.d_lut, h.lut.data(), h.lut.size() * sizeof(int), cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(D.d_bcoord, h.bcoord.data(), h.bcoord.size() * sizeof(int), cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(D.d_type, h.type.data(), ncs, cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(D.d_code, h.code.data(), ncs * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  D.b = alloc(ncs * tsz);
+  D.x0 = alloc(ncs * tsz);
+  D.x1 = alloc(ncs * tsz);
+  NB_CUDA(cudaMemset(D.b, 0, ncs * tsz));
+  NB_CUDA(cudaMemset(D.x0, 0, ncs * tsz));
+  NB_CUDA(cudaMemset(D.x1, 0, ncs * tsz));
+  D.wfluid = static_cast<double>(h.nfluid);
+  D.ncell = static_cast<double>(h.nx) * h.ny * h.nz;
+  LevelView& v = D.v;
+  v = LevelView{};
+  v.nx = h.nx;
+  v.ny = h.ny;
+  v.nz = h.nz;
+  v.nbx = h.nbx;
+  v.nby = h.nby;
+  v.nbz = h.nbz;
+  v.nbrick = h.nbrick;
+  for (int f = 0; f < 6; ++f) v.bc[f] = bcs[f];
+  v.dxyz[0] = h.dx;
+  v.dxyz[1] = h.dy;
+  v.dxyz[2] = h.dz;
+  v.h2[0] = 1.0 / (h.dx * h.dx);
+  v.h2[1] = 1.0 / (h.dy * h.dy);
+  v.h2[2] = 1.0 / (h.dz * h.dz);
+  v.twoD = h.nz == 1;
+  v.lut = D.d_lut;
+  v.bcoord = D.d_bcoord;
+  v.type = D.d_type;
+  v.code = D.d_code;
+}
+
+void MgSolver::upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]) {
+  const AmrTree& t = A.tree;
+  const size_t tsz = precision_ == NB_PRECISION_MIXED ? sizeof(float) : sizeof(double);
+  const int nbrick = static_cast<int>(t.leaves.size());
+  const size_t ncs = static_cast<size_t>(nbrick) * BR3;
+  auto up = [&](const void* src, size_t bytes) {
+    void* d = alloc(bytes);
+    if (src) NB_CUDA(cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice));  // empty lists stay unread
+    else NB_CUDA(cudaMemset(d, 0, bytes));
+    return d;
+  };
+  D.h = HostLevel{};
+  D.h.nbrick = nbrick;
+  D.h.nfluid = A.nfluid;
+  D.wfluid = A.wfluid;
+  D.ncell = static_cast<double>(ncs);
+  D.d_lut = static_cast<int*>(up(t.lut.data(), t.lut.size() * sizeof(int)));
+  D.d_bcoord = static_cast<int*>(up(A.bcoord.data(), A.bcoord.size() * sizeof(int)));
+  D.d_type = static_cast<uint8_t*>(up(A.type.data(), ncs));
+  D.d_code = static_cast<uint16_t*>(up(A.code.data(), ncs * sizeof(uint16_t)));
+  D.b = alloc(ncs * tsz);
+  D.x0 = alloc(ncs * tsz);
+  D.x1 = alloc(ncs * tsz);
+  NB_CUDA(cudaMemset(D.b, 0, ncs * tsz));
+  NB_CUDA(cudaMemset(D.x0, 0, ncs * tsz));
+  NB_CUDA(cudaMemset(D.x1, 0, ncs * tsz));
+  LevelView& v = D.v;
+  v = LevelView{};
+  v.amr = 1;
+  v.nbrick = nbrick;
+  v.nlev = t.nlev;
+  for (int f = 0; f < 6; ++f) v.bc[f] = bcs[f];
+  v.nx = t.cells(0, 0);
+  v.ny = t.cells(0, 1);
+  v.nz = t.cells(0, 2);
+  for (int L = 0; L < t.nlev && L < AMR_MAXLEV; ++L) {
+    v.lut_off[L] = t.lut_off[L];
+    for (int a = 0; a < 3; ++a) {
+      v.lnb[L][a] = t.lnb(L, a);
+      v.lcells[L][a] = t.cells(L, a);
+      const double h = t.h(L, a);
+      v.lh2[L][a] = 1.0 / (h * h);
+    }
   }
+  for (int a = 0; a < 3; ++a) v.dxyz[a] = t.h(0, a);
+  v.lut = D.d_lut;
+  v.bcoord = D.d_bcoord;
+  v.type = D.d_type;
+  v.code = D.d_code;
+  v.blevel = static_cast<const int8_t*>(up(A.blevel.data(), A.blevel.size()));
+  v.bweight = static_cast<const double*>(up(A.bweight.data(), A.bweight.size() * sizeof(double)));
+  v.cf_off = static_cast<const int*>(up(A.cf_off.data(), A.cf_off.size() * sizeof(int)));
+  v.cf_nbr = static_cast<const int*>(up(A.cf_nbr.data(), std::max<size_t>(1, A.cf_nbr.size()) * sizeof(int)));
+  v.cf_coef = static_cast<const double*>(
+      up(A.cf_coef.data(), std::max<size_t>(1, A.cf_coef.size()) * sizeof(double)));
+  if (!A.xf_brick.empty()) {
+    D.d_xfb = static_cast<int*>(up(A.xf_brick.data(), A.xf_brick.size() * sizeof(int)));
+    D.d_xfo = static_cast<int*>(up(A.xf_oct.data(), A.xf_oct.size() * sizeof(int)));
+    v.xf_brick = D.d_xfb;
+    v.xf_oct = D.d_xfo;
+  }
+}
+
+void MgSolver::common_alloc() {
+  const HostLevel& last = lv_.back().h;
+  if (lv_.back().v.amr || static_cast<size_t>(last.nx) * last.ny * last.nz > COARSE_MAX_CELLS)
+    throw ApiError{NB_ERR_UNSUPPORTED, "coarsest multigrid level exceeds 4096 cells"};
   n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
   double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
   for (double** v : vecs) {
@@ -847,6 +1008,81 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
   NB_CUDA(cudaFuncSetAttribute(k_coarse_cg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
 }
 
+MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
+    : precision_(precision), lc_(lc) {
+  std::vector<HostLevel> H = build_hierarchy(g);
+  singular_ = true;
+  for (int f = 0; f < 6; ++f)
+    if (g.face[f].type == NB_BC_OUTLET) singular_ = false;  // hasDirichlet, poisson.cpp:93-100
+  int bcs[6];
+  for (int f = 0; f < 6; ++f) bcs[f] = g.face[f].type;
+  lv_.resize(H.size());
+  for (size_t l = 0; l < H.size(); ++l) {
+    lv_[l].h = std::move(H[l]);
+    upload_uniform(lv_[l], bcs);
+  }
+  common_alloc();
+}
+
+// Composite hierarchy: MG level m+1 merges the finest octree level of level m
+// into its parents (cells fluid if any child is); once a single octree level
+// remains the grid is uniform and coarsens as MgPoisson does
+// (core/src/flow/multigrid.cpp:211-266).
+MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc)
+    : precision_(precision), lc_(lc) {
+  const AmrGeom& geo = fine.tree.geom;
+  singular_ = true;
+  for (int f = 0; f < 6; ++f)
+    if (geo.bc[f] == NB_BC_OUTLET) singular_ = false;
+  std::vector<AmrLevelHost> comp;
+  comp.push_back(fine);
+  while (comp.back().tree.nlev > 1) {
+    AmrLevelHost& F = comp.back();
+    AmrLevelHost C;
+    C.tree = coarsen_tree(F.tree, F.xf_brick, F.xf_oct);
+    C.wlmax = F.wlmax;
+    amr_level_geometry(C);
+    amr_level_types_coarsened(C, F);
+    amr_level_codes(C);
+    comp.push_back(std::move(C));
+  }
+  // The last composite level has one octree level: hand it to the uniform chain.
+  const AmrLevelHost& U = comp.back();
+  const int nx = U.tree.cells(0, 0), ny = U.tree.cells(0, 1), nz = U.tree.cells(0, 2);
+  std::vector<uint8_t> solid(static_cast<size_t>(nx) * ny * nz, 0);
+  for (size_t r = 0; r < U.tree.leaves.size(); ++r)
+    for (int l = 0; l < BR3; ++l) {
+      const AmrLeaf& f = U.tree.leaves[r];
+      const int i = f.b[0] * BR + (l & 7), j = f.b[1] * BR + ((l >> 3) & 7), k = f.b[2] * BR + (l >> 6);
+      solid[static_cast<size_t>(i) + static_cast<size_t>(nx) * (j + static_cast<size_t>(ny) * k)] =
+          U.type[r * BR3 + l] == CELL_SOLID;
+    }
+  nb_grid_desc g0{};
+  g0.nx = nx;
+  g0.ny = ny;
+  g0.nz = nz;
+  g0.dx = U.tree.h(0, 0);
+  g0.dy = U.tree.h(0, 1);
+  g0.dz = U.tree.h(0, 2);
+  for (int f = 0; f < 6; ++f) g0.face[f].type = geo.bc[f];
+  g0.solid = solid.data();
+  std::vector<HostLevel> H = build_hierarchy(g0);
+  // Uniform brick ranks equal the single-level tree's ranks (both Morton).
+  for (size_t r = 0; r < U.tree.leaves.size(); ++r) {
+    const AmrLeaf& f = U.tree.leaves[r];
+    if (H[0].lut[(f.b[2] * H[0].nby + f.b[1]) * H[0].nbx + f.b[0]] != static_cast<int>(r))
+      throw ApiError{NB_ERR_UNSUPPORTED, "brick ranking mismatch between composite and uniform levels"};
+  }
+  const size_t ncomp = comp.size() - 1;  // composite levels with >= 2 octree levels
+  lv_.resize(ncomp + H.size());
+  for (size_t m = 0; m < ncomp; ++m) upload_amr(lv_[m], comp[m], geo.bc);
+  for (size_t l = 0; l < H.size(); ++l) {
+    lv_[ncomp + l].h = std::move(H[l]);
+    upload_uniform(lv_[ncomp + l], geo.bc);
+  }
+  common_alloc();
+}
+
 MgSolver::~MgSolver() {
   for (void* p : allocs_) cudaFree(p);
   if (h_flags_) cudaFreeHost(h_flags_);
@@ -856,7 +1092,7 @@ MgSolver::~MgSolver() {
 
 void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
   const LevelView& L = lv_[0].v;
-  NB_LAUNCH(lc_, "apply_a", s, static_cast<double>(L.nx) * L.ny * L.nz * 17,
+  NB_LAUNCH(lc_, "apply_a", s, lv_[0].ncell * 17,
             (k_apply_a<<<grid_for(L.nbrick), NT, 0, s>>>(L, x, out)));
   NB_CUDA(cudaGetLastError());
 }
@@ -872,7 +1108,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double* bmean = (singular_ && bmean_slot >= 0) ? S_ + bmean_slot : nullptr;
   const int grid = grid_for(L.nbrick);
   const double tsz = sizeof(T);
-  const double ncell = static_cast<double>(L.nx) * L.ny * L.nz;
+  const double ncell = D.ncell;
   if (lvl + 1 == static_cast<int>(lv_.size())) {
     const size_t smem = static_cast<size_t>(L.nx) * L.ny * L.nz * (6 * sizeof(double) + 1);
     NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
@@ -882,7 +1118,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
     *out_mean_slot = -1;
     return;
   }
-  const double inv_nf = D.h.nfluid ? 1.0 / static_cast<double>(D.h.nfluid) : 0.0;
+  const double inv_nf = D.h.nfluid ? 1.0 / D.wfluid : 0.0;
   const bool sing = singular_ && D.h.nfluid > 0;
   T* xa = static_cast<T*>(D.x0);
   T* xb = static_cast<T*>(D.x1);
@@ -891,7 +1127,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const LevelView dummy = L;
   DevLevel& Cd = lv_[lvl + 1];
   const LevelView& C = Cd.v;
-  const double ncoarse = static_cast<double>(C.nx) * C.ny * C.nz;
+  const double ncoarse = Cd.ncell;
   // pre-smoothing (2 sweeps), first from x = 0
   NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
             (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean,
@@ -901,7 +1137,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
             (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
                                              xb, rb_, mB, inv_nf, flags_, maxit_)));
   // residual + restriction
-  const double inv_nfc = Cd.h.nfluid ? 1.0 / static_cast<double>(Cd.h.nfluid) : 0.0;
+  const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
   double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
   NB_LAUNCH(lc_, "resid_restrict", s, ncell * (2 * tsz + 1) + ncoarse * tsz,
@@ -917,7 +1153,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
             (k_smooth<T><<<grid, NT, 0, s>>>(
                 L, b, bmean,
-                XFetch<T>{xb, mB, static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy, Cd.h.fz}, xa, rb_,
+                XFetch<T>{xb, mB, static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy, Cd.h.fz, D.d_xfb, D.d_xfo}, xa, rb_,
                 mA, inv_nf, flags_, maxit_)));
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
             (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
@@ -931,10 +1167,10 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
 void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   const LevelView& L = lv_[0].v;
   const int grid = grid_for(L.nbrick);
-  const double inv_nf = lv_[0].h.nfluid ? 1.0 / static_cast<double>(lv_[0].h.nfluid) : 0.0;
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   const bool sing = singular_ && lv_[0].h.nfluid > 0;
   const bool mixed = precision_ == NB_PRECISION_MIXED;
-  const double n = static_cast<double>(L.nx) * L.ny * L.nz;
+  const double n = lv_[0].ncell;
   const double zsz = mixed ? 4.0 : 8.0;
   for (int k = 0; k < count; ++k) {
     NB_LAUNCH(lc_, "pcg_matvec", s, n * 17,
@@ -1035,7 +1271,7 @@ void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int ma
 void MgSolver::finish(cudaStream_t s, double* report) {
   const LevelView& L = lv_[0].v;
   const int grid = grid_for(L.nbrick);
-  const double inv_nf = lv_[0].h.nfluid ? 1.0 / static_cast<double>(lv_[0].h.nfluid) : 0.0;
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   const bool sing = singular_ && lv_[0].h.nfluid > 0;
   // final removeMean(x) + true residual (multigrid.cpp:341-353)
   if (sing) {
@@ -1071,7 +1307,7 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit) {
   maxit_ = maxit;
   const LevelView& L = lv_[0].v;
   const int grid = grid_for(L.nbrick);
-  const double inv_nf = lv_[0].h.nfluid ? 1.0 / static_cast<double>(lv_[0].h.nfluid) : 0.0;
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   const bool sing = singular_ && lv_[0].h.nfluid > 0;
   const bool mixed = precision_ == NB_PRECISION_MIXED;
   // rhs = b masked (+ mean removal), r = rhs, x = 0, bnorm, early exit

@@ -12,6 +12,7 @@
 #include <memory>
 #include <vector>
 
+#include "nb_amr_level.h"
 #include "nb_internal.h"
 
 namespace nb {
@@ -23,6 +24,10 @@ struct DevLevel {
   int* d_bcoord = nullptr;
   uint8_t* d_type = nullptr;
   uint16_t* d_code = nullptr;
+  int* d_xfb = nullptr;  // composite levels: transfer maps to the next level
+  int* d_xfo = nullptr;
+  double wfluid = 0.0;   // fluid volume in cell-weight units (= fluid cells on uniform levels)
+  double ncell = 0.0;    // cells of the level (for algorithmic byte counts)
   // V-cycle vectors in the level's arithmetic type (double or float):
   // b (restricted residual), x ping, x pong.
   void* b = nullptr;
@@ -33,6 +38,9 @@ struct DevLevel {
 class MgSolver {
  public:
   MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc);
+  // Composite (octree-AMR) operator on the leaves of `fine` (types and codes
+  // already built), with the composite-then-uniform MG hierarchy.
+  MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc);
   ~MgSolver();
   MgSolver(const MgSolver&) = delete;
   MgSolver& operator=(const MgSolver&) = delete;
@@ -81,6 +89,9 @@ class MgSolver {
   void iterate(cudaStream_t s, double tol, int maxit, int count);
   void setup(cudaStream_t s, const double* b, double tol, int maxit);
   void finish(cudaStream_t s, double* report);
+  void upload_uniform(DevLevel& D, const int bcs[6]);
+  void upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]);
+  void common_alloc();
   void* alloc(size_t bytes);
   cudaStream_t side_ = nullptr;               // capture stream of the loop body
   unsigned long long* body_execs_ = nullptr;  // device counter

@@ -101,6 +101,16 @@ class PoissonReport(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("residual", C.c_double)]
 
 
+class AmrGeom(C.Structure):
+    _fields_ = [
+        ("nb0", C.c_int32 * 3),
+        ("lmax", C.c_int32),
+        ("h0", C.c_double * 3),
+        ("origin", C.c_double * 3),
+        ("face", FaceBC * 6),
+    ]
+
+
 DP = C.POINTER(C.c_double)
 VP = C.c_void_p
 
@@ -139,6 +149,15 @@ PROTOTYPES = [
                                    C.POINTER(PoissonReport)]),
     ("nb_apply_laplacian", C.c_int, [VP, C.POINTER(GridDesc), DP, DP]),
     ("nb_apply_laplacian_noalloc", C.c_int, [C.POINTER(GridDesc), VP, VP, VP]),
+    ("nb_amr_refine", C.c_int, [C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_uint8),
+                                C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
+    ("nb_amr_mesh_create", C.c_int, [VP, C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64,
+                                     C.POINTER(C.c_uint8), C.POINTER(VP)]),
+    ("nb_amr_mesh_destroy", None, [VP]),
+    ("nb_amr_mesh_leaf_count", C.c_int64, [VP]),
+    ("nb_amr_mesh_leaves", C.c_int, [VP, C.POINTER(C.c_int32)]),
+    ("nb_amr_apply_laplacian", C.c_int, [VP, VP, DP, DP]),
+    ("nb_amr_poisson_solve", C.c_int, [VP, VP, DP, DP, C.c_double, C.c_int, C.c_int, C.POINTER(PoissonReport)]),
 ]
 
 

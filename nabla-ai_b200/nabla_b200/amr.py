@@ -1,0 +1,128 @@
+"""Octree-AMR brick meshes over the C ABI (nb_amr_*).
+
+A leaf is (level, bx, by, bz): a brick of 8x8x8 cells at octree level
+`level`, brick coordinates in that level's brick grid. Cell arrays over a
+mesh are nleaf*512 float64 in the mesh's rank order (Morton order of the
+leaf anchors on the finest level), x fastest inside a brick.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .solver import Context, NablaError, Report, default_context
+
+
+def make_geom(nb0, h0, lmax, faces, origin=(0.0, 0.0, 0.0)) -> abi.AmrGeom:
+    g = abi.AmrGeom()
+    g.nb0[:] = list(nb0)
+    g.h0[:] = list(h0)
+    g.origin[:] = list(origin)
+    g.lmax = lmax
+    for f in range(6):
+        spec = faces[f]
+        g.face[f].type = spec.get("type", abi.BC_WALL)
+        g.face[f].profile = spec.get("profile", abi.PROFILE_UNIFORM)
+        g.face[f].inlet_axis = spec.get("inlet_axis", 0)
+        g.face[f].inlet_speed = spec.get("inlet_speed", 0.0)
+        g.face[f].wall_velocity[:] = list(spec.get("wall_velocity", (0.0, 0.0, 0.0)))
+    return g
+
+
+def base_leaves(nb0) -> np.ndarray:
+    z, y, x = np.meshgrid(np.arange(nb0[2]), np.arange(nb0[1]), np.arange(nb0[0]), indexing="ij")
+    n = x.size
+    return np.stack([np.zeros(n, dtype=np.int32), x.ravel(), y.ravel(), z.ravel()], axis=1).astype(np.int32)
+
+
+def refine(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray) -> np.ndarray:
+    """Split flagged leaves and restore 26-neighbour 2:1 balance (host maps)."""
+    lib = abi.load()
+    leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+    flags = np.ascontiguousarray(flags, dtype=np.uint8)
+    n = leaves.shape[0]
+    need = C.c_int64()
+    cap = max(8 * n, 64)
+    while True:
+        out = np.zeros((cap, 4), dtype=np.int32)
+        st = lib.nb_amr_refine(C.byref(geom), leaves.ctypes.data_as(C.POINTER(C.c_int32)), n,
+                               flags.ctypes.data_as(C.POINTER(C.c_uint8)),
+                               out.ctypes.data_as(C.POINTER(C.c_int32)), cap, C.byref(need))
+        if st == abi.NB_OK:
+            return out[:need.value].copy()
+        if need.value > cap:
+            cap = need.value
+            continue
+        raise NablaError(st, "nb_amr_refine failed")
+
+
+def cell_coords(leaves: np.ndarray):
+    """(level, i, j, k) of every cell, leaves x 512, in array order."""
+    l = np.arange(512)
+    li, lj, lk = l & 7, (l >> 3) & 7, l >> 6
+    lev = np.repeat(leaves[:, 0], 512)
+    i = (leaves[:, 1:2] * 8 + li[None, :]).ravel()
+    j = (leaves[:, 2:3] * 8 + lj[None, :]).ravel()
+    k = (leaves[:, 3:4] * 8 + lk[None, :]).ravel()
+    return lev, i, j, k
+
+
+class AmrMesh:
+    def __init__(self, geom: abi.AmrGeom, leaves: np.ndarray, solid: np.ndarray | None = None,
+                 ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.geom = geom
+        leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+        sp = None
+        if solid is not None:
+            solid = np.ascontiguousarray(solid, dtype=np.uint8)
+            sp = solid.ctypes.data_as(C.POINTER(C.c_uint8))
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.nb_amr_mesh_create(self.ctx.h, C.byref(geom),
+                                                       leaves.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                       leaves.shape[0], sp, C.byref(h)), "nb_amr_mesh_create")
+        self.h = h
+        n = self.ctx.lib.nb_amr_mesh_leaf_count(h)
+        self.leaves = np.zeros((n, 4), dtype=np.int32)
+        self.ctx.lib.nb_amr_mesh_leaves(h, self.leaves.ctypes.data_as(C.POINTER(C.c_int32)))
+
+    @property
+    def ncell(self) -> int:
+        return self.leaves.shape[0] * 512
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.nb_amr_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def cell_size(self):
+        """Per-cell (hx, hy, hz) arrays."""
+        lev = np.repeat(self.leaves[:, 0], 512)
+        return tuple(self.geom.h0[a] / (2.0 ** lev) for a in range(3))
+
+    def cell_centers(self):
+        lev, i, j, k = cell_coords(self.leaves)
+        hx, hy, hz = self.cell_size()
+        o = self.geom.origin
+        return o[0] + (i + 0.5) * hx, o[1] + (j + 0.5) * hy, o[2] + (k + 0.5) * hz
+
+    def apply_a(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros(self.ncell)
+        self.ctx.check(self.ctx.lib.nb_amr_apply_laplacian(self.ctx.h, self.h, abi.dptr(x), abi.dptr(out)),
+                       "nb_amr_apply_laplacian")
+        return out
+
+    def solve(self, b: np.ndarray, tol=1e-10, max_cycles=200, precision=abi.PRECISION_FP64):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.ncell)
+        rep = abi.PoissonReport()
+        self.ctx.check(self.ctx.lib.nb_amr_poisson_solve(self.ctx.h, self.h, abi.dptr(b), abi.dptr(x), tol,
+                                                         max_cycles, precision, C.byref(rep)),
+                       "nb_amr_poisson_solve")
+        return x, Report(rep.iterations, rep.residual, bool(rep.converged))
