@@ -22,6 +22,7 @@ from nabla_b200 import abi  # noqa: E402  (struct layouts shared with the C ABI 
 
 ORC_PATH = os.path.join(HERE, "_build", "liborc.so")
 REF_PATH = os.path.join(HERE, "_ref", "libnabla_ref.so")
+DROPIN_PATH = os.path.join(HERE, "_ref", "libnabla_dropin.so")
 
 GP = C.POINTER(abi.GridDesc)
 FP = C.POINTER(abi.FlowConfig)
@@ -262,3 +263,40 @@ class _NS:
         rep = abi.StepReport()
         getattr(self.lib, f"{self.p}_ns_step")(self.h, dt, C.byref(rep))
         return rep
+
+
+class Dropin:
+    """The reference's own NSSolver / PoissonSolver seams with the B200 library
+    plugged in (oracle/_ref/libnabla_dropin.so, built from oracle/dropin_shim.cpp
+    and nabla-ai_b200/integration/nabla_flow_cuda.hpp). Modes: 0 the reference's
+    CPU MgPoisson, 1 CudaMgPoisson inside the reference NSSolver, 2 CudaNSSolver."""
+
+    def __init__(self, path=DROPIN_PATH):
+        L = self.lib = _load(path)
+        L.dropin_last_error.restype = C.c_char_p
+        L.dropin_run.argtypes = [GP, FP, C.c_int, C.c_int, C.c_double, DP, DP, DP, DP,
+                                 C.POINTER(C.c_int), DP]
+        L.dropin_poisson.argtypes = [GP, DP, DP, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                     DP, C.POINTER(C.c_int)]
+
+    def run(self, grid, cfg, mode, state, nsteps, dt=0.0):
+        gd = grid.desc()
+        out = [np.array(a, dtype=np.float64, copy=True) for a in state]
+        iters = (C.c_int * nsteps)()
+        dts = np.zeros(nsteps)
+        st = self.lib.dropin_run(C.byref(gd), C.byref(cfg), mode, nsteps, dt,
+                                 *[abi.dptr(a) for a in out], iters, abi.dptr(dts))
+        if st != 0:
+            raise RuntimeError(self.lib.dropin_last_error().decode())
+        return out, list(iters), dts
+
+    def poisson(self, grid, b, tol, max_cycles, mode):
+        gd = grid.desc()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        it, res, conv = C.c_int(), C.c_double(), C.c_int()
+        st = self.lib.dropin_poisson(C.byref(gd), abi.dptr(b), abi.dptr(x), tol, max_cycles, mode,
+                                     C.byref(it), C.byref(res), C.byref(conv))
+        if st != 0:
+            raise RuntimeError(self.lib.dropin_last_error().decode())
+        return x, it.value, res.value, bool(conv.value)

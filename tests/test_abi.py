@@ -47,3 +47,20 @@ def test_library_links_no_oracle():
     out = subprocess.run(["ldd", abi.LIB_PATH], capture_output=True, text=True).stdout
     assert "orc" not in out and "nabla_ref" not in out
     assert os.path.basename(abi.LIB_PATH) == "libnabla_b200.so"
+
+
+def test_cpp_header_compiles_against_c_abi(tmp_path):
+    """include/nabla_b200.hpp (the C++20 host API) compiles and links against the library."""
+    import subprocess
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "use.cpp"
+    src.write_text('#include "nabla_b200.hpp"\n'
+                   'int main() { try { auto c = std::make_shared<nabla_b200::Context>(0);'
+                   ' nabla_b200::MgPoisson mg(c); return mg.name().empty(); }'
+                   ' catch (const nabla_b200::Error& e) { return e.status() == NB_ERR_CUDA ? 0 : 2; } }\n')
+    exe = tmp_path / "use"
+    r = subprocess.run(["g++", "-std=c++20", "-I", os.path.join(repo, "include"), str(src), "-o", str(exe),
+                        "-L", os.path.dirname(abi.LIB_PATH), "-lnabla_b200",
+                        "-Wl,-rpath," + os.path.dirname(abi.LIB_PATH)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([str(exe)]).returncode == 0
