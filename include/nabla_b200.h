@@ -211,6 +211,31 @@ nb_status nb_amr_apply_laplacian(nb_ctx* ctx, nb_amr_mesh* m, const double* x, d
 nb_status nb_amr_poisson_solve(nb_ctx* ctx, nb_amr_mesh* m, const double* b, double* x, double tol,
                                int max_cycles, int precision, nb_poisson_report* rep);
 
+/* ---- MAC step on an octree-AMR mesh ------------------------------------------
+ * NSSolver (core/include/nabla/flow/ns_solver.hpp:58-96) on the composite
+ * mesh: the same SSP-RK3 / WENO-5 / MG-PCG step, with the octree face rule of
+ * OctreePoisson (core/src/flow/octree_poisson.cpp:24-32) at 2:1 interfaces.
+ * The returned case is driven by nb_case_initialize, nb_case_compute_dt,
+ * nb_step, nb_step_many, nb_case_destroy; the mesh must outlive it. BCs come
+ * from the mesh geometry's faces.
+ * Face storage of component a (0 u, 1 v, 2 w): nbrick*512 + nslab*64 doubles.
+ * Slot r*512 + l is the low a-face of cell l of leaf r; slab s holds the 64
+ * high a-faces (local index a-th coordinate 8, the other two x-fastest) of
+ * leaf slabs[s] (nb_amr_case_slabs). A leaf has an a-slab iff its +a
+ * neighbour is not a same-level leaf. On periodic axes the domain high face
+ * is the low face of the first cell (no second copy). At a 2:1 interface the
+ * fine side's four sub-faces are the state; the coarse face is their average
+ * (overwritten on every update). Pressure: nbrick*512 cell values. */
+nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* m, const nb_flow_config* cfg, int precision,
+                             nb_case** out);
+/* sizes[0..2] = face storage lengths of u, v, w; sizes[3] = cells. */
+nb_status nb_amr_case_sizes(const nb_case* c, int64_t sizes[4]);
+/* Leaf rank of every a-slab, in slab order ((sizes[a] - cells) / 64 values). */
+nb_status nb_amr_case_slabs(const nb_case* c, int axis, int32_t* bricks);
+nb_status nb_amr_case_set_state(nb_case* c, const double* u, const double* v, const double* w, const double* p);
+/* Any pointer may be NULL to skip that field. */
+nb_status nb_amr_case_get_state(nb_case* c, double* u, double* v, double* w, double* p);
+
 /* ---- allocation-free operator ---------------------------------------------
  * No counterpart in the reference. The same -Laplacian as nb_apply_laplacian,
  * for callers that cannot call cudaMalloc: code issuing work while a stream is

@@ -1,0 +1,654 @@
+// nb_amr_flow.cu — sm_100a kernels of the MAC step on octree-AMR bricks.
+//
+// The multi-level step generalises the uniform one (core/src/flow/ns_solver.cpp)
+// by the conservative face rule of the octree Poisson operator
+// (core/src/flow/octree_poisson.cpp:24-32): the fine side of a 2:1 interface
+// owns the four sub-faces; the coarse face is their average; the projection
+// corrects a sub-face with the gradient over the true centre distance 1.5 h.
+// WENO halos across a level jump come from the neighbour level: a fine ghost
+// face inside a coarse cell is the linear interpolation of the coarse cell's
+// two faces along the normal (constant across), a coarse ghost face is the
+// average of its four fine sub-faces; the scheme is locally lower order at
+// the interface (the policy of docs/adr/0008-octree-native-flow-solve.md:58-62).
+// On a single-level mesh every formula reduces to the uniform reference step.
+//
+// Every kernel walks bricks with a grid-stride loop and cells with a
+// block-stride loop, so any launch shape covers the mesh.
+#include <algorithm>
+#include <cmath>
+
+#include "nb_amr_flow.cuh"
+#include "nb_momentum.cuh"
+#include "nb_reduce.cuh"
+
+namespace nb {
+
+namespace {
+
+constexpr int NT = 512;
+constexpr int MAX_GRID = 148 * 4;
+constexpr int RHS_NT = 256;
+constexpr int TW = 15;  // tile offsets -3 .. 11: the brick, its high face layer, 3 ghosts each side
+constexpr int TN = TW * TW * TW;
+constexpr int8_t R_SAME = 0, R_COARSER = 1, R_FINER = 2, R_BOUNDARY = 3;
+constexpr int ACC_MAX = 16;
+
+inline int grid_for(int nbrick) { return nbrick < MAX_GRID ? nbrick : MAX_GRID; }
+
+__device__ __forceinline__ int slab_local(int a, int li, int lj, int lk) {
+  return a == 0 ? lj + 8 * lk : (a == 1 ? li + 8 * lk : li + 8 * lj);
+}
+__device__ __forceinline__ int local_of(const int p[3]) {
+  return ((p[2] & 7) << 6) | ((p[1] & 7) << 3) | (p[0] & 7);
+}
+__device__ __forceinline__ int tix(int a, int b, int c) { return ((c + 3) * TW + (b + 3)) * TW + (a + 3); }
+
+// Leaf rank at level-`lev` brick coordinates (x, y, z), or -1 (no leaf, or
+// level/coordinates outside the mesh).
+__device__ __forceinline__ int lut_at(const LevelView& L, int lev, int x, int y, int z) {
+  if (lev < 0 || lev >= L.nlev) return -1;
+  if (x < 0 || y < 0 || z < 0 || x >= L.lnb[lev][0] || y >= L.lnb[lev][1] || z >= L.lnb[lev][2]) return -1;
+  return L.lut[L.lut_off[lev] + (z * L.lnb[lev][1] + y) * L.lnb[lev][0] + x];
+}
+
+// Leaf containing in-domain level-`lev0` cell p and its level (lev0 - 1,
+// lev0 or lev0 + 1 on a balanced mesh); -1 if none.
+__device__ __forceinline__ int leaf_of(const LevelView& L, int lev0, const int p[3], int& lev) {
+  int r = lut_at(L, lev0, p[0] >> 3, p[1] >> 3, p[2] >> 3);
+  if (r >= 0) {
+    lev = lev0;
+    return r;
+  }
+  r = lut_at(L, lev0 - 1, p[0] >> 4, p[1] >> 4, p[2] >> 4);
+  if (r >= 0) {
+    lev = lev0 - 1;
+    return r;
+  }
+  r = lut_at(L, lev0 + 1, p[0] >> 2, p[1] >> 2, p[2] >> 2);
+  lev = r >= 0 ? lev0 + 1 : -1;
+  return r;
+}
+
+// Stored a-face at a face position of level `lev0`: p[a] in [0, N_a], the
+// other coordinates in-domain. Reads the owner: the minus-side cell's slab
+// when that cell is at lev0 and has one (domain high faces, coarse-fine
+// sub-faces owned by the fine side), else the plus-side cell's low face
+// (same level), the average of its four sub-faces (plus side finer), or the
+// coarse face containing it (plus side coarser; p[a] even there).
+__device__ double face_at(const AmrFlowView& F, int a, const double* __restrict__ f, int lev0, const int p0[3]) {
+  const LevelView& L = F.L;
+  const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
+  const int N = L.lcells[lev0][a];
+  int p[3] = {p0[0], p0[1], p0[2]};
+  if (F.per[a] && p[a] >= N) p[a] -= N;
+  const bool has_plus = p[a] < N;
+  int m[3] = {p[0], p[1], p[2]};
+  m[a] -= 1;
+  bool has_minus = true;
+  if (m[a] < 0) {
+    if (F.per[a]) m[a] += N;
+    else has_minus = false;
+  }
+  if (has_minus) {
+    int lm;
+    const int rm = leaf_of(L, lev0, m, lm);
+    if (rm >= 0 && (m[a] & 7) == 7) {
+      const int sid = F.slab_id[3 * rm + a];
+      if (lm == lev0 && sid >= 0) return f[F.nb + sid * 64LL + slab_local(a, m[0] & 7, m[1] & 7, m[2] & 7)];
+      if (!has_plus && lm == lev0 + 1 && sid >= 0) {  // domain high face over finer cells
+        double s = 0.0;
+        for (int d2 = 0; d2 < 2; ++d2)
+          for (int d1 = 0; d1 < 2; ++d1) {
+            int c[3];
+            c[a] = 2 * m[a] + 1;
+            c[t1] = 2 * m[t1] + d1;
+            c[t2] = 2 * m[t2] + d2;
+            s += f[F.nb + sid * 64LL + slab_local(a, c[0] & 7, c[1] & 7, c[2] & 7)];
+          }
+        return 0.25 * s;
+      }
+    }
+    if (!has_plus && rm >= 0 && lm == lev0 - 1) {  // domain high face over a coarser cell
+      const int c[3] = {m[0] >> 1, m[1] >> 1, m[2] >> 1};
+      const int sid = F.slab_id[3 * rm + a];
+      if (sid >= 0) return f[F.nb + sid * 64LL + slab_local(a, c[0] & 7, c[1] & 7, c[2] & 7)];
+    }
+  }
+  if (!has_plus) return 0.0;
+  int lp;
+  const int rp = leaf_of(L, lev0, p, lp);
+  if (rp < 0) return 0.0;
+  if (lp == lev0) return f[rp * static_cast<long long>(BR3) + local_of(p)];
+  if (lp == lev0 + 1) {
+    double s = 0.0;
+    for (int d2 = 0; d2 < 2; ++d2)
+      for (int d1 = 0; d1 < 2; ++d1) {
+        int c[3];
+        c[a] = 2 * p[a];
+        c[t1] = 2 * p[t1] + d1;
+        c[t2] = 2 * p[t2] + d2;
+        s += f[rp * static_cast<long long>(BR3) + local_of(c)];
+      }
+    return 0.25 * s;
+  }
+  const int c[3] = {p[0] >> 1, p[1] >> 1, p[2] >> 1};  // coarser: the coarse cell's low face
+  return f[rp * static_cast<long long>(BR3) + local_of(c)];
+}
+
+// a-face value at level `lev0` position p, including the positions that fall
+// mid-cell inside a coarser leaf (linear interpolation along the normal).
+__device__ double face_read(const AmrFlowView& F, int a, const double* __restrict__ f, int lev0, const int p[3]) {
+  const int N = F.L.lcells[lev0][a];
+  if ((p[a] & 1) && p[a] < N && lev0 >= 1) {
+    int lev;
+    const int r = leaf_of(F.L, lev0, p, lev);
+    if (r >= 0 && lev == lev0 - 1) {
+      int q[3] = {p[0] >> 1, p[1] >> 1, p[2] >> 1};
+      const double lo = face_at(F, a, f, lev0 - 1, q);
+      q[a] += 1;
+      const double hi = face_at(F, a, f, lev0 - 1, q);
+      return 0.5 * (lo + hi);
+    }
+  }
+  return face_at(F, a, f, lev0, p);
+}
+
+__device__ __forceinline__ double inlet_amr(const AmrFlowView& F, int face, int lev, int jidx, int comp) {
+  double mag = F.inlet_speed[face];
+  if (F.profile[face] == NB_PROFILE_PARABOLIC) {
+    const double dy = F.h[lev][1];
+    const double H = F.L.lcells[lev][1] * dy;
+    const double yc = F.origin[1] + 0.5 * H;
+    const double y = F.origin[1] + (jidx + 0.5) * dy;
+    const double r = (y - yc) / (0.5 * H);
+    mag = 1.5 * F.inlet_speed[face] * (1.0 - r * r);
+  }
+  return F.inlet_axis[face] == comp ? mag : 0.0;
+}
+
+// Ghost accessors U / Vv / W (core/src/flow/ns_solver.cpp:116-219) at level
+// `lev`: domain rules first (wrap, wall reflection 2 u_w - u_m, reflection
+// about the stored boundary face 2 u_b - u_r, outlet copy, inlet value), then
+// the level-aware face read. The constants of the reference's nested
+// expressions c0 - (c1 - (... - term)) are unwound innermost-first.
+__device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restrict__ f, int lev, int i, int j,
+                          int k) {
+  const int nx = F.L.lcells[lev][0], ny = F.L.lcells[lev][1], nz = F.L.lcells[lev][2];
+  double cst[ACC_MAX];
+  int d = 0;
+  double term = 0.0;
+  for (int guard = 0; guard < ACC_MAX; ++guard) {
+    if (comp == 0) {
+      if (k < 0 || k >= nz) {
+        if (F.per[2]) { k = wrapi(k, nz); continue; }
+        const int face = k < 0 ? 4 : 5;
+        cst[d++] = 2.0 * F.wallv[face][0];
+        k = k < 0 ? (-1 - k) : (2 * nz - 1 - k);
+        continue;
+      }
+      if (j < 0 || j >= ny) {
+        if (F.per[1]) { j = wrapi(j, ny); continue; }
+        const int face = j < 0 ? 2 : 3;
+        cst[d++] = 2.0 * F.wallv[face][0];
+        j = j < 0 ? (-1 - j) : (2 * ny - 1 - j);
+        continue;
+      }
+      if (i < 0 || i > nx) {
+        if (F.per[0]) { i = wrapi(i, nx); continue; }
+        const int ib = i < 0 ? 0 : nx, face = i < 0 ? 0 : 1;
+        const int pb[3] = {ib, j, k};
+        if (F.L.bc[face] == NB_BC_OUTLET) { term = face_read(F, 0, f, lev, pb); break; }
+        cst[d++] = 2.0 * face_read(F, 0, f, lev, pb);
+        i = 2 * ib - i;
+        continue;
+      }
+    } else if (comp == 1) {
+      if (k < 0 || k >= nz) {
+        if (F.per[2]) { k = wrapi(k, nz); continue; }
+        const int face = k < 0 ? 4 : 5;
+        cst[d++] = 2.0 * F.wallv[face][1];
+        k = k < 0 ? (-1 - k) : (2 * nz - 1 - k);
+        continue;
+      }
+      if (i < 0 || i >= nx) {
+        if (F.per[0]) { i = wrapi(i, nx); continue; }
+        const int im = i < 0 ? (-1 - i) : (2 * nx - 1 - i), face = i < 0 ? 0 : 1;
+        if (F.L.bc[face] == NB_BC_INLET) {
+          cst[d++] = 2.0 * inlet_amr(F, face, lev, j, 1);
+          i = im;
+          continue;
+        }
+        if (F.L.bc[face] == NB_BC_OUTLET) {
+          // j is unresolved here; stencil points have it in range, the clamp
+          // keeps unused corner points in bounds.
+          const int pb[3] = {i < 0 ? 0 : nx - 1, min(max(j, 0), ny), k};
+          term = face_read(F, 1, f, lev, pb);
+          break;
+        }
+        cst[d++] = 2.0 * F.wallv[face][1];
+        i = im;
+        continue;
+      }
+      if (j < 0 || j > ny) {
+        if (F.per[1]) { j = wrapi(j, ny); continue; }
+        const int jb = j < 0 ? 0 : ny, face = j < 0 ? 2 : 3;
+        const int pb[3] = {i, jb, k};
+        if (F.L.bc[face] == NB_BC_OUTLET) { term = face_read(F, 1, f, lev, pb); break; }
+        cst[d++] = 2.0 * face_read(F, 1, f, lev, pb);
+        j = 2 * jb - j;
+        continue;
+      }
+    } else {
+      if (j < 0 || j >= ny) {
+        if (F.per[1]) { j = wrapi(j, ny); continue; }
+        const int face = j < 0 ? 2 : 3;
+        cst[d++] = 2.0 * F.wallv[face][2];
+        j = j < 0 ? (-1 - j) : (2 * ny - 1 - j);
+        continue;
+      }
+      if (i < 0 || i >= nx) {
+        if (F.per[0]) { i = wrapi(i, nx); continue; }
+        const int im = i < 0 ? (-1 - i) : (2 * nx - 1 - i), face = i < 0 ? 0 : 1;
+        if (F.L.bc[face] == NB_BC_OUTLET) {
+          const int pb[3] = {i < 0 ? 0 : nx - 1, j, min(max(k, 0), nz)};
+          term = face_read(F, 2, f, lev, pb);
+          break;
+        }
+        cst[d++] = 2.0 * F.wallv[face][2];
+        i = im;
+        continue;
+      }
+      if (k < 0 || k > nz) {
+        if (F.per[2]) { k = wrapi(k, nz); continue; }
+        const int kb = k < 0 ? 0 : nz;
+        const int pb[3] = {i, j, kb};
+        cst[d++] = 2.0 * face_read(F, 2, f, lev, pb);
+        k = 2 * kb - k;
+        continue;
+      }
+    }
+    const int pt[3] = {i, j, k};
+    term = face_read(F, comp, f, lev, pt);
+    break;
+  }
+  for (int q = d - 1; q >= 0; --q) term = cst[q] - term;
+  return term;
+}
+
+// Solid flag of the level-`lev0` cell p (outside the domain: not solid).
+__device__ __forceinline__ bool solid_at(const AmrFlowView& F, int lev0, const int p0[3]) {
+  int p[3] = {p0[0], p0[1], p0[2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int n = F.L.lcells[lev0][a];
+    if (p[a] < 0 || p[a] >= n) {
+      if (!F.per[a]) return false;
+      p[a] = wrapi(p[a], n);
+    }
+  }
+  int lev;
+  const int r = leaf_of(F.L, lev0, p, lev);
+  if (r < 0) return false;
+  int q[3] = {p[0], p[1], p[2]};
+  if (lev == lev0 - 1)
+    for (int d = 0; d < 3; ++d) q[d] >>= 1;
+  if (lev == lev0 + 1)
+    for (int d = 0; d < 3; ++d) q[d] <<= 1;
+  return F.L.type[r * static_cast<long long>(BR3) + local_of(q)] == CELL_SOLID;
+}
+
+template <typename T>
+struct TileRef {
+  const T* t;
+  __device__ __forceinline__ T operator()(int i, int j, int k) const { return t[tix(i, j, k)]; }
+};
+
+// ---------------------------------------------------------------------------
+// Fused momentum RHS + SSP-RK3 combine on AMR bricks (owned faces only).
+// One CTA per brick (grid-stride): stage u, v, w at the brick's level over
+// offsets -3..11 in shared memory, then every owned face of the brick (low
+// faces, plus the high slab faces it owns at a coarser neighbour) gets
+// R = -div(u u) + nu lap u + f and the stage combination. R = 0 on domain
+// boundary faces (ns_solver.cpp:325, even when periodic) and on faces touching
+// a solid.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(RHS_NT) k_amr_rhs_rk(AmrFlowView F, int stage, const double* __restrict__ dtp,
+                                                       const double* __restrict__ u, const double* __restrict__ v,
+                                                       const double* __restrict__ w, const double* __restrict__ u0,
+                                                       const double* __restrict__ v0, const double* __restrict__ w0,
+                                                       double* __restrict__ uo, double* __restrict__ vo,
+                                                       double* __restrict__ wo) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* tile[3];
+  tile[0] = reinterpret_cast<T*>(smraw);
+  tile[1] = tile[0] + TN;
+  tile[2] = tile[1] + TN;
+  const LevelView& L = F.L;
+  const double dt = *dtp;
+  const double c1 = 1.0 / 3.0, c2 = 2.0 / 3.0;
+  auto comb = [&](double a0, double a, double r) -> double {
+    if (stage == 1) return a0 + dt * r;
+    if (stage == 2) return 0.75 * a0 + 0.25 * (a + dt * r);
+    return c1 * a0 + c2 * (a + dt * r);
+  };
+  const double* in[3] = {u, v, w};
+  const double* in0[3] = {u0, v0, w0};
+  double* out[3] = {uo, vo, wo};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int lev = L.blevel[brick];
+    const int o[3] = {L.bcoord[3 * brick] * BR, L.bcoord[3 * brick + 1] * BR, L.bcoord[3 * brick + 2] * BR};
+    for (int p = threadIdx.x; p < TN; p += blockDim.x) {
+      const int ti = p % TW - 3, tj = (p / TW) % TW - 3, tk = p / (TW * TW) - 3;
+      const int far = (ti < -1 || ti > 9) + (tj < -1 || tj > 9) + (tk < -1 || tk > 9);
+      if (far > 1) continue;  // never read by a stencil
+      const bool inner = ti >= 0 && ti < 8 && tj >= 0 && tj < 8 && tk >= 0 && tk < 8;
+      for (int a = 0; a < 3; ++a) {
+        double val;
+        if (inner) val = in[a][brick * static_cast<long long>(BR3) + ((tk << 6) | (tj << 3) | ti)];
+        else val = amr_acc(F, a, in[a], lev, o[0] + ti, o[1] + tj, o[2] + tk);
+        tile[a][p] = static_cast<T>(val);
+      }
+    }
+    __syncthreads();
+    const T dx = T(F.h[lev][0]), dy = T(F.h[lev][1]), dz = T(F.h[lev][2]);
+    const T nu = T(F.nu);
+    const TileRef<T> TU{tile[0]}, TV{tile[1]}, TWW{tile[2]};
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      const int p[3] = {o[0] + loc[0], o[1] + loc[1], o[2] + loc[2]};
+      const long long c = brick * static_cast<long long>(BR3) + l;
+      const bool sc = L.type[c] == CELL_SOLID;
+      for (int a = 0; a < 3; ++a) {
+        const int stride = a == 0 ? 1 : (a == 1 ? 8 : 64);
+        const T bf = T(F.bf[a]);
+        // low face (derived when the -a side is finer: synced afterwards)
+        if (!(loc[a] == 0 && F.rel_lo[3 * brick + a] == R_FINER)) {
+          double r = 0.0;
+          if (p[a] != 0 && !sc) {
+            bool sn;
+            if (loc[a] > 0) {
+              sn = L.type[c - stride] == CELL_SOLID;
+            } else {
+              int q[3] = {p[0], p[1], p[2]};
+              q[a] -= 1;
+              sn = solid_at(F, lev, q);
+            }
+            if (!sn)
+              r = static_cast<double>(a == 0   ? rhs_u<T>(TU, TV, TWW, loc[0], loc[1], loc[2], F.weno, dx, dy, dz, nu, bf)
+                                      : a == 1 ? rhs_v<T>(TU, TV, TWW, loc[0], loc[1], loc[2], F.weno, dx, dy, dz, nu, bf)
+                                               : rhs_w<T>(TU, TV, TWW, loc[0], loc[1], loc[2], F.weno, dx, dy, dz, nu, bf));
+          }
+          out[a][c] = comb(in0[a][c], in[a][c], r);
+        }
+        // high slab face: owned at a coarser neighbour (RHS) or the domain boundary (R = 0)
+        const int sid = F.slab_id[3 * brick + a];
+        if (loc[a] == 7 && sid >= 0 && F.rel_hi[3 * brick + a] != R_FINER) {
+          const long long s = F.nb + sid * 64LL + slab_local(a, loc[0], loc[1], loc[2]);
+          double r = 0.0;
+          if (F.rel_hi[3 * brick + a] == R_COARSER && !sc) {
+            int q[3] = {p[0], p[1], p[2]};
+            q[a] += 1;
+            if (!solid_at(F, lev, q)) {
+              int e[3] = {loc[0], loc[1], loc[2]};
+              e[a] = 8;
+              r = static_cast<double>(a == 0   ? rhs_u<T>(TU, TV, TWW, e[0], e[1], e[2], F.weno, dx, dy, dz, nu, bf)
+                                      : a == 1 ? rhs_v<T>(TU, TV, TWW, e[0], e[1], e[2], F.weno, dx, dy, dz, nu, bf)
+                                               : rhs_w<T>(TU, TV, TWW, e[0], e[1], e[2], F.weno, dx, dy, dz, nu, bf));
+            }
+          }
+          out[a][s] = comb(in0[a][s], in[a][s], r);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Derived coarse faces = average of their four fine sub-faces.
+__global__ void k_amr_sync(const long long* __restrict__ list, int n, double* __restrict__ f) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    const long long* e = list + 5 * static_cast<long long>(m);
+    f[e[0]] = 0.25 * (((f[e[1]] + f[e[2]]) + f[e[3]]) + f[e[4]]);
+  }
+}
+
+// High a-face of brick-local cell l: next cell's low face, the brick's slab,
+// or the same-level +a neighbour's low face.
+__device__ __forceinline__ double hi_face(const AmrFlowView& F, int a, const double* __restrict__ f, int brick,
+                                          int l, const int loc[3]) {
+  if (loc[a] < 7) return f[brick * static_cast<long long>(BR3) + l + (a == 0 ? 1 : (a == 1 ? 8 : 64))];
+  const int sid = F.slab_id[3 * brick + a];
+  if (sid >= 0) return f[F.nb + sid * 64LL + slab_local(a, loc[0], loc[1], loc[2])];
+  const int nb = F.nbr_hi[3 * brick + a];
+  if (nb < 0) return 0.0;
+  int e[3] = {loc[0], loc[1], loc[2]};
+  e[a] = 0;
+  return f[nb * static_cast<long long>(BR3) + ((e[2] << 6) | (e[1] << 3) | e[0])];
+}
+
+__device__ __forceinline__ double cell_div(const AmrFlowView& F, const double* u, const double* v, const double* w,
+                                           int brick, int l, int lev) {
+  const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+  const long long c = brick * static_cast<long long>(BR3) + l;
+  double d = (hi_face(F, 0, u, brick, l, loc) - u[c]) / F.h[lev][0] +
+             (hi_face(F, 1, v, brick, l, loc) - v[c]) / F.h[lev][1];
+  d += (hi_face(F, 2, w, brick, l, loc) - w[c]) / F.h[lev][2];
+  return d;
+}
+
+// b = -div u* on fluid cells (ns_solver.cpp:482-498), per unit volume.
+__global__ void __launch_bounds__(NT) k_amr_div(AmrFlowView F, const double* __restrict__ u,
+                                                const double* __restrict__ v, const double* __restrict__ w,
+                                                double* __restrict__ b) {
+  const LevelView& L = F.L;
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x)
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      const long long c = brick * static_cast<long long>(BR3) + l;
+      double o = 0.0;
+      if (L.type[c] == CELL_FLUID) o = -cell_div(F, u, v, w, brick, l, L.blevel[brick]);
+      b[c] = o;
+    }
+}
+
+// phi of the level-lev0 cell p (wrapped into the domain; at a finer leaf the
+// first child, which the caller never asks for).
+__device__ __forceinline__ double phi_cell(const AmrFlowView& F, const double* __restrict__ phi, int lev0,
+                                           const int p0[3]) {
+  int p[3] = {p0[0], p0[1], p0[2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p[a] = wrapi(p[a], F.L.lcells[lev0][a]);
+  int lev;
+  const int r = leaf_of(F.L, lev0, p, lev);
+  if (r < 0) return 0.0;
+  int q[3] = {p[0], p[1], p[2]};
+  if (lev == lev0 - 1)
+    for (int d = 0; d < 3; ++d) q[d] >>= 1;
+  if (lev == lev0 + 1)
+    for (int d = 0; d < 3; ++d) q[d] <<= 1;
+  return phi[r * static_cast<long long>(BR3) + local_of(q)];
+}
+
+// Projection correction on owned faces (ns_solver.cpp:528-562) + p = phi/dt.
+__global__ void __launch_bounds__(NT) k_amr_correct(AmrFlowView F, const double* __restrict__ phi,
+                                                    const double* __restrict__ dtp, double* __restrict__ u,
+                                                    double* __restrict__ v, double* __restrict__ w,
+                                                    double* __restrict__ pout) {
+  const LevelView& L = F.L;
+  const double dt = *dtp;
+  double* f[3] = {u, v, w};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x)
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      const long long c = brick * static_cast<long long>(BR3) + l;
+      pout[c] = phi[c] / dt;
+      if (L.type[c] == CELL_SOLID) continue;
+      const int lev = L.blevel[brick];
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      const int o[3] = {L.bcoord[3 * brick] * BR, L.bcoord[3 * brick + 1] * BR, L.bcoord[3 * brick + 2] * BR};
+      const int p[3] = {o[0] + loc[0], o[1] + loc[1], o[2] + loc[2]};
+      const double pc = phi[c];
+      for (int a = 0; a < 3; ++a) {
+        const int stride = a == 0 ? 1 : (a == 1 ? 8 : 64);
+        const double h = F.h[lev][a];
+        if (loc[a] > 0) {
+          if (L.type[c - stride] != CELL_SOLID) f[a][c] -= (pc - phi[c - stride]) / h;
+        } else {
+          const int8_t rel = F.rel_lo[3 * brick + a];
+          if (rel == R_BOUNDARY) {
+            // outlet ghost -phi (Dirichlet 0), Neumann ghost phi (ns_solver.cpp:508-526)
+            const double g = L.bc[2 * a] == NB_BC_OUTLET ? -pc : pc;
+            f[a][c] -= (pc - g) / h;
+          } else if (rel != R_FINER) {
+            int q[3] = {p[0], p[1], p[2]};
+            q[a] -= 1;
+            if (!solid_at(F, lev, q)) {
+              const double d = rel == R_COARSER ? 1.5 * h : h;
+              f[a][c] -= (pc - phi_cell(F, phi, lev, q)) / d;
+            }
+          }
+        }
+        const int sid = F.slab_id[3 * brick + a];
+        if (loc[a] == 7 && sid >= 0) {
+          const int8_t rel = F.rel_hi[3 * brick + a];
+          const long long s = F.nb + sid * 64LL + slab_local(a, loc[0], loc[1], loc[2]);
+          if (rel == R_BOUNDARY) {
+            const double g = L.bc[2 * a + 1] == NB_BC_OUTLET ? -pc : pc;
+            f[a][s] -= (g - pc) / h;
+          } else if (rel == R_COARSER) {
+            int q[3] = {p[0], p[1], p[2]};
+            q[a] += 1;
+            if (!solid_at(F, lev, q)) f[a][s] -= (phi_cell(F, phi, lev, q) - pc) / (1.5 * h);
+          }
+        }
+      }
+    }
+}
+
+// Step diagnostics: [0] sum (u-u0)^2 over owned faces, [1] sum div^2 and
+// [2] max |div| over fluid cells, [3] net boundary mass flux.
+__global__ void __launch_bounds__(NT) k_amr_diag(AmrFlowView F, const double* __restrict__ u,
+                                                 const double* __restrict__ v, const double* __restrict__ w,
+                                                 const double* __restrict__ u0, const double* __restrict__ v0,
+                                                 const double* __restrict__ w0, RedBuf rb, AmrStepScalars* out) {
+  const LevelView& L = F.L;
+  const double* f[3] = {u, v, w};
+  const double* f0[3] = {u0, v0, w0};
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x)
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      const long long c = brick * static_cast<long long>(BR3) + l;
+      const int lev = L.blevel[brick];
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      for (int a = 0; a < 3; ++a) {
+        const double area = F.h[lev][(a + 1) % 3] * F.h[lev][(a + 2) % 3];
+        if (!(loc[a] == 0 && F.rel_lo[3 * brick + a] == R_FINER)) {
+          const double d = f[a][c] - f0[a][c];
+          acc[0] += d * d;
+          if (loc[a] == 0 && F.rel_lo[3 * brick + a] == R_BOUNDARY) acc[3] += f[a][c] * area;
+        }
+        const int sid = F.slab_id[3 * brick + a];
+        if (loc[a] == 7 && sid >= 0 && F.rel_hi[3 * brick + a] != R_FINER) {
+          const long long s = F.nb + sid * 64LL + slab_local(a, loc[0], loc[1], loc[2]);
+          const double d = f[a][s] - f0[a][s];
+          acc[0] += d * d;
+          if (F.rel_hi[3 * brick + a] == R_BOUNDARY) acc[3] -= f[a][s] * area;
+        }
+      }
+      if (L.type[c] == CELL_FLUID) {
+        const double d = cell_div(F, u, v, w, brick, l, lev);
+        acc[1] += d * d;
+        acc[2] = fmax(acc[2], fabs(d));
+      }
+    }
+  grid_reduce<4, (1u << 2)>(acc, rb, [=] __device__(const double* t) {
+    out->du2 = t[0];
+    out->div2 = t[1];
+    out->divmax = t[2];
+    out->mass = t[3];
+  });
+}
+
+// computeDt over leaf cells (ns_solver.cpp:581-603), each with its own spacing;
+// the running maximum starts from the level-0 viscous term as the reference's does.
+__global__ void __launch_bounds__(NT) k_amr_max_inv(AmrFlowView F, const double* __restrict__ u,
+                                                    const double* __restrict__ v, const double* __restrict__ w,
+                                                    double cfl, double* dt_out, RedBuf rb, AmrStepScalars* out) {
+  const LevelView& L = F.L;
+  auto visc_of = [&](int lev) {
+    return 2.0 * F.nu *
+           (1.0 / (F.h[lev][0] * F.h[lev][0]) + 1.0 / (F.h[lev][1] * F.h[lev][1]) +
+            1.0 / (F.h[lev][2] * F.h[lev][2]));
+  };
+  double m[1] = {visc_of(0) + 1e-300};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x)
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      const long long c = brick * static_cast<long long>(BR3) + l;
+      if (L.type[c] != CELL_FLUID) continue;
+      const int lev = L.blevel[brick];
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      const double uc = fabs(0.5 * (u[c] + hi_face(F, 0, u, brick, l, loc)));
+      const double vc = fabs(0.5 * (v[c] + hi_face(F, 1, v, brick, l, loc)));
+      const double wc = fabs(0.5 * (w[c] + hi_face(F, 2, w, brick, l, loc)));
+      const double inv = uc / F.h[lev][0] + vc / F.h[lev][1] + wc / F.h[lev][2] + visc_of(lev);
+      m[0] = fmax(m[0], inv);
+    }
+  grid_reduce<1, 1u>(m, rb, [=] __device__(const double* t) {
+    out->maxinv = t[0];
+    if (dt_out) *dt_out = cfl / t[0];
+  });
+}
+
+}  // namespace
+
+void amr_flow_setup() {
+  NB_CUDA(cudaFuncSetAttribute(k_amr_rhs_rk<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               3 * TN * static_cast<int>(sizeof(double))));
+  NB_CUDA(cudaFuncSetAttribute(k_amr_rhs_rk<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               3 * TN * static_cast<int>(sizeof(float))));
+}
+
+void launch_amr_rhs_rk(cudaStream_t s, const AmrFlowView& F, int stage, const double* dtp, const double* u,
+                       const double* v, const double* w, const double* u0, const double* v0,
+                       const double* w0, double* uo, double* vo, double* wo, int mixed) {
+  const int grid = std::min(F.L.nbrick, 148 * 2);
+  if (mixed)
+    k_amr_rhs_rk<float><<<grid, RHS_NT, 3 * TN * sizeof(float), s>>>(F, stage, dtp, u, v, w, u0, v0, w0, uo, vo,
+                                                                     wo);
+  else
+    k_amr_rhs_rk<double><<<grid, RHS_NT, 3 * TN * sizeof(double), s>>>(F, stage, dtp, u, v, w, u0, v0, w0, uo,
+                                                                       vo, wo);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_sync(cudaStream_t s, const long long* list, int n, double* f) {
+  if (n <= 0) return;
+  k_amr_sync<<<std::min((n + 255) / 256, 1024), 256, 0, s>>>(list, n, f);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_div(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v, const double* w,
+                    double* b) {
+  k_amr_div<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, b);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_correct(cudaStream_t s, const AmrFlowView& F, const double* phi, const double* dtp,
+                        double* u, double* v, double* w, double* p) {
+  k_amr_correct<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, phi, dtp, u, v, w, p);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_diag(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
+                     const double* w, const double* u0, const double* v0, const double* w0, RedBuf rb,
+                     AmrStepScalars* out) {
+  k_amr_diag<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, u0, v0, w0, rb, out);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_max_inv(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
+                        const double* w, double cfl, double* dt_out, RedBuf rb, AmrStepScalars* out) {
+  k_amr_max_inv<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, cfl, dt_out, rb, out);
+  NB_CUDA(cudaGetLastError());
+}
+
+}  // namespace nb

@@ -1,0 +1,47 @@
+// nb_amr_flow.cuh — device view and launchers of the octree-AMR MAC step.
+#pragma once
+#include "nb_flow.cuh"
+#include "nb_internal.h"
+
+namespace nb {
+
+struct AmrFlowView {
+  LevelView L;  // composite level (amr = 1): per-level LUTs, bcoord, blevel, type
+  double origin[3];
+  double h[AMR_MAXLEV][3];
+  double wallv[6][3];
+  double inlet_speed[6];
+  int profile[6];
+  int inlet_axis[6];
+  int per[3];
+  long long nb;          // nbrick * 512 (slab base)
+  const int* slab_id;    // [nbrick][3] slab index or -1
+  const int8_t* rel_lo;  // [nbrick][3] REL_*
+  const int8_t* rel_hi;
+  const int* nbr_lo;     // [nbrick][3] same-level neighbour brick or -1
+  const int* nbr_hi;
+  int weno;
+  double nu;
+  double bf[3];
+};
+
+struct AmrStepScalars {
+  double du2, div2, divmax, mass, maxinv;
+};
+
+void amr_flow_setup();
+void launch_amr_rhs_rk(cudaStream_t s, const AmrFlowView& F, int stage, const double* dtp, const double* u,
+                       const double* v, const double* w, const double* u0, const double* v0,
+                       const double* w0, double* uo, double* vo, double* wo, int mixed);
+void launch_amr_sync(cudaStream_t s, const long long* list, int n, double* f);
+void launch_amr_div(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v, const double* w,
+                    double* b);
+void launch_amr_correct(cudaStream_t s, const AmrFlowView& F, const double* phi, const double* dtp,
+                        double* u, double* v, double* w, double* p);
+void launch_amr_diag(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
+                     const double* w, const double* u0, const double* v0, const double* w0, RedBuf rb,
+                     AmrStepScalars* out);
+void launch_amr_max_inv(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
+                        const double* w, double cfl, double* dt_out, RedBuf rb, AmrStepScalars* out);
+
+}  // namespace nb

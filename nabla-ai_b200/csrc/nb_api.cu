@@ -1,7 +1,7 @@
 // nb_api.cu — the extern "C" boundary (include/nabla_b200.h) over the device
 // solver: context, resident cases, the SSP-RK3 step driver and the Poisson
 // seam. Host orchestration only; all arithmetic on the solution runs in the
-// kernels of nb_flow.cu and nb_mg.cu.
+// kernels of nb_flow.cu, nb_amr_flow.cu and nb_mg.cu.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -10,6 +10,9 @@
 #include <string>
 #include <vector>
 
+#include "nb_amr_faces.h"
+#include "nb_amr_flow.cuh"
+#include "nb_amr_mesh.h"
 #include "nb_ctx.h"
 #include "nb_flow.cuh"
 #include "nb_mg.cuh"
@@ -19,6 +22,7 @@ using namespace nb;
 // Results of one step, written by the step's kernels.
 struct StepBlock {
   StepScalars sc;
+  AmrStepScalars asc;  // octree-AMR cases
   double rep[3][6];  // per projection: MgSolver report
   double dt;
   unsigned long long execs;  // MG loop-body executions so far
@@ -65,6 +69,13 @@ struct nb_case {
   uint64_t nfluid = 0;
   int step = 0;
   double t = 0.0, dt_last = 0.0;
+  // ---- octree-AMR cases (the mesh outlives the case) ----
+  bool amr = false;
+  nb_amr_mesh* mesh = nullptr;
+  AmrFaceMaps fm;
+  AmrFlowView AF{};
+  long long* d_sync[3] = {nullptr, nullptr, nullptr};
+  int nsync[3] = {0, 0, 0};
 
   void* alloc(size_t n) {
     void* q = nullptr;
@@ -264,6 +275,7 @@ void flow_launch(nb_case& c, const char* fam, double bytes, Fn&& fn) {
 }
 
 double ncell_of(const nb_case& c) {
+  if (c.amr) return static_cast<double>(c.fm.nbrick) * BR3;
   return static_cast<double>(c.grid.nx) * c.grid.ny * c.grid.nz;
 }
 
@@ -309,17 +321,88 @@ double visc_of(const nb_case& c) {
 
 double compute_dt(nb_case& c) {
   double* const* f = c.uvw[c.cur];
-  flow_launch(c, "max_inv", ncell_of(c) * 25, [&] {
-    launch_max_inv(c.stream, c.F, f[0], f[1], f[2], visc_of(c), c.cfg.cfl, nullptr, c.rb, &c.d_blk->sc);
-  });
+  if (c.amr) {
+    flow_launch(c, "max_inv", ncell_of(c) * 25, [&] {
+      launch_amr_max_inv(c.stream, c.AF, f[0], f[1], f[2], c.cfg.cfl, nullptr, c.rb, &c.d_blk->asc);
+    });
+  } else {
+    flow_launch(c, "max_inv", ncell_of(c) * 25, [&] {
+      launch_max_inv(c.stream, c.F, f[0], f[1], f[2], visc_of(c), c.cfg.cfl, nullptr, c.rb, &c.d_blk->sc);
+    });
+  }
   NB_CUDA(cudaMemcpyAsync(c.h_blk, c.d_blk, sizeof(StepBlock), cudaMemcpyDeviceToHost, c.stream));
   NB_CUDA(cudaStreamSynchronize(c.stream));
-  return c.cfg.cfl / c.h_blk->sc.maxinv;
+  return c.cfg.cfl / (c.amr ? c.h_blk->asc.maxinv : c.h_blk->sc.maxinv);
+}
+
+// ---- octree-AMR step ---------------------------------------------------------
+// Derived coarse faces <- average of their fine sub-faces.
+void amr_sync(nb_case& c, double* const* f) {
+  for (int a = 0; a < 3; ++a)
+    if (c.nsync[a])
+      flow_launch(c, "sync", c.nsync[a] * 40.0, [&] { launch_amr_sync(c.stream, c.d_sync[a], c.nsync[a], f[a]); });
+}
+
+void amr_bc(nb_case& c, double* const* f, bool outflow) {
+  apply_bc(c, f, outflow);
+  amr_sync(c, f);
+}
+
+// NSSolver::project (ns_solver.cpp:475-579) on the composite mesh.
+void project_amr(nb_case& c, double* const* f, int stage, bool direct) {
+  StepBlock* blk = c.d_blk;
+  amr_bc(c, f, true);
+  flow_launch(c, "div", ncell_of(c) * 33, [&] { launch_amr_div(c.stream, c.AF, f[0], f[1], f[2], c.b); });
+  if (direct) {
+    c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage]);
+  } else {
+    uint64_t nbody = 0;
+    c.mg->capture_solve(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage],
+                        &nbody);
+    c.body_kernels = nbody;
+  }
+  flow_launch(c, "correct", ncell_of(c) * 65,
+              [&] { launch_amr_correct(c.stream, c.AF, c.mg->phi(), &blk->dt, f[0], f[1], f[2], c.p); });
+  amr_bc(c, f, false);
+}
+
+void issue_step_amr(nb_case& c, int cur, bool cfl_dt, bool direct) {
+  StepBlock* blk = c.d_blk;
+  double** A = c.uvw[cur];
+  double** B = c.uvw[1 - cur];
+  if (cfl_dt)
+    flow_launch(c, "max_inv", ncell_of(c) * 25, [&] {
+      launch_amr_max_inv(c.stream, c.AF, A[0], A[1], A[2], c.cfg.cfl, &blk->dt, c.rb, &blk->asc);
+    });
+  for (int q = 0; q < 3; ++q)
+    NB_CUDA(cudaMemcpyAsync(c.uvw0[q], A[q], static_cast<size_t>(c.fm.store[q]) * 8, cudaMemcpyDeviceToDevice,
+                            c.stream));
+  amr_bc(c, A, true);
+  const int mixed = c.precision == NB_PRECISION_MIXED;
+  for (int stage = 1; stage <= 3; ++stage) {
+    double** in = (stage == 2) ? B : A;
+    double** out = (stage == 2) ? A : B;
+    flow_launch(c, "rhs_rk", ncell_of(c) * 73, [&] {
+      launch_amr_rhs_rk(c.stream, c.AF, stage, &blk->dt, in[0], in[1], in[2], c.uvw0[0], c.uvw0[1], c.uvw0[2],
+                        out[0], out[1], out[2], mixed);
+    });
+    amr_sync(c, out);
+    project_amr(c, out, stage - 1, direct);
+  }
+  flow_launch(c, "diag", ncell_of(c) * 49, [&] {
+    launch_amr_diag(c.stream, c.AF, B[0], B[1], B[2], c.uvw0[0], c.uvw0[1], c.uvw0[2], c.rb, &blk->asc);
+  });
+  NB_CUDA(cudaMemcpyAsync(&blk->execs, c.mg->body_execs(), sizeof(unsigned long long),
+                          cudaMemcpyDeviceToDevice, c.stream));
 }
 
 // Issues one SSP-RK3 step (NSSolver::step, core/src/flow/ns_solver.cpp:765-824)
 // starting from state parity `cur`. cfl_dt: dt = computeDt() on the device.
 void issue_step(nb_case& c, int cur, bool cfl_dt, bool direct) {
+  if (c.amr) {
+    issue_step_amr(c, cur, cfl_dt, direct);
+    return;
+  }
   StepBlock* blk = c.d_blk;
   double** A = c.uvw[cur];
   double** B = c.uvw[1 - cur];
@@ -398,8 +481,17 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
   nb_poisson_report pr[3];
   for (int s = 0; s < 3; ++s) pr[s] = MgSolver::report_from(hb.rep[s], c.cfg.poisson_tol);
   const nb_grid_desc& g = c.grid;
-  const double nfaces = static_cast<double>(lex_size(c.F, 0) + lex_size(c.F, 1) + lex_size(c.F, 2));
-  const StepScalars& sc = hb.sc;
+  const double nfaces =
+      c.amr ? static_cast<double>(c.fm.owned[0] + c.fm.owned[1] + c.fm.owned[2])
+            : static_cast<double>(lex_size(c.F, 0) + lex_size(c.F, 1) + lex_size(c.F, 2));
+  StepScalars sc = hb.sc;
+  if (c.amr) {
+    sc = StepScalars{};
+    sc.du2 = hb.asc.du2;
+    sc.div2 = hb.asc.div2;
+    sc.divmax = hb.asc.divmax;
+    sc.mass = hb.asc.mass;
+  }
   std::memset(rep, 0, sizeof(*rep));
   rep->step = c.step;
   rep->t = c.t;
@@ -413,14 +505,14 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
   rep->poisson_iters = pr[0].iterations + pr[1].iterations + pr[2].iterations;
   rep->poisson_residual = std::max(pr[0].residual, std::max(pr[1].residual, pr[2].residual));
   rep->converged = pr[0].converged && pr[1].converged && pr[2].converged;
-  if (c.has_solid) {
+  if (c.has_solid && !c.amr) {
     double aref = c.cfg.ref_area;
     if (aref <= 0.0) aref = c.cfg.ref_length * c.cfg.ref_length;
     const double q = 0.5 * c.cfg.density * c.cfg.velocity_scale * c.cfg.velocity_scale * aref + 1e-300;
     rep->cd = sc.fx / q;
     rep->cl = sc.fy / q;
   }
-  rep->cell_count = static_cast<uint64_t>(g.nx) * g.ny * g.nz;
+  rep->cell_count = c.amr ? static_cast<uint64_t>(c.fm.nbrick) * BR3 : static_cast<uint64_t>(g.nx) * g.ny * g.nz;
   rep->accepted = (rep->continuity_residual < c.cfg.tol_continuity && rep->mass_error < c.cfg.tol_mass) ? 1 : 0;
 }
 
@@ -476,6 +568,7 @@ nb_status nb_ctx_create(int device, nb_ctx** out) {
   const nb_status s = guarded(ctx, [&] {
     NB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     flow_kernel_setup();
+    amr_flow_setup();
     return NB_OK;
   });
   if (s != NB_OK) {
@@ -627,12 +720,14 @@ nb_status nb_ctx_profile_read(nb_ctx* ctx, double* total_ms, uint64_t* launches,
 }
 
 uint64_t nb_case_cell_count(const nb_case* c) {
+  if (c && c->amr) return static_cast<uint64_t>(c->fm.nbrick) * BR3;
   return c ? static_cast<uint64_t>(c->grid.nx) * c->grid.ny * c->grid.nz : 0;
 }
 
 nb_status nb_case_set_state(nb_case* c, const double* u, const double* v, const double* w,
                             const double* p, int step, double t, double dt_last) {
   if (!c || !u || !v || !w || !p) return NB_ERR_BAD_ARG;
+  if (c->amr) return fail(c->ctx, NB_ERR_UNSUPPORTED, "AMR cases take nb_amr_case_set_state");
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
     double** f = c->uvw[c->cur];
@@ -650,6 +745,7 @@ nb_status nb_case_set_state(nb_case* c, const double* u, const double* v, const 
 
 nb_status nb_case_get_state(nb_case* c, double* u, double* v, double* w, double* p) {
   if (!c) return NB_ERR_BAD_ARG;
+  if (c->amr) return fail(c->ctx, NB_ERR_UNSUPPORTED, "AMR cases take nb_amr_case_get_state");
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
     double** f = c->uvw[c->cur];
@@ -674,6 +770,27 @@ nb_status nb_case_initialize(nb_case* c) {
   if (!c) return NB_ERR_BAD_ARG;
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
+    if (c->amr) {  // zero interior, inlet speed on u as the initial guess
+      double s = 0.0;
+      for (int f = 0; f < 6; ++f)
+        if (c->grid.face[f].type == NB_BC_INLET && c->grid.face[f].inlet_axis == 0) {
+          s = c->grid.face[f].inlet_speed;
+          break;
+        }
+      double** fl = c->uvw[c->cur];
+      for (int a = 0; a < 3; ++a) {
+        std::vector<double> F0(static_cast<size_t>(c->fm.store[a]), a == 0 ? s : 0.0);
+        NB_CUDA(cudaMemcpyAsync(fl[a], F0.data(), F0.size() * 8, cudaMemcpyHostToDevice, c->stream));
+        NB_CUDA(cudaStreamSynchronize(c->stream));
+      }
+      NB_CUDA(cudaMemsetAsync(c->p, 0, static_cast<size_t>(c->fm.nbrick) * BR3 * 8, c->stream));
+      amr_bc(*c, fl, true);
+      NB_CUDA(cudaStreamSynchronize(c->stream));
+      c->step = 0;
+      c->t = 0.0;
+      c->dt_last = 0.0;
+      return NB_OK;
+    }
     const long long nu = lex_size(c->F, 0), nv = lex_size(c->F, 1), nw = lex_size(c->F, 2),
                     np = lex_size(c->F, 3);
     std::vector<double> U(nu, 0.0), V(nv, 0.0), W(nw, 0.0), P(np, 0.0);
@@ -776,6 +893,199 @@ nb_status nb_apply_laplacian(nb_ctx* ctx, const nb_grid_desc* grid, const double
     ctx->launches += 2;
     NB_CUDA(cudaMemcpyAsync(out, ctx->stage_a, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     NB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return NB_OK;
+  });
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// octree-AMR cases
+// ===========================================================================
+extern "C" {
+
+nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_config* cfg, int precision,
+                             nb_case** out) {
+  if (!ctx || !mesh || !cfg || !out) return NB_ERR_BAD_ARG;
+  *out = nullptr;
+  if (precision != NB_PRECISION_FP64 && precision != NB_PRECISION_MIXED)
+    return fail(ctx, NB_ERR_BAD_ARG, "precision must be NB_PRECISION_FP64 or NB_PRECISION_MIXED");
+  if (!(cfg->reynolds > 0.0)) return fail(ctx, NB_ERR_BAD_ARG, "reynolds must be > 0");
+  auto c = std::make_unique<nb_case>();
+  c->ctx = ctx;
+  c->amr = true;
+  c->mesh = mesh;
+  const nb_status s = guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    NB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    const AmrLevelHost& lv = mesh->lvl;
+    const AmrTree& t = lv.tree;
+    const nb_amr_geom& g = mesh->geom;
+    c->cfg = *cfg;
+    c->precision = precision;
+    c->nu = cfg->velocity_scale * cfg->ref_length / cfg->reynolds;  // ns_solver.cpp:54
+    // level-0 description: report normalisation and inlet data
+    c->grid.nx = t.cells(0, 0);
+    c->grid.ny = t.cells(0, 1);
+    c->grid.nz = t.cells(0, 2);
+    c->grid.dx = g.h0[0];
+    c->grid.dy = g.h0[1];
+    c->grid.dz = g.h0[2];
+    for (int a = 0; a < 3; ++a) c->grid.origin[a] = g.origin[a];
+    for (int f = 0; f < 6; ++f) c->grid.face[f] = g.face[f];
+    for (uint8_t v : lv.type)
+      if (v == CELL_SOLID) {
+        c->has_solid = true;
+        break;
+      }
+    c->nfluid = lv.nfluid;
+    c->mg = std::make_unique<MgSolver>(lv, precision, LaunchCounter{&ctx->launches, &ctx->prof});
+    build_face_maps(t, c->fm);
+    AmrFlowView& F = c->AF;
+    auto up = [&](const void* src, size_t bytes) {
+      void* d = c->alloc(bytes);
+      if (src && bytes) NB_CUDA(cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice));
+      else NB_CUDA(cudaMemset(d, 0, bytes ? bytes : 16));
+      return d;
+    };
+    // The flow kernels' own view of the leaves (per-level LUTs, coordinates,
+    // levels, cell types). It does not come from the multigrid hierarchy,
+    // whose finest level is a uniform view when the mesh has one level.
+    LevelView& V = F.L;
+    V = LevelView{};
+    V.amr = 1;
+    V.nbrick = static_cast<int>(t.leaves.size());
+    V.nlev = t.nlev;
+    for (int f = 0; f < 6; ++f) V.bc[f] = g.face[f].type;
+    V.nx = t.cells(0, 0);
+    V.ny = t.cells(0, 1);
+    V.nz = t.cells(0, 2);
+    for (int L = 0; L < t.nlev && L < AMR_MAXLEV; ++L) {
+      V.lut_off[L] = t.lut_off[L];
+      for (int a = 0; a < 3; ++a) {
+        V.lnb[L][a] = t.lnb(L, a);
+        V.lcells[L][a] = t.cells(L, a);
+        V.lh2[L][a] = 1.0 / (t.h(L, a) * t.h(L, a));
+      }
+    }
+    for (int a = 0; a < 3; ++a) V.dxyz[a] = t.h(0, a);
+    V.lut = static_cast<const int*>(up(t.lut.data(), t.lut.size() * sizeof(int)));
+    V.bcoord = static_cast<const int*>(up(lv.bcoord.data(), lv.bcoord.size() * sizeof(int)));
+    V.type = static_cast<const uint8_t*>(up(lv.type.data(), lv.type.size()));
+    V.blevel = static_cast<const int8_t*>(up(lv.blevel.data(), lv.blevel.size()));
+    for (int a = 0; a < 3; ++a) F.origin[a] = g.origin[a];
+    for (int L = 0; L < t.nlev && L < AMR_MAXLEV; ++L)
+      for (int a = 0; a < 3; ++a) F.h[L][a] = t.h(L, a);
+    for (int f = 0; f < 6; ++f) {
+      for (int a = 0; a < 3; ++a) F.wallv[f][a] = g.face[f].wall_velocity[a];
+      F.inlet_speed[f] = g.face[f].inlet_speed;
+      F.profile[f] = g.face[f].profile;
+      F.inlet_axis[f] = g.face[f].inlet_axis;
+    }
+    for (int a = 0; a < 3; ++a) F.per[a] = g.face[2 * a].type == NB_BC_PERIODIC;
+    F.nb = static_cast<long long>(c->fm.nbrick) * BR3;
+    if (t.nlev > AMR_MAXLEV) throw ApiError{NB_ERR_UNSUPPORTED, "mesh has more octree levels than supported"};
+    F.slab_id = static_cast<const int*>(up(c->fm.slab_id.data(), c->fm.slab_id.size() * sizeof(int)));
+    F.rel_lo = static_cast<const int8_t*>(up(c->fm.rel_lo.data(), c->fm.rel_lo.size()));
+    F.rel_hi = static_cast<const int8_t*>(up(c->fm.rel_hi.data(), c->fm.rel_hi.size()));
+    F.nbr_lo = static_cast<const int*>(up(c->fm.nbr_lo.data(), c->fm.nbr_lo.size() * sizeof(int)));
+    F.nbr_hi = static_cast<const int*>(up(c->fm.nbr_hi.data(), c->fm.nbr_hi.size() * sizeof(int)));
+    F.weno = cfg->convection == NB_CONV_WENO5;
+    F.nu = c->nu;
+    for (int a = 0; a < 3; ++a) F.bf[a] = cfg->body_force[a];
+    for (int h = 0; h < 2; ++h)
+      for (int q = 0; q < 3; ++q) {
+        const size_t nb = static_cast<size_t>(c->fm.store[q]) * sizeof(double);
+        c->uvw[h][q] = static_cast<double*>(c->alloc(nb));
+        NB_CUDA(cudaMemset(c->uvw[h][q], 0, nb));
+      }
+    for (int q = 0; q < 3; ++q) {
+      const size_t nb = static_cast<size_t>(c->fm.store[q]) * sizeof(double);
+      c->uvw0[q] = static_cast<double*>(c->alloc(nb));
+      NB_CUDA(cudaMemset(c->uvw0[q], 0, nb));
+    }
+    const size_t ncs = static_cast<size_t>(F.nb);
+    c->p = static_cast<double*>(c->alloc(ncs * sizeof(double)));
+    c->b = static_cast<double*>(c->alloc(ncs * sizeof(double)));
+    NB_CUDA(cudaMemset(c->p, 0, ncs * sizeof(double)));
+    NB_CUDA(cudaMemset(c->b, 0, ncs * sizeof(double)));
+    for (int a = 0; a < 3; ++a) {
+      c->nsync[a] = static_cast<int>(c->fm.sync[a].size() / 5);
+      if (c->nsync[a])
+        c->d_sync[a] =
+            static_cast<long long*>(up(c->fm.sync[a].data(), c->fm.sync[a].size() * sizeof(long long)));
+    }
+    std::vector<BcOp> out_ops, in_ops, solid_ops, unused;
+    build_amr_bc(t, c->fm, lv.type, g, true, out_ops, solid_ops);
+    build_amr_bc(t, c->fm, lv.type, g, false, in_ops, unused);
+    c->n_out = static_cast<int>(out_ops.size());
+    c->n_in = static_cast<int>(in_ops.size());
+    c->n_solid = static_cast<int>(solid_ops.size());
+    c->serial_out = needs_serial(out_ops);
+    c->serial_in = needs_serial(in_ops);
+    c->bc_out = upload_ops(*c, out_ops);
+    c->bc_in = upload_ops(*c, in_ops);
+    c->bc_solid = upload_ops(*c, solid_ops);
+    c->rb.max_blocks = 148 * 4;
+    c->rb.partials = static_cast<double*>(c->alloc(RED_KMAX * c->rb.max_blocks * sizeof(double)));
+    c->rb.counter = static_cast<unsigned*>(c->alloc(sizeof(unsigned)));
+    NB_CUDA(cudaMemset(c->rb.counter, 0, sizeof(unsigned)));
+    c->d_blk = static_cast<StepBlock*>(c->alloc(sizeof(StepBlock)));
+    NB_CUDA(cudaMemset(c->d_blk, 0, sizeof(StepBlock)));
+    NB_CUDA(cudaMallocHost(&c->h_blk, sizeof(StepBlock)));
+    NB_CUDA(cudaMallocHost(&c->h_dt, sizeof(double)));
+    NB_CUDA(cudaDeviceSynchronize());
+    return NB_OK;
+  });
+  if (s != NB_OK) return s;
+  *out = c.release();
+  return NB_OK;
+}
+
+nb_status nb_amr_case_sizes(const nb_case* c, int64_t sizes[4]) {
+  if (!c || !c->amr || !sizes) return NB_ERR_BAD_ARG;
+  for (int a = 0; a < 3; ++a) sizes[a] = c->fm.store[a];
+  sizes[3] = static_cast<int64_t>(c->fm.nbrick) * BR3;
+  return NB_OK;
+}
+
+nb_status nb_amr_case_slabs(const nb_case* c, int axis, int32_t* bricks) {
+  if (!c || !c->amr || axis < 0 || axis > 2 || !bricks) return NB_ERR_BAD_ARG;
+  for (size_t s = 0; s < c->fm.slab_brick[axis].size(); ++s) bricks[s] = c->fm.slab_brick[axis][s];
+  return NB_OK;
+}
+
+nb_status nb_amr_case_set_state(nb_case* c, const double* u, const double* v, const double* w, const double* p) {
+  if (!c || !c->amr || !u || !v || !w || !p) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    double** f = c->uvw[c->cur];
+    const double* src[3] = {u, v, w};
+    for (int a = 0; a < 3; ++a)
+      NB_CUDA(cudaMemcpyAsync(f[a], src[a], static_cast<size_t>(c->fm.store[a]) * 8, cudaMemcpyHostToDevice,
+                              c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->p, p, static_cast<size_t>(c->fm.nbrick) * BR3 * 8, cudaMemcpyHostToDevice,
+                            c->stream));
+    amr_sync(*c, f);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NB_OK;
+  });
+}
+
+nb_status nb_amr_case_get_state(nb_case* c, double* u, double* v, double* w, double* p) {
+  if (!c || !c->amr) return NB_ERR_BAD_ARG;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    double** f = c->uvw[c->cur];
+    double* dst[3] = {u, v, w};
+    for (int a = 0; a < 3; ++a)
+      if (dst[a])
+        NB_CUDA(cudaMemcpyAsync(dst[a], f[a], static_cast<size_t>(c->fm.store[a]) * 8, cudaMemcpyDeviceToHost,
+                                c->stream));
+    if (p)
+      NB_CUDA(cudaMemcpyAsync(p, c->p, static_cast<size_t>(c->fm.nbrick) * BR3 * 8, cudaMemcpyDeviceToHost,
+                              c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
     return NB_OK;
   });
 }

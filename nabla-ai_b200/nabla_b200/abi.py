@@ -158,6 +158,11 @@ PROTOTYPES = [
     ("nb_amr_mesh_leaves", C.c_int, [VP, C.POINTER(C.c_int32)]),
     ("nb_amr_apply_laplacian", C.c_int, [VP, VP, DP, DP]),
     ("nb_amr_poisson_solve", C.c_int, [VP, VP, DP, DP, C.c_double, C.c_int, C.c_int, C.POINTER(PoissonReport)]),
+    ("nb_amr_case_create", C.c_int, [VP, VP, C.POINTER(FlowConfig), C.c_int, C.POINTER(VP)]),
+    ("nb_amr_case_sizes", C.c_int, [VP, C.POINTER(C.c_int64)]),
+    ("nb_amr_case_slabs", C.c_int, [VP, C.c_int, C.POINTER(C.c_int32)]),
+    ("nb_amr_case_set_state", C.c_int, [VP, DP, DP, DP, DP]),
+    ("nb_amr_case_get_state", C.c_int, [VP, DP, DP, DP, DP]),
 ]
 
 

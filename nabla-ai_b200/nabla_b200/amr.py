@@ -126,3 +126,97 @@ class AmrMesh:
                                                          max_cycles, precision, C.byref(rep)),
                        "nb_amr_poisson_solve")
         return x, Report(rep.iterations, rep.residual, bool(rep.converged))
+
+
+class AmrCase:
+    """NSSolver-style MAC step on an AMR mesh, state resident on the device
+    (nb_amr_case_*). Face arrays are in the library's storage order (see
+    ``face_positions``)."""
+
+    def __init__(self, mesh: AmrMesh, config: abi.FlowConfig, precision: int = abi.PRECISION_FP64):
+        self.mesh, self.ctx, self.config = mesh, mesh.ctx, config
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.nb_amr_case_create(self.ctx.h, mesh.h, C.byref(config), precision,
+                                                       C.byref(h)), "nb_amr_case_create")
+        self.h = h
+        sz = (C.c_int64 * 4)()
+        self.ctx.check(self.ctx.lib.nb_amr_case_sizes(h, sz), "nb_amr_case_sizes")
+        self.sizes = tuple(int(s) for s in sz)
+        ncell = mesh.leaves.shape[0] * 512
+        self.slabs = []
+        for a in range(3):
+            arr = np.zeros((self.sizes[a] - ncell) // 64, dtype=np.int32)
+            if arr.size:
+                self.ctx.check(self.ctx.lib.nb_amr_case_slabs(h, a, arr.ctypes.data_as(C.POINTER(C.c_int32))),
+                               "nb_amr_case_slabs")
+            self.slabs.append(arr)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.nb_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def face_index(self, a: int):
+        """(level, i, j, k) face coordinates of every stored a-face, storage
+        order: i, j, k are level-`level` indices with the a-th one the face
+        index (low face of cell i is i; a slab face is 8*b + 8)."""
+        lv = self.mesh.leaves
+        lev, i, j, k = cell_coords(lv)
+        idx = [i, j, k]
+        sl = self.slabs[a]
+        if sl.size:
+            m = np.arange(64)
+            t1, t2 = [(1, 2), (0, 2), (0, 1)][a]
+            sb = lv[sl]
+            slev = np.repeat(sb[:, 0], 64)
+            sidx = [None, None, None]
+            sidx[a] = np.repeat(sb[:, 1 + a] * 8 + 8, 64)
+            sidx[t1] = (sb[:, 1 + t1:2 + t1] * 8 + (m & 7)[None, :]).ravel()
+            sidx[t2] = (sb[:, 1 + t2:2 + t2] * 8 + (m >> 3)[None, :]).ravel()
+            lev = np.concatenate([lev, slev])
+            idx = [np.concatenate([idx[d], sidx[d]]) for d in range(3)]
+        return lev, idx[0], idx[1], idx[2]
+
+    def face_positions(self, a: int):
+        """Physical (x, y, z) of every stored a-face (storage order)."""
+        lev, i, j, k = self.face_index(a)
+        h = [self.mesh.geom.h0[d] / (2.0 ** lev) for d in range(3)]
+        o = self.mesh.geom.origin
+        idx = (i, j, k)
+        return [o[d] + (idx[d] + (0.0 if d == a else 0.5)) * h[d] for d in range(3)]
+
+    def initialize(self):
+        self.ctx.check(self.ctx.lib.nb_case_initialize(self.h), "initialize")
+
+    def set_state(self, u, v, w, p):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v, w, p)]
+        if [x.size for x in arrs] != list(self.sizes):
+            raise ValueError(f"state sizes {[x.size for x in arrs]} != {list(self.sizes)}")
+        self.ctx.check(self.ctx.lib.nb_amr_case_set_state(self.h, *[abi.dptr(x) for x in arrs]), "set_state")
+
+    def get_state(self):
+        out = [np.zeros(n) for n in self.sizes]
+        self.ctx.check(self.ctx.lib.nb_amr_case_get_state(self.h, *[abi.dptr(x) for x in out]), "get_state")
+        return out
+
+    def compute_dt(self) -> float:
+        dt = C.c_double()
+        self.ctx.check(self.ctx.lib.nb_case_compute_dt(self.h, C.byref(dt)), "computeDt")
+        return dt.value
+
+    def step(self, dt: float = 0.0) -> abi.StepReport:
+        rep = abi.StepReport()
+        self.ctx.check(self.ctx.lib.nb_step(self.h, dt, C.byref(rep)), "step")
+        return rep
+
+    def step_many(self, dt: float, n: int) -> abi.StepReport:
+        rep = abi.StepReport()
+        self.ctx.check(self.ctx.lib.nb_step_many(self.h, dt, n, C.byref(rep)), "step_many")
+        return rep
+
+    @property
+    def cell_count(self) -> int:
+        return self.ctx.lib.nb_case_cell_count(self.h)
