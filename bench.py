@@ -1,23 +1,34 @@
 """Benchmark: Mcell-steps/s of the SSP-RK3 / WENO-5 / MG-PCG step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tgv64] [--precision fp64|mixed]
+                    [--workload channel3|tgv64] [--precision fp64|mixed]
+
+Workloads (seeded synthetic inputs, no datasets):
+  channel3  3-level octree obstacle channel, [0,4]x[0,1]^2, base 64x16x16 in 8^3
+            bricks refined to effective 256x64x64 where the initial vorticity is in
+            its top fifth or near the 6 seeded boxes; inflow U=1, outlet, walls,
+            nu=1/1000, CFL 0.4 (dt from the CFL condition every step). Default.
+  tgv64     Taylor-Green vortex on the periodic 64^3 box, nu=1/1600, fixed dt.
 
 One step = one full SSP-RK3 step (three RHS evaluations, three projections
-solved by MG-PCG to the case tolerance) over the whole case. Prints one JSON
-line on rank 0. N > 1 runs one independent replica per GPU (the path does not
-shard: no collective on the data path); the time is the max over ranks.
+solved by MG-PCG to 1e-10) over every leaf cell. Prints one JSON line on rank
+0. N > 1 runs one independent replica per GPU (the path does not shard: no
+collective on the data path); the time is the max over ranks.
 
 `value` is device-timed with CUDA events on the case's stream with the state
-resident in HBM; the L2 is flushed (a 256 MiB write) between timed steps.
+resident in HBM; the L2 is flushed (a 256 MiB write) between timed steps. For
+the octree workload both arithmetic forms are timed (`forms`); `value` is the
+form named by --precision (mixed by default there) and `accuracy` states the
+mixed form's velocity / pressure / divergence error against the FP64 form.
 `e2e` is the same metric through the C ABI with host buffers: the state is
 uploaded from pinned memory, stepped and downloaded every step.
 `--impl reference` times the reference's own CPU implementation (oracle/_ref,
-compiled from the reference sources) on this host's cores on the same workload.
+compiled from the reference sources) on this host's cores; the reference has no
+octree MAC step, so for channel3 it runs its uniform NSSolver on the
+uniform-fine (256x64x64) version of the same case.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -30,17 +41,76 @@ sys.path.insert(0, os.path.join(REPO, "nabla-ai_b200"))
 METRIC = "Mcell-steps/s (mixed vs FP64 plain, div<1e-8) on 1 B200; p50/p99 solve latency"
 UNIT = "Mcell-steps/s"
 FAMILIES = ["rhs_rk", "smooth", "resid_restrict", "coarse_cg", "pcg_matvec", "pcg_update",
-            "pcg_center", "pcg_mean", "pcg_dots", "pcg_dir", "div", "correct", "diag"]
+            "pcg_center", "pcg_mean", "pcg_dots", "pcg_dir", "div", "correct", "diag", "sync"]
 
 
-def workload(name):
-    from nabla_b200 import cases
-    if name == "tgv64":
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+class UniformRun:
+    """A uniform-grid case through nb_case_* (fixed dt from the initial state)."""
+
+    def __init__(self, ctx, prec):
+        from nabla_b200 import cases, solver
         g, cfg = cases.taylor_green(64)
-        st = cases.taylor_green_state(g)
-        desc = ("Taylor-Green vortex, periodic [0,2pi]^3, uniform 64^3 MAC grid (512 bricks of 8^3), "
-                "nu=1/1600, WENO-5, fixed dt=computeDt at CFL 0.4, MG-PCG to 1e-10")
-        return g, cfg, st, desc
+        self.ns = solver.NSSolver(g, cfg, precision=prec, ctx=ctx)
+        self.ns.set_state(*cases.taylor_green_state(g))
+        self.dt = self.ns.compute_dt()
+        self.cells = self.ns.cell_count
+        self.h = self.ns.h
+        self.desc = ("Taylor-Green vortex, periodic [0,2pi]^3, uniform 64^3 MAC grid (512 bricks of 8^3), "
+                     "nu=1/1600, WENO-5, fixed dt=computeDt at CFL 0.4, MG-PCG to 1e-10")
+        self.data = "synthetic (analytic Taylor-Green initial state)"
+
+    def step(self):
+        return self.ns.step(self.dt)
+
+    def get_state(self):
+        return self.ns.get_state()
+
+    def set_state(self, *st):
+        self.ns.set_state(*st)
+
+
+_CHANNEL = {}
+
+
+def channel_workload(seed=0):
+    from nabla_b200 import workloads
+    if seed not in _CHANNEL:
+        _CHANNEL[seed] = workloads.obstacle_channel(seed)
+    return _CHANNEL[seed]
+
+
+class AmrRun:
+    """The octree obstacle channel through nb_amr_case_* (CFL dt every step)."""
+
+    def __init__(self, ctx, prec, mesh=None):
+        from nabla_b200 import amr
+        w = channel_workload()
+        self.mesh = mesh or amr.AmrMesh(w.geom, w.leaves, solid=w.solid, ctx=ctx)
+        self.case = amr.AmrCase(self.mesh, w.config, precision=prec)
+        self.case.set_state(*w.initial_state(self.case))
+        self.cells = self.case.cell_count
+        self.h = self.case.h
+        self.desc = w.description
+        self.data = "synthetic (seeded boxes and random-potential perturbation, seed 0)"
+
+    def step(self):
+        return self.case.step(0.0)
+
+    def get_state(self):
+        return self.case.get_state()
+
+    def set_state(self, *st):
+        self.case.set_state(*st)
+
+
+def make_run(name, ctx, prec, mesh=None):
+    if name == "tgv64":
+        return UniformRun(ctx, prec)
+    if name == "channel3":
+        return AmrRun(ctx, prec, mesh)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -101,82 +171,105 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def timed_steps(run, steps, stream, flush, clock=None):
+    """K steps, each bracketed by CUDA events on the case stream; the L2 is
+    flushed before every step outside the events. Returns (ms total, reports)."""
+    import torch
+    elapsed, reps = 0.0, []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        reps.append(run.step())
+        e1.record(stream)
+        e1.synchronize()
+        elapsed += e0.elapsed_time(e1)
+    return elapsed, reps
+
+
+def profile_step(ctx, run, fam):
+    import ctypes as C
+    ctx.lib.nb_ctx_profile(ctx.h, fam.encode())
+    try:
+        run.step()
+    finally:
+        ms, nl, nb = C.c_double(), C.c_uint64(), C.c_double()
+        ctx.lib.nb_ctx_profile_read(ctx.h, C.byref(ms), C.byref(nl), C.byref(nb))
+        ctx.lib.nb_ctx_profile(ctx.h, None)
+    return ms.value, nl.value, nb.value
+
+
+def max_over_ranks(x, world, device):
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rel_err(a, b):
+    import numpy as np
+    den = float(np.abs(b).max()) if b.size else 0.0
+    return float(np.abs(a - b).max()) / max(den, 1e-300)
+
+
 def run_ours(args, rank, world, local_rank):
     import ctypes as C
 
-    import numpy as np
     import torch
 
     from nabla_b200 import abi, solver
 
+    device = f"cuda:{local_rank}"
     torch.cuda.set_device(local_rank)
     ctx = solver.Context(local_rank)
-    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
-    g, cfg, st, desc = workload(args.workload)
-    ns = solver.NSSolver(g, cfg, precision=prec, ctx=ctx)
-    ns.set_state(*st)
-    dt = ns.compute_dt()
-    cells = ns.cell_count
-    stream = torch.cuda.ExternalStream(ns.ctx.lib.nb_case_stream(ns.h))
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    precision = args.precision or ("mixed" if args.workload == "channel3" else "fp64")
+    prec = abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64
+    run = make_run(args.workload, ctx, prec)
+    cells = run.cells
+    stream = torch.cuda.ExternalStream(ctx.lib.nb_case_stream(run.h))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
-    def one_step():
-        return ns.step(dt)
-
-    # warm-up
     for _ in range(args.warmup):
-        rep = one_step()
+        run.step()
     torch.cuda.synchronize()
-    # share of each kernel family (one profiled step per family, untimed)
+    # share of each kernel family (one profiled direct-launch step per family, untimed)
     shares = {}
     for fam in (FAMILIES if args.shares else ["smooth"]):
-        ctx.lib.nb_ctx_profile(ctx.h, fam.encode())
-        one_step()
-        ms, nl, nb = C.c_double(), C.c_uint64(), C.c_double()
-        ctx.lib.nb_ctx_profile_read(ctx.h, C.byref(ms), C.byref(nl), C.byref(nb))
-        shares[fam] = {"ms": ms.value, "launches": nl.value, "bytes": nb.value}
-    ctx.lib.nb_ctx_profile(ctx.h, None)
+        ms, nl, nb = profile_step(ctx, run, fam)
+        shares[fam] = {"ms": ms, "launches": nl, "bytes": nb}
     total = sum(v["ms"] for v in shares.values()) or 1.0
     top = max(shares, key=lambda k: shares[k]["ms"])
-    # timed region: K steps, each bracketed by events on the case stream,
-    # L2 flushed between steps outside the events; the top family profiled
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     launches0 = ctx.launches
-    elapsed = 0.0
-    reps = []
     with ClockSampler(local_rank) as clk:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            reps.append(one_step())
-            e1.record(stream)
-            e1.synchronize()
-            elapsed += e0.elapsed_time(e1)
+        elapsed, reps = timed_steps(run, args.steps, stream, flush)
     torch.cuda.synchronize()
     launches = ctx.launches - launches0
-    # Roofline of the dominant kernel family: the same K steps again, issued
-    # as direct launches with CUDA events around every launch of that family
-    # (events cannot sit inside the graph's device-side MG-PCG loop).
+    if world > 1:
+        torch.distributed.barrier()
+    elapsed_max = max_over_ranks(elapsed, world, device)
+    value = world * cells * args.steps / (elapsed_max * 1e-3) / 1e6
+    # Roofline of the dominant kernel family: K more steps issued as direct
+    # launches with CUDA events around every launch of that family (events
+    # cannot sit inside the graph's device-side MG-PCG loop).
     ctx.lib.nb_ctx_profile(ctx.h, top.encode())
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
-        one_step()
+        run.step()
     torch.cuda.synchronize()
     ms, nl, nb = C.c_double(), C.c_uint64(), C.c_double()
     ctx.lib.nb_ctx_profile_read(ctx.h, C.byref(ms), C.byref(nl), C.byref(nb))
     ctx.lib.nb_ctx_profile(ctx.h, None)
-    t = torch.tensor([elapsed], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    elapsed_max = float(t.item())
-    value = world * cells * args.steps / (elapsed_max * 1e-3) / 1e6
     # end to end through the C ABI with host buffers (pinned)
-    pinned = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in ns.get_state()]
+    pinned = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in run.get_state()]
     outs = [torch.empty(a.size, dtype=torch.float64).pin_memory().numpy() for a in pinned]
     n_e2e = max(2, args.steps // 2)
     e2e_ms = 0.0
@@ -185,28 +278,23 @@ def run_ours(args, rank, world, local_rank):
             flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ns.set_state(*pinned)
-        ns.step(dt)
-        st_ = ns.get_state()
-        for o, s in zip(outs, st_):
+        run.set_state(*pinned)
+        run.step()
+        for o, s in zip(outs, run.get_state()):
             o[:] = s
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * cells * n_e2e / (float(te.item()) * 1e-3) / 1e6
+    e2e_value = world * cells * n_e2e / (max_over_ranks(e2e_ms, world, device) * 1e-3) / 1e6
     hbm, peak_kind = peaks()
     achieved = (nb.value / (ms.value * 1e-3) / 1e9) if ms.value > 0 else 0.0
-    per_launch_bytes = nb.value / max(nl.value, 1)
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(elapsed_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == abi.PRECISION_FP64 else "f32+f64",
-        "data": "synthetic (analytic Taylor-Green initial state)",
-        "config": {"workload": desc, "cells": cells, "precision": args.precision,
+        "data": run.data,
+        "config": {"workload": run.desc, "cells": cells, "precision": precision,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed between timed steps (256 MiB write); working set < L2",
                    "poisson_cycles_per_step": reps[-1].poisson_iters},
@@ -216,37 +304,110 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 5),
-                     "bytes_per_launch": per_launch_bytes, "launches": int(nl.value),
+                     "bytes_per_launch": nb.value / max(nl.value, 1), "launches": int(nl.value),
                      "avg_launch_us": round(ms.value * 1e3 / max(nl.value, 1), 3), "traffic": None},
         "kernel_shares": {k: round(v["ms"] / total, 4) for k, v in sorted(shares.items(),
                                                                          key=lambda kv: -kv[1]["ms"])},
-        "divergence_max": reps[-1].divergence_max,
+        "divergence_max": max(r.divergence_max for r in reps),
+        "converged": all(bool(r.converged) for r in reps),
         "clocks": clk.summary(),
     }
+    if args.workload == "channel3":
+        out["forms"], out["accuracy"] = other_form_and_accuracy(args, ctx, run, prec, precision, value,
+                                                                stream, flush, world, device)
     return out
 
 
-def cpu_sample(args, steps):
-    """The reference's CPU step on this host (oracle/_ref); returns s/step."""
+def other_form_and_accuracy(args, ctx, run, prec, precision, value, stream, flush, world, device):
+    """Times the other arithmetic form on the same mesh, then states the mixed
+    form's error against the FP64 form after the same steps from the same state."""
+    import torch
+
+    from nabla_b200 import abi
+    other_prec = abi.PRECISION_FP64 if prec == abi.PRECISION_MIXED else abi.PRECISION_MIXED
+    other_name = "fp64" if precision == "mixed" else "mixed"
+    other = make_run(args.workload, ctx, other_prec, mesh=run.mesh)
+    for _ in range(args.warmup):
+        other.step()
+    torch.cuda.synchronize()
+    el, reps = timed_steps(other, args.steps, stream_of(ctx, other), flush)
+    v_other = world * other.cells * args.steps / (max_over_ranks(el, world, device) * 1e-3) / 1e6
+    forms = {precision: round(value, 4), other_name: round(v_other, 4)}
+    forms["mixed_over_fp64"] = round(forms["mixed"] / forms["fp64"], 4)
+    # accuracy: fresh cases from the initial state, the same number of steps
+    n = 10
+    a = make_run(args.workload, ctx, abi.PRECISION_FP64, mesh=run.mesh)
+    b = make_run(args.workload, ctx, abi.PRECISION_MIXED, mesh=run.mesh)
+    ra = rb = None
+    for _ in range(n):
+        ra, rb = a.step(), b.step()
+    sa, sb = a.get_state(), b.get_state()
+    acc = {"steps": n, "velocity_rel_err": max(rel_err(x, y) for x, y in zip(sb[:3], sa[:3])),
+           "pressure_rel_err": rel_err(sb[3], sa[3]), "mixed_divergence_max": rb.divergence_max,
+           "fp64_divergence_max": ra.divergence_max,
+           "note": "max-norm errors of the mixed form against the FP64 form (same mesh, same steps)"}
+    return forms, acc
+
+
+def stream_of(ctx, run):
+    import torch
+    return torch.cuda.ExternalStream(ctx.lib.nb_case_stream(run.h))
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the reference's own code, oracle/_ref)
+# ---------------------------------------------------------------------------
+def reference_case(name):
+    """(grid, config, state, dt or 0, description) of the reference's CPU run."""
+    from nabla_b200 import cases
+    if name == "tgv64":
+        g, cfg = cases.taylor_green(64)
+        return g, cfg, cases.taylor_green_state(g), None, "the same case"
+    import numpy as np
+
+    from nabla_b200 import abi, workloads
+    w = channel_workload()
+    h = 1.0 / 64.0  # effective fine grid: 256 x 64 x 64
+    nx, ny, nz = 256, 64, 64
+    faces = [dict(type=abi.BC_INLET, profile=abi.PROFILE_UNIFORM, inlet_speed=1.0, inlet_axis=0),
+             dict(type=abi.BC_OUTLET), dict(type=abi.BC_WALL), dict(type=abi.BC_WALL),
+             dict(type=abi.BC_WALL), dict(type=abi.BC_WALL)]
+    g = cases.Grid(nx, ny, nz, h, h, h, faces=faces)
+    zc, yc, xc = np.meshgrid((np.arange(nz) + 0.5) * h, (np.arange(ny) + 0.5) * h, (np.arange(nx) + 0.5) * h,
+                             indexing="ij")
+    g.solid[:] = workloads.inside_boxes(w.boxes, xc.ravel(), yc.ravel(), zc.ravel()).astype(np.uint8)
+    st = []
+    for a, (ex, ey, ez) in enumerate([(nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1)]):
+        off = [0.5, 0.5, 0.5]
+        off[a] = 0.0
+        Z, Y, X = np.meshgrid((np.arange(ez) + off[2]) * h, (np.arange(ey) + off[1]) * h,
+                              (np.arange(ex) + off[0]) * h, indexing="ij")
+        u = w.modes.velocity(X.ravel(), Y.ravel(), Z.ravel())[a]
+        st.append(u + (w.mean_u if a == 0 else 0.0))
+    st.append(np.zeros(g.ncell))
+    return g, w.config, tuple(st), 0.0, "the reference NSSolver on the uniform-fine 256x64x64 version of the case " \
+                                        "(the reference has no octree MAC step)"
+
+
+def cpu_sample(workload_name, steps):
+    """The reference's CPU step on this host (oracle/_ref); returns (s/step, cells, sample)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    g, cfg, st, _ = workload(args.workload)
+    g, cfg, st, dt, sample = reference_case(workload_name)
     ref = oracle.Reference()
     ns = ref.ns(g, cfg)
     ns.set_state(*st)
-    dt = ns.compute_dt()
+    if dt is None:
+        dt = ns.compute_dt()
     t0 = time.perf_counter()
     for _ in range(steps):
         ns.step(dt)
-    return (time.perf_counter() - t0) / steps, g.ncell
+    return (time.perf_counter() - t0) / steps, g.ncell, sample
 
 
-def _ref_worker(q, args_dict, steps, warmup):
-    a = argparse.Namespace(**args_dict)
-    if warmup:
-        cpu_sample(a, warmup)
-    s, cells = cpu_sample(a, steps)
-    q.put((s, cells))
+def _ref_worker(q, workload_name, steps):
+    s, cells, sample = cpu_sample(workload_name, steps)
+    q.put((s, cells, sample))
 
 
 def run_reference(args):
@@ -254,11 +415,10 @@ def run_reference(args):
     case per host core (it has no threading), aggregate Mcell-steps/s."""
     import multiprocessing as mp
     cores = int(os.environ.get("NB_REF_CORES", min(os.cpu_count() or 1, 16)))
-    steps = max(1, args.steps)
+    steps = max(1, min(args.steps, args.cpu_steps))
     ctxm = mp.get_context("spawn")
     q = ctxm.Queue()
-    procs = [ctxm.Process(target=_ref_worker, args=(q, vars(args), steps, min(args.warmup, 1)))
-             for _ in range(cores)]
+    procs = [ctxm.Process(target=_ref_worker, args=(q, args.workload, steps)) for _ in range(cores)]
     t0 = time.perf_counter()
     for p in procs:
         p.start()
@@ -267,17 +427,16 @@ def run_reference(args):
         p.join()
     wall = time.perf_counter() - t0
     s_per_step = max(r[0] for r in res)
-    cells = res[0][1]
+    cells, sample = res[0][1], res[0][2]
     value = cores * cells / s_per_step / 1e6
-    _, _, _, desc = workload(args.workload)
     return {
         "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": args.warmup, "ms_per_step": round(s_per_step * 1e3, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (analytic Taylor-Green initial state)", "impl": "reference",
-        "config": {"workload": desc, "cells": cells, "precision": "fp64"},
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, "cells": cells, "precision": "fp64", "sample": sample},
         "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{steps} NSSolver::step per process, {cores} independent processes"},
+                         "sample": f"{steps} NSSolver::step per process, {cores} independent processes; {sample}"},
         "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 1),
     }
@@ -286,12 +445,13 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tgv64")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
+    ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--shares", type=int, default=1,
                     help="1: time each kernel family once before the timed region")
     args = ap.parse_args()
@@ -312,10 +472,10 @@ def main():
     out = run_ours(args, rank, world, local_rank)
     if rank == 0:
         if args.cpu_steps > 0:
-            s, cells = cpu_sample(args, args.cpu_steps)
+            s, cells, sample = cpu_sample(args.workload, args.cpu_steps)
             out["cpu_baseline"] = {"value": round(cells / s / 1e6, 5), "unit": UNIT, "cores": 1,
                                    "kind": "reference",
-                                   "sample": f"{args.cpu_steps} NSSolver::step of the same case, 1 thread"}
+                                   "sample": f"{args.cpu_steps} NSSolver::step, 1 thread: {sample}"}
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch

@@ -99,9 +99,9 @@ void build_codes(HostLevel& L, const int bc[6]) {
 // MgPoisson hierarchy construction (core/src/flow/multigrid.cpp:211-266):
 // halve an axis only if its length is >= 4, stop at <= 2048 cells or 8 levels;
 // a coarse cell is fluid if any child is fluid.
-std::vector<HostLevel> build_hierarchy(const nb_grid_desc& g) {
+std::vector<HostLevel> build_hierarchy(const nb_grid_desc& g, size_t coarsest_max) {
   constexpr int kMaxLevels = 8;
-  constexpr size_t kCoarsestMax = 2048;
+  const size_t kCoarsestMax = coarsest_max;
   constexpr int kMinCoarsen = 4;
   std::vector<HostLevel> H;
   H.reserve(kMaxLevels);

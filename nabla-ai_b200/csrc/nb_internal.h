@@ -106,7 +106,7 @@ __device__ __forceinline__ int resolve_face(const LevelView& L, int gi, int gj, 
 // ---------------------------------------------------------------------------
 // Device scalar slots of one solve (FP64, in device memory).
 // ---------------------------------------------------------------------------
-constexpr int MAX_LEVELS = 8;
+constexpr int MAX_LEVELS = 16;  // composite octree levels + the uniform tail
 enum Slot : int {
   S_BSUM = 0,   // sum of b over fluid (rhs mean)
   S_BNORM2,     // rhs . rhs
@@ -171,8 +171,10 @@ void build_codes(HostLevel& L, const int bc[6]);
 // solid mask (NULL = none).
 void build_level(HostLevel& L, int nx, int ny, int nz, double dx, double dy, double dz,
                  const uint8_t* solid);
-// Builds the MG hierarchy exactly as MgPoisson::solve does (multigrid.cpp:211-266).
-std::vector<HostLevel> build_hierarchy(const nb_grid_desc& g);
+// Builds the MG hierarchy exactly as MgPoisson::solve does (multigrid.cpp:211-266):
+// halve every axis of >= 4 cells until the coarse level has <= coarsest_max
+// cells (the reference's 2048) or 8 levels exist.
+std::vector<HostLevel> build_hierarchy(const nb_grid_desc& g, size_t coarsest_max = 2048);
 uint64_t grid_signature(const nb_grid_desc& g);  // multigrid.cpp:43-61 (+ spacing)
 
 // Brackets the launches of one kernel family with CUDA events on the

@@ -980,6 +980,8 @@ void MgSolver::common_alloc() {
   const HostLevel& last = lv_.back().h;
   if (lv_.back().v.amr || static_cast<size_t>(last.nx) * last.ny * last.nz > COARSE_MAX_CELLS)
     throw ApiError{NB_ERR_UNSUPPORTED, "coarsest multigrid level exceeds 4096 cells"};
+  if (lv_.size() > static_cast<size_t>(MAX_LEVELS))
+    throw ApiError{NB_ERR_UNSUPPORTED, "multigrid hierarchy deeper than " + std::to_string(MAX_LEVELS) + " levels"};
   n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
   double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
   for (double** v : vecs) {
@@ -1066,7 +1068,12 @@ MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc)
   g0.dz = U.tree.h(0, 2);
   for (int f = 0; f < 6; ++f) g0.face[f].type = geo.bc[f];
   g0.solid = solid.data();
-  std::vector<HostLevel> H = build_hierarchy(g0);
+  // A single-level mesh is a uniform grid and keeps the reference hierarchy
+  // (<= 2048 coarsest cells). Below a multi-level mesh the uniform tail is
+  // coarsened on to <= 512 cells: the coarsest level is solved by one CTA,
+  // whose Jacobi-CG cost grows with the level's size.
+  const size_t coarsest = fine.tree.nlev > 1 ? 512 : 2048;
+  std::vector<HostLevel> H = build_hierarchy(g0, coarsest);
   // Uniform brick ranks equal the single-level tree's ranks (both Morton).
   for (size_t r = 0; r < U.tree.leaves.size(); ++r) {
     const AmrLeaf& f = U.tree.leaves[r];

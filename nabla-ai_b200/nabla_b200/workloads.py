@@ -1,0 +1,171 @@
+"""Seeded synthetic workloads on octree-AMR meshes (host-side set-up only).
+
+``obstacle_channel`` builds the 3-level channel case: [0,4]x[0,1]x[0,1],
+base 64x16x16 cells (8x2x2 bricks of 8^3, h0 = 1/16), refined twice
+(effective 256x64x64) where the initial vorticity is in its top fifth or a
+cell lies within 0.05 of a solid. Uniform inflow U = 1 at x = 0, outlet at
+x = 4, no-slip walls on y and z, nu = 1/1000, CFL 0.4. The obstacle is the
+union of 6 seeded axis-aligned boxes (sides U[0.05, 0.2], centres x in
+U[0.5, 1.5], y, z in U[0.2, 0.8]); a cell is solid when its centre is inside
+a box (staircase, as core/src/flow/case.cpp:113-122 marks the cube). The
+initial velocity is U plus the curl of a seeded Gaussian random vector
+potential whose spectrum peaks at wavenumber 8 (in cycles per unit length),
+scaled to an rms perturbation of 0.05.
+
+Refinement works at brick granularity: a leaf is split when the maximum of
+|omega| over its cells (sampled on the effective finest grid) is in the top
+fifth of that maximum over the leaves of its level, or when any of its cells
+is within 0.05 of a box; 2:1 balance is then restored (nb_amr_refine).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi, amr, cases
+
+
+@dataclass
+class Modes:
+    k: np.ndarray      # [M, 3] angular wave vectors
+    c: np.ndarray      # [M, 3] potential amplitudes
+    phase: np.ndarray  # [M]
+    scale: float = 1.0
+
+    def velocity(self, x, y, z):
+        """curl of A = sum_m c_m cos(k_m . x + phase_m): -sin(theta) (k x c)."""
+        kc = np.cross(self.k, self.c) * self.scale
+        out = [np.zeros_like(x), np.zeros_like(x), np.zeros_like(x)]
+        for m in range(self.k.shape[0]):
+            s = -np.sin(self.k[m, 0] * x + self.k[m, 1] * y + self.k[m, 2] * z + self.phase[m])
+            for d in range(3):
+                out[d] += s * kc[m, d]
+        return out
+
+    def vorticity_mag(self, x, y, z):
+        """|curl curl A| = |-cos(theta) k x (k x c)| summed over modes."""
+        kkc = np.cross(self.k, np.cross(self.k, self.c)) * self.scale
+        w = [np.zeros_like(x), np.zeros_like(x), np.zeros_like(x)]
+        for m in range(self.k.shape[0]):
+            cth = -np.cos(self.k[m, 0] * x + self.k[m, 1] * y + self.k[m, 2] * z + self.phase[m])
+            for d in range(3):
+                w[d] += cth * kkc[m, d]
+        return np.sqrt(w[0] ** 2 + w[1] ** 2 + w[2] ** 2)
+
+
+def random_modes(rng, n_modes=48, k_peak=8.0, k_width=1.5, rms=0.05, sample=None):
+    """Gaussian random vector potential: wave numbers |k|/(2 pi) ~ N(k_peak, k_width),
+    isotropic directions, Gaussian amplitudes; scaled so the velocity rms over
+    `sample` (x, y, z arrays) is `rms`."""
+    kmag = 2.0 * np.pi * np.abs(rng.normal(k_peak, k_width, n_modes))
+    d = rng.normal(size=(n_modes, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    k = d * kmag[:, None]
+    c = rng.normal(size=(n_modes, 3)) / kmag[:, None]
+    phase = rng.uniform(0.0, 2.0 * np.pi, n_modes)
+    m = Modes(k, c, phase)
+    if sample is not None:
+        u = m.velocity(*sample)
+        cur = np.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2))
+        m.scale = rms / cur
+    return m
+
+
+def random_boxes(rng, n=6):
+    """[n, 2, 3] lower/upper corners."""
+    side = rng.uniform(0.05, 0.2, (n, 3))
+    centre = np.stack([rng.uniform(0.5, 1.5, n), rng.uniform(0.2, 0.8, n), rng.uniform(0.2, 0.8, n)], axis=1)
+    return np.stack([centre - side / 2, centre + side / 2], axis=1)
+
+
+def inside_boxes(boxes, x, y, z):
+    s = np.zeros(x.shape, dtype=bool)
+    for lo, hi in boxes:
+        s |= (x > lo[0]) & (x < hi[0]) & (y > lo[1]) & (y < hi[1]) & (z > lo[2]) & (z < hi[2])
+    return s
+
+
+def box_distance(boxes, x, y, z):
+    d = np.full(x.shape, np.inf)
+    for lo, hi in boxes:
+        dx = np.maximum(np.maximum(lo[0] - x, 0.0), x - hi[0])
+        dy = np.maximum(np.maximum(lo[1] - y, 0.0), y - hi[1])
+        dz = np.maximum(np.maximum(lo[2] - z, 0.0), z - hi[2])
+        d = np.minimum(d, np.sqrt(dx * dx + dy * dy + dz * dz))
+    return d
+
+
+@dataclass
+class AmrWorkload:
+    geom: abi.AmrGeom
+    leaves: np.ndarray
+    solid: np.ndarray  # 512 bytes per leaf, in `leaves` order
+    config: abi.FlowConfig
+    modes: Modes
+    boxes: np.ndarray
+    mean_u: float
+    description: str
+
+    def initial_state(self, case: amr.AmrCase):
+        st = []
+        for a in range(3):
+            x, y, z = case.face_positions(a)
+            u = self.modes.velocity(x, y, z)[a]
+            st.append(u + (self.mean_u if a == 0 else 0.0))
+        st.append(np.zeros(case.sizes[3]))
+        return st
+
+
+def _leaf_metric(modes, boxes, leaves, h0, lmax, near):
+    """Per leaf: max |omega| over its region sampled at the finest cell centres
+    (4^3 samples per finest brick-cell block are enough at this resolution:
+    every second finest cell), and whether any of its cells is within `near`
+    of a box."""
+    out_w = np.zeros(len(leaves))
+    out_near = np.zeros(len(leaves), dtype=bool)
+    for q, (lev, bx, by, bz) in enumerate(leaves):
+        h = h0 / (1 << lev)
+        n = 8 << (lmax - lev)  # finest cells per brick edge
+        hf = h0 / (1 << lmax)
+        s = np.arange(0, n, 2) + 0.5
+        X, Y, Z = np.meshgrid(bx * 8 * h + s * hf, by * 8 * h + s * hf, bz * 8 * h + s * hf, indexing="ij")
+        out_w[q] = modes.vorticity_mag(X.ravel(), Y.ravel(), Z.ravel()).max()
+        c = (np.arange(8) + 0.5) * h
+        Xc, Yc, Zc = np.meshgrid(bx * 8 * h + c, by * 8 * h + c, bz * 8 * h + c, indexing="ij")
+        out_near[q] = (box_distance(boxes, Xc.ravel(), Yc.ravel(), Zc.ravel()) <= near).any()
+    return out_w, out_near
+
+
+def obstacle_channel(seed: int = 0, lmax: int = 2, n_boxes: int = 6, precision_note: str = "") -> AmrWorkload:
+    rng = np.random.default_rng(seed)
+    h0 = 1.0 / 16.0
+    nb0 = (8, 2, 2)
+    faces = [dict(type=abi.BC_INLET, profile=abi.PROFILE_UNIFORM, inlet_speed=1.0, inlet_axis=0),
+             dict(type=abi.BC_OUTLET), dict(type=abi.BC_WALL), dict(type=abi.BC_WALL),
+             dict(type=abi.BC_WALL), dict(type=abi.BC_WALL)]
+    geom = amr.make_geom(nb0, (h0, h0, h0), lmax, faces)
+    boxes = random_boxes(rng, n_boxes)
+    sx = rng.uniform(0, 4, 20000)
+    sy, sz = rng.uniform(0, 1, 20000), rng.uniform(0, 1, 20000)
+    modes = random_modes(rng, sample=(sx, sy, sz))
+    leaves = amr.base_leaves(nb0)
+    for lev in range(lmax):
+        w, near = _leaf_metric(modes, boxes, leaves, h0, lmax, 0.05)
+        at = leaves[:, 0] == lev
+        thr = np.percentile(w[at], 80.0) if at.any() else np.inf
+        flags = (at & ((w > thr) | near)).astype(np.uint8)
+        if not flags.any():
+            break
+        leaves = amr.refine(geom, leaves, flags)
+    lev, i, j, k = amr.cell_coords(leaves)
+    h = h0 / (2.0 ** lev)
+    solid = inside_boxes(boxes, (i + 0.5) * h, (j + 0.5) * h, (k + 0.5) * h).astype(np.uint8)
+    cfg = cases.flow_config(reynolds=1000.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
+                            convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
+    nl = np.bincount(leaves[:, 0], minlength=lmax + 1)
+    desc = (f"obstacle channel [0,4]x[0,1]^2, octree of 8^3 bricks, base 64x16x16, {lmax + 1} levels "
+            f"(effective {64 << lmax}x{16 << lmax}x{16 << lmax}), leaves per level {nl.tolist()}, "
+            f"{n_boxes} seeded boxes, inflow U=1 + curl of a k=8 random potential (rms 0.05), "
+            f"nu=1/1000, WENO-5, CFL 0.4, MG-PCG to 1e-10, seed {seed}")
+    return AmrWorkload(geom, leaves, solid, cfg, modes, boxes, 1.0, desc)
