@@ -65,6 +65,15 @@ struct LevelView {
   // transfer to the next coarser MG level: coarse brick, octant (-1 kept)
   const int* xf_brick;
   const int* xf_oct;
+  // ---- per-brick maps for one-round halo staging (fast != 0: every brick is
+  // full, i.e. composite levels and uniform levels whose sizes are multiples
+  // of 8) ----
+  int fast;
+  const int* nbr6;   // [nbrick][6] same-level face neighbour brick (periodic wrap) or -1
+  const int* par;    // [nbrick] brick of the next coarser level holding this brick's parents
+  const int* poct;   // [nbrick] octant bits of this brick in its parent brick, -1 identity
+  const int* npar6;  // [nbrick][6] par of nbr6 (-1 where no neighbour)
+  const int* npoct6; // [nbrick][6] poct of nbr6
 };
 constexpr int CODE_DIRICHLET = 6;
 constexpr int CODE_TYPE = 12;
@@ -259,5 +268,37 @@ struct ApiError {
   nb_status status;
   std::string what;
 };
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch. A kernel launched with launch_pdl may be
+// scheduled while its stream predecessor is still running (hiding the launch
+// latency of the long chains of small multigrid kernels); it calls pdl_wait()
+// before its first access to global memory, which returns once the
+// predecessor grid has completed and its writes are visible. pdl_wait() first
+// lets this grid's own successor be scheduled. In a kernel launched without
+// the attribute both instructions return at once.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  NB_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
 
 }  // namespace nb

@@ -27,6 +27,12 @@ constexpr int NT = 512;          // threads per CTA = cells per brick
 constexpr int MAX_GRID = 148 * 4;  // grid-stride CTA cap (4 CTAs of 512 per SM)
 constexpr double kOmega = 0.8;   // multigrid.cpp:38
 constexpr int COARSE_MAX_CELLS = 4096;
+constexpr int COARSE_PRE_CELLS = 2048;  // coarsest levels up to this size keep a resolved stencil
+
+// Dynamic shared memory of the coarsest-level CTA for n cells.
+inline size_t coarse_smem(size_t n) {
+  return n * (6 * sizeof(double) + 1) + (n <= static_cast<size_t>(COARSE_PRE_CELLS) ? n * 6 * sizeof(int16_t) : 0);
+}
 
 inline int grid_for(int nbrick) { return nbrick < MAX_GRID ? nbrick : MAX_GRID; }
 
@@ -62,6 +68,29 @@ struct XFetch {
     if (xmean) v = v - static_cast<T>(*xmean);
     if (ec) {
       T e = ec[parent(n, gi, gj, gk)];
+      if (ecmean) e = e - static_cast<T>(*ecmean);
+      v = v + e;
+    }
+    return v;
+  }
+  __device__ __forceinline__ bool prolongs() const { return ec != nullptr; }
+  // The same value for the one-round staging: the parent of cell n lies in
+  // brick pb of the coarser level at octant po (-1: cell for cell); composite
+  // levels merge by 2 on every axis, uniform levels by fx, fy, fz.
+  __device__ __forceinline__ T at(int n, int pb, int po, int amr) const {
+    T v = x ? x[n] : T(0);
+    if (xmean) v = v - static_cast<T>(*xmean);
+    if (ec) {
+      const int l = n & 511;
+      int pl = l;
+      if (po >= 0) {
+        const int li = l & 7, lj = (l >> 3) & 7, lk = l >> 6;
+        const int ci = (amr || fx == 2) ? ((po & 1) << 2) + (li >> 1) : li;
+        const int cj = (amr || fy == 2) ? (((po >> 1) & 1) << 2) + (lj >> 1) : lj;
+        const int ck = (amr || fz == 2) ? (((po >> 2) & 1) << 2) + (lk >> 1) : lk;
+        pl = (ck << 6) | (cj << 3) | ci;
+      }
+      T e = ec[pb * BR3 + pl];
       if (ecmean) e = e - static_cast<T>(*ecmean);
       v = v + e;
     }
@@ -149,8 +178,42 @@ __device__ __forceinline__ void fill_halo_amr(const LevelView& L, int brick, T* 
   }
 }
 
+// One-round staging (levels with per-brick maps, 512 threads): thread t loads
+// its own cell; threads 0..383 each load one face-halo cell from the
+// neighbour brick (6 faces x 64). All loads are independent.
+template <typename T, class F>
+__device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T* tile, const F& fx) {
+  const int t = threadIdx.x;
+  const bool pro = fx.prolongs();
+  const int pb = pro ? L.par[brick] : 0, po = pro ? L.poct[brick] : -1;
+  const T own = fx.at(brick * BR3 + t, pb, po, L.amr);
+  T halo = T(0);
+  int hpos = -1;
+  if (t < 384) {
+    const int f = t >> 6, m = t & 63, u = m & 7, w = m >> 3, a = f >> 1, s = f & 1;
+    const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
+    int tc[3], lc[3];
+    tc[a] = s ? 8 : -1;
+    lc[a] = s ? 0 : 7;
+    tc[t1] = lc[t1] = u;
+    tc[t2] = lc[t2] = w;
+    hpos = tpos(tc[0], tc[1], tc[2]);
+    const int nb = L.nbr6[brick * 6 + f];
+    if (nb >= 0) {
+      const int npb = pro ? L.npar6[brick * 6 + f] : 0, npo = pro ? L.npoct6[brick * 6 + f] : -1;
+      halo = fx.at(nb * BR3 + ((lc[2] << 6) | (lc[1] << 3) | lc[0]), npb, npo, L.amr);
+    }
+  }
+  tile[tpos_local(t)] = own;
+  if (hpos >= 0) tile[hpos] = halo;
+}
+
 template <typename T, class F>
 __device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile, const F& fx) {
+  if (L.fast && blockDim.x == BR3) {
+    fill_halo_fast<T>(L, brick, tile, fx);
+    return;
+  }
   if (L.amr) {
     fill_halo_amr<T>(L, brick, tile, fx);
     return;
@@ -232,6 +295,7 @@ __global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict_
                                                const double* bmean, XFetch<T> X, T* __restrict__ xout,
                                                RedBuf rb, double* mean_out, double inv_nfluid,
                                                const SolveFlags* flags, int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   double part[1] = {0.0};
@@ -288,6 +352,7 @@ __global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __r
                                                        int fx, int fy, int fz, T* __restrict__ rc,
                                                        RedBuf rb, double* mean_out, double inv_nfluid_c,
                                                        const SolveFlags* flags, int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   __shared__ T rs[BR3];
@@ -398,16 +463,22 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
                                                   const double* bmean, T* __restrict__ xout,
                                                   int singular, double tol, int maxit_cg,
                                                   const SolveFlags* flags, int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   extern __shared__ double sm[];
   const int n = C.nx * C.ny * C.nz;
+  const bool pre = n <= COARSE_PRE_CELLS;
   double* xs = sm;
   double* rs = xs + n;
   double* ps = rs + n;
   double* zs = ps + n;  // z, then Ap
   double* ds = zs + n;  // preconditioner diagonal
   double* rh = ds + n;  // rhs
-  uint8_t* fl = reinterpret_cast<uint8_t*>(rh + n);
+  // Per-cell stencil, resolved once (levels of <= COARSE_PRE_CELLS cells): the
+  // six neighbours in the row order below; >= 0 coupled cell, -1 no coupling,
+  // -2 Dirichlet outlet face.
+  int16_t* nb6 = reinterpret_cast<int16_t*>(rh + n);
+  uint8_t* fl = pre ? reinterpret_cast<uint8_t*>(nb6 + 6 * n) : reinterpret_cast<uint8_t*>(rh + n);
   __shared__ double red[128];
   const int tid = threadIdx.x;
   auto lex_coords = [&](int m, int& i, int& j, int& k) {
@@ -465,11 +536,58 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
     xs[m] = 0.0;
   }
   __syncthreads();
+  if (pre) {  // resolve every fluid row once, in rowA's face order
+    for (int m = tid; m < n; m += blockDim.x) {
+      if (!fl[m]) continue;
+      int i, j, k;
+      lex_coords(m, i, j, k);
+      const int dims[3] = {C.nx, C.ny, C.nz};
+      for (int f = 0; f < 6; ++f) {
+        const int axis = f >> 1, side = (f & 1) ? 1 : -1;
+        int16_t code = -1;
+        if (!(axis == 2 && C.twoD)) {
+          int c[3] = {i, j, k};
+          c[axis] += side;
+          if (c[axis] < 0 || c[axis] >= dims[axis]) {
+            const int bt = C.bc[2 * axis + (side > 0 ? 1 : 0)];
+            if (bt == NB_BC_PERIODIC) {
+              c[axis] = (c[axis] + dims[axis]) % dims[axis];
+              const int nn = c[0] + C.nx * (c[1] + C.ny * c[2]);
+              if (fl[nn]) code = static_cast<int16_t>(nn);
+            } else if (bt == NB_BC_OUTLET) {
+              code = -2;
+            }
+          } else {
+            const int nn = c[0] + C.nx * (c[1] + C.ny * c[2]);
+            if (fl[nn]) code = static_cast<int16_t>(nn);
+          }
+        }
+        nb6[6 * m + f] = code;
+      }
+    }
+  }
+  // Row of A from the resolved stencil (same face order and sums as rowA).
+  auto rowP = [&](int m, const double* v, double& diag, double& off) {
+    diag = 0.0;
+    off = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int code = nb6[6 * m + f];
+      const double h2 = C.h2[f >> 1];
+      if (code >= 0) {
+        diag += h2;
+        off += h2 * v[code];
+      } else if (code == -2) {
+        diag += 2.0 * h2;
+      }
+    }
+  };
   for (int m = tid; m < n; m += blockDim.x) {
     double d = 1.0;
     if (fl[m]) {
       double dg, off;
-      rowA(m, xs, dg, off);
+      if (pre) rowP(m, xs, dg, off);
+      else rowA(m, xs, dg, off);
       d = dg > 0.0 ? dg : 1.0;
     }
     ds[m] = d;
@@ -502,7 +620,8 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
         ap = ps[m];
       } else {
         double dg, off;
-        rowA(m, ps, dg, off);
+        if (pre) rowP(m, ps, dg, off);
+        else rowA(m, ps, dg, off);
         ap = dg * ps[m] - off;
       }
       zs[m] = ap;
@@ -511,20 +630,20 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
     const double pAp = bsum_bcast(pap_l, red);
     if (fabs(pAp) < 1e-300) break;
     const double alpha = rz / pAp;
-    double rr_l = 0.0;
+    // x, r update with |r|^2 and the next r.z in one pass (each thread owns
+    // its cells; z overwrites Ap cell by cell); z is unused if r has converged.
+    double rr_l = 0.0, rzn_l = 0.0;
     for (int m = tid; m < n; m += blockDim.x) {
       xs[m] += alpha * ps[m];
       rs[m] -= alpha * zs[m];
       rr_l += rs[m] * rs[m];
-    }
-    const double rnorm = sqrt(bsum_bcast(rr_l, red));
-    if (rnorm <= tol * bnorm) break;
-    double rzn_l = 0.0;
-    for (int m = tid; m < n; m += blockDim.x) {
       zs[m] = rs[m] / ds[m];
       rzn_l += rs[m] * zs[m];
     }
-    const double rzNew = bsum_bcast(rzn_l, red);
+    bsum2_bcast(rr_l, rzn_l, red);
+    const double rnorm = sqrt(rr_l);
+    if (rnorm <= tol * bnorm) break;
+    const double rzNew = rzn_l;
     const double beta = rzNew / rz;
     for (int m = tid; m < n; m += blockDim.x) ps[m] = zs[m] + beta * ps[m];
     rz = rzNew;
@@ -555,11 +674,14 @@ struct DFetch {
   __device__ __forceinline__ double operator()(int n, int, int, int) const {
     return xmean ? x[n] - *xmean : x[n];
   }
+  __device__ __forceinline__ bool prolongs() const { return false; }
+  __device__ __forceinline__ double at(int n, int, int, int) const { return xmean ? x[n] - *xmean : x[n]; }
 };
 
 // out = A x, identity rows on solid cells (poisson.cpp:102-134); void cells 0.
 __global__ void __launch_bounds__(NT) k_apply_a(LevelView L, const double* __restrict__ x,
                                                 double* __restrict__ out) {
+  pdl_wait();
   DFetch X{x, nullptr};
   __shared__ double tile[TSN];
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -587,6 +709,7 @@ __global__ void __launch_bounds__(NT) k_fluid_mean(LevelView L, const double* __
                                                    const double* vmean, RedBuf rb, double* mean_out,
                                                    double inv_nfluid, const SolveFlags* flags,
                                                    int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -601,6 +724,7 @@ __global__ void __launch_bounds__(NT) k_fluid_mean_f(LevelView L, const float* _
                                                      const double* vmean, RedBuf rb, double* mean_out,
                                                      double inv_nfluid, const SolveFlags* flags,
                                                      int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -620,6 +744,7 @@ __global__ void __launch_bounds__(NT) k_pcg_setup(LevelView L, const double* __r
                                                   double* __restrict__ r, double* __restrict__ x,
                                                   float* __restrict__ r_f, RedBuf rb, double* S,
                                                   SolveFlags* flags, double tol) {
+  pdl_wait();
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
     const int c = brick * BR3 + threadIdx.x;
@@ -657,6 +782,7 @@ __global__ void __launch_bounds__(NT) k_pcg_dots(LevelView L, const TZ* __restri
                                                  const double* __restrict__ rnew,
                                                  const double* __restrict__ r, int first, RedBuf rb,
                                                  double* S, SolveFlags* flags, int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   double part[2] = {0.0, 0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -693,6 +819,7 @@ __global__ void __launch_bounds__(NT) k_pcg_dots(LevelView L, const TZ* __restri
 __global__ void __launch_bounds__(NT) k_pcg_dir(LevelView L, const double* __restrict__ z,
                                                 double* __restrict__ p, const double* S,
                                                 const SolveFlags* flags, int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   const double beta = S[S_BETA];
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -705,6 +832,7 @@ __global__ void __launch_bounds__(NT) k_pcg_dir(LevelView L, const double* __res
 __global__ void __launch_bounds__(NT) k_pcg_matvec(LevelView L, const double* __restrict__ p,
                                                    double* __restrict__ Ap, RedBuf rb, double* S,
                                                    SolveFlags* flags, int maxit) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   DFetch X{p, nullptr};
   __shared__ double tile[TSN];
@@ -762,6 +890,7 @@ __global__ void __launch_bounds__(NT) k_pcg_update(LevelView L, double* __restri
                                                    int singular, double inv_nfluid, RedBuf rb,
                                                    double* S, SolveFlags* flags, int maxit,
                                                    double tol) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   const double alpha = S[S_ALPHA];
   double part[1] = {0.0};
@@ -787,6 +916,7 @@ __global__ void __launch_bounds__(NT) k_pcg_update(LevelView L, double* __restri
 __global__ void __launch_bounds__(NT) k_pcg_center(LevelView L, double* __restrict__ rnew,
                                                    float* __restrict__ rnew_f, RedBuf rb, double* S,
                                                    SolveFlags* flags, int maxit, double tol) {
+  pdl_wait();
   if (stopped(flags, maxit)) return;
   const double mean = S[S_RMEAN];
   double part[1] = {0.0};
@@ -806,6 +936,7 @@ __global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double*
                                                       const double* xmean,
                                                       const double* __restrict__ rhs,
                                                       double* __restrict__ xf, RedBuf rb, double* S) {
+  pdl_wait();
   DFetch X{x, xmean};
   __shared__ double tile[TSN];
   double part[1] = {0.0};
@@ -843,6 +974,7 @@ __global__ void k_set_cond(cudaGraphConditionalHandle h, const SolveFlags* f, in
 
 // Per-solve report: iterations, stop code, early exit, |rhs|^2, |true residual|^2, NaN.
 __global__ void k_report(const SolveFlags* f, const double* S, double* out) {
+  pdl_wait();
   out[0] = static_cast<double>(f->iters);
   out[1] = static_cast<double>(f->stop);
   out[2] = static_cast<double>(f->early);
@@ -974,6 +1106,85 @@ void MgSolver::upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]) 
     v.xf_brick = D.d_xfb;
     v.xf_oct = D.d_xfo;
   }
+  // same-level face neighbours (the staged halo never reads across a level jump)
+  D.h_nbr6.assign(static_cast<size_t>(nbrick) * 6, -1);
+  for (int r = 0; r < nbrick; ++r) {
+    const AmrLeaf& f = t.leaves[r];
+    for (int face = 0; face < 6; ++face) {
+      const int a = face >> 1;
+      int c[3] = {f.b[0], f.b[1], f.b[2]};
+      c[a] += (face & 1) ? 1 : -1;
+      const int n = t.lnb(f.level, a);
+      if (c[a] < 0 || c[a] >= n) {
+        if (bcs[2 * a] != NB_BC_PERIODIC) continue;
+        c[a] = (c[a] + n) % n;
+      }
+      D.h_nbr6[6 * r + face] = t.find(f.level, c[0], c[1], c[2]);
+    }
+  }
+  D.h_par = A.xf_brick;
+  D.h_poct = A.xf_oct;
+}
+
+// Per-brick maps that let a CTA stage a brick and its face halo (and the
+// parents of both, for the prolongation folded into the first post-smoothing
+// sweep) with one round of independent loads instead of chained LUT lookups.
+void MgSolver::build_halo_maps() {
+  const int nl = static_cast<int>(lv_.size());
+  for (int m = 0; m < nl; ++m) {
+    DevLevel& D = lv_[m];
+    LevelView& v = D.v;
+    const int nb = v.nbrick;
+    if (!v.amr) {
+      const HostLevel& h = D.h;
+      if (h.nx % BR || h.ny % BR || h.nz % BR) continue;  // partial bricks: staged through the LUT
+      D.h_nbr6.assign(static_cast<size_t>(nb) * 6, -1);
+      const int nbs[3] = {h.nbx, h.nby, h.nbz};
+      for (int r = 0; r < nb; ++r)
+        for (int face = 0; face < 6; ++face) {
+          const int a = face >> 1;
+          int c[3] = {h.bcoord[3 * r], h.bcoord[3 * r + 1], h.bcoord[3 * r + 2]};
+          c[a] += (face & 1) ? 1 : -1;
+          if (c[a] < 0 || c[a] >= nbs[a]) {
+            if (v.bc[2 * a] != NB_BC_PERIODIC) continue;
+            c[a] = (c[a] + nbs[a]) % nbs[a];
+          }
+          D.h_nbr6[6 * r + face] = h.lut[(c[2] * h.nby + c[1]) * h.nbx + c[0]];
+        }
+      D.h_par.assign(nb, -1);
+      D.h_poct.assign(nb, -1);
+      if (m + 1 < nl && !lv_[m + 1].v.amr) {
+        const HostLevel& C = lv_[m + 1].h;
+        for (int r = 0; r < nb; ++r) {
+          const int bx = h.bcoord[3 * r], by = h.bcoord[3 * r + 1], bz = h.bcoord[3 * r + 2];
+          const int cx = C.fx == 2 ? bx >> 1 : bx, cy = C.fy == 2 ? by >> 1 : by, cz = C.fz == 2 ? bz >> 1 : bz;
+          D.h_par[r] = C.lut[(cz * C.nby + cy) * C.nbx + cx];
+          D.h_poct[r] = (bx & 1) | ((by & 1) << 1) | ((bz & 1) << 2);
+        }
+      }
+    }
+    if (D.h_par.size() != static_cast<size_t>(nb)) D.h_par.assign(nb, -1);
+    if (D.h_poct.size() != static_cast<size_t>(nb)) D.h_poct.assign(nb, -1);
+    std::vector<int> npar(static_cast<size_t>(nb) * 6, -1), npoct(static_cast<size_t>(nb) * 6, -1);
+    for (size_t q = 0; q < npar.size(); ++q) {
+      const int n = D.h_nbr6[q];
+      if (n >= 0) {
+        npar[q] = D.h_par[n];
+        npoct[q] = D.h_poct[n];
+      }
+    }
+    auto up = [&](const std::vector<int>& src) {
+      int* d = static_cast<int*>(alloc(std::max<size_t>(1, src.size()) * sizeof(int)));
+      if (!src.empty()) NB_CUDA(cudaMemcpy(d, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
+      return d;
+    };
+    v.nbr6 = up(D.h_nbr6);
+    v.par = up(D.h_par);
+    v.poct = up(D.h_poct);
+    v.npar6 = up(npar);
+    v.npoct6 = up(npoct);
+    v.fast = 1;
+  }
 }
 
 void MgSolver::common_alloc() {
@@ -982,6 +1193,7 @@ void MgSolver::common_alloc() {
     throw ApiError{NB_ERR_UNSUPPORTED, "coarsest multigrid level exceeds 4096 cells"};
   if (lv_.size() > static_cast<size_t>(MAX_LEVELS))
     throw ApiError{NB_ERR_UNSUPPORTED, "multigrid hierarchy deeper than " + std::to_string(MAX_LEVELS) + " levels"};
+  build_halo_maps();
   n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
   double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
   for (double** v : vecs) {
@@ -1100,7 +1312,7 @@ MgSolver::~MgSolver() {
 void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
   const LevelView& L = lv_[0].v;
   NB_LAUNCH(lc_, "apply_a", s, lv_[0].ncell * 17,
-            (k_apply_a<<<grid_for(L.nbrick), NT, 0, s>>>(L, x, out)));
+            launch_pdl(k_apply_a, dim3(grid_for(L.nbrick)), dim3(NT), 0, s, L, x, out));
   NB_CUDA(cudaGetLastError());
 }
 
@@ -1117,9 +1329,10 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double tsz = sizeof(T);
   const double ncell = D.ncell;
   if (lvl + 1 == static_cast<int>(lv_.size())) {
-    const size_t smem = static_cast<size_t>(L.nx) * L.ny * L.nz * (6 * sizeof(double) + 1);
+    const size_t nco = static_cast<size_t>(L.nx) * L.ny * L.nz;
+    const size_t smem = coarse_smem(nco);
     NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
-              (k_coarse_cg<T><<<1, NT, smem, s>>>(L, b, bmean, static_cast<T*>(D.x0), singular_ ? 1 : 0,
+              (launch_pdl(k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0), singular_ ? 1 : 0,
                                                   1e-6, 500, flags_, maxit_)));
     *out_x = D.x0;
     *out_mean_slot = -1;
@@ -1137,18 +1350,18 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double ncoarse = Cd.ncell;
   // pre-smoothing (2 sweeps), first from x = 0
   NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
-            (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean,
+            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean,
                                              XFetch<T>{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1}, xa,
                                              rb_, mA, inv_nf, flags_, maxit_)));
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-            (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
+            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
                                              xb, rb_, mB, inv_nf, flags_, maxit_)));
   // residual + restriction
   const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
   double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
   NB_LAUNCH(lc_, "resid_restrict", s, ncell * (2 * tsz + 1) + ncoarse * tsz,
-            (k_resid_restrict<T><<<grid, NT, 0, s>>>(L, b, bmean,
+            (launch_pdl(k_resid_restrict<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean,
                                                      XFetch<T>{xb, mB, nullptr, nullptr, dummy, 1, 1, 1}, C,
                                                      Cd.h.fx, Cd.h.fy, Cd.h.fz, static_cast<T*>(Cd.b), rb_,
                                                      cmean, inv_nfc, flags_, maxit_)));
@@ -1158,12 +1371,12 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
   // post-smoothing: first sweep folds in the prolongation x += P e
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
-            (k_smooth<T><<<grid, NT, 0, s>>>(
+            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,
                 L, b, bmean,
                 XFetch<T>{xb, mB, static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy, Cd.h.fz, D.d_xfb, D.d_xfo}, xa, rb_,
                 mA, inv_nf, flags_, maxit_)));
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-            (k_smooth<T><<<grid, NT, 0, s>>>(L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
+            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
                                              xb, rb_, mB, inv_nf, flags_, maxit_)));
   *out_x = xb;
   *out_mean_slot = sing ? lvl_slot(lvl, 1) : -1;
@@ -1181,13 +1394,13 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   const double zsz = mixed ? 4.0 : 8.0;
   for (int k = 0; k < count; ++k) {
     NB_LAUNCH(lc_, "pcg_matvec", s, n * 17,
-              (k_pcg_matvec<<<grid, NT, 0, s>>>(L, p_, Ap_, rb_, S_, flags_, maxit)));
+              launch_pdl(k_pcg_matvec, dim3(grid), dim3(NT), 0, s, L, p_, Ap_, rb_, S_, flags_, maxit));
     NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0)),
-              (k_pcg_update<<<grid, NT, 0, s>>>(L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
+              (launch_pdl(k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
                                                 sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol)));
     if (sing) {
       NB_LAUNCH(lc_, "pcg_center", s, n * (17 + (mixed ? 4 : 0)),
-                (k_pcg_center<<<grid, NT, 0, s>>>(L, rnew_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, maxit,
+                (launch_pdl(k_pcg_center, dim3(grid), dim3(NT), 0, s, L, rnew_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, maxit,
                                                   tol)));
     }
     void* zx = nullptr;
@@ -1199,22 +1412,22 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
     if (sing) {
       if (mixed)
         NB_LAUNCH(lc_, "pcg_mean", s, n * (zsz + 1),
-                  (k_fluid_mean_f<<<grid, NT, 0, s>>>(L, static_cast<const float*>(zx), m1, rb_, S_ + S_ZMEAN2,
+                  (launch_pdl(k_fluid_mean_f, dim3(grid), dim3(NT), 0, s,L, static_cast<const float*>(zx), m1, rb_, S_ + S_ZMEAN2,
                                                       inv_nf, flags_, maxit)));
       else
         NB_LAUNCH(lc_, "pcg_mean", s, n * (zsz + 1),
-                  (k_fluid_mean<<<grid, NT, 0, s>>>(L, static_cast<const double*>(zx), m1, rb_, S_ + S_ZMEAN2,
+                  (launch_pdl(k_fluid_mean, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, rb_, S_ + S_ZMEAN2,
                                                     inv_nf, flags_, maxit)));
     }
     if (mixed)
       NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
-                (k_pcg_dots<float><<<grid, NT, 0, s>>>(L, static_cast<const float*>(zx), m1, m2, z_, p_, rnew_,
+                (launch_pdl(k_pcg_dots<float>, dim3(grid), dim3(NT), 0, s,L, static_cast<const float*>(zx), m1, m2, z_, p_, rnew_,
                                                        r_, 0, rb_, S_, flags_, maxit)));
     else
       NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
-                (k_pcg_dots<double><<<grid, NT, 0, s>>>(L, static_cast<const double*>(zx), m1, m2, z_, p_,
+                (launch_pdl(k_pcg_dots<double>, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, m2, z_, p_,
                                                         rnew_, r_, 0, rb_, S_, flags_, maxit)));
-    NB_LAUNCH(lc_, "pcg_dir", s, n * 24, (k_pcg_dir<<<grid, NT, 0, s>>>(L, z_, p_, S_, flags_, maxit)));
+    NB_LAUNCH(lc_, "pcg_dir", s, n * 24, launch_pdl(k_pcg_dir, dim3(grid), dim3(NT), 0, s, L, z_, p_, S_, flags_, maxit));
     std::swap(r_, rnew_);
   }
   NB_CUDA(cudaGetLastError());

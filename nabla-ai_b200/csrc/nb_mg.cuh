@@ -26,6 +26,8 @@ struct DevLevel {
   uint16_t* d_code = nullptr;
   int* d_xfb = nullptr;  // composite levels: transfer maps to the next level
   int* d_xfo = nullptr;
+  // host copies for the one-round halo maps (built once all levels exist)
+  std::vector<int> h_nbr6, h_par, h_poct;
   double wfluid = 0.0;   // fluid volume in cell-weight units (= fluid cells on uniform levels)
   double ncell = 0.0;    // cells of the level (for algorithmic byte counts)
   // V-cycle vectors in the level's arithmetic type (double or float):
@@ -91,6 +93,7 @@ class MgSolver {
   void finish(cudaStream_t s, double* report);
   void upload_uniform(DevLevel& D, const int bcs[6]);
   void upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]);
+  void build_halo_maps();
   void common_alloc();
   void* alloc(size_t bytes);
   cudaStream_t side_ = nullptr;               // capture stream of the loop body
