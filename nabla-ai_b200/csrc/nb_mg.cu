@@ -666,6 +666,59 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Exact coarsest-level solve (composite hierarchies): x = Minv (b - mean) on
+// the fluid cells with the host-factored inverse, FP64, one CTA (a warp per
+// row, lanes across columns). rhs preparation and the final mean removal are
+// those of the CG path above.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) k_coarse_direct(LevelView C, const T* __restrict__ b, const double* bmean,
+                                                      T* __restrict__ xout, const double* __restrict__ inv,
+                                                      const int* __restrict__ fmap, const int* __restrict__ lexpos,
+                                                      const int* __restrict__ lexcell, int nf, int singular,
+                                                      const SolveFlags* flags, int maxit) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;
+  extern __shared__ double sm[];
+  double* rh = sm;       // [nf]
+  double* xs = rh + nf;  // [nf]
+  __shared__ double red[128];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const double bm = bmean ? *bmean : 0.0;
+  double s = 0.0;
+  for (int q = tid; q < nf; q += blockDim.x) {
+    const double v = static_cast<double>(b[fmap[q]]) - (bmean ? bm : 0.0);
+    rh[q] = v;
+    s += v;
+  }
+  if (singular && nf > 0) {  // poisson.cpp:160-178 (rhs projected to zero mean)
+    const double mean = bsum_bcast(s, red) / nf;
+    for (int q = tid; q < nf; q += blockDim.x) rh[q] -= mean;
+  }
+  __syncthreads();
+  for (int q = warp; q < nf; q += nwarp) {
+    const double* row = inv + static_cast<size_t>(q) * nf;
+    double acc = 0.0;
+    for (int c = lane; c < nf; c += 32) acc += row[c] * rh[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) xs[q] = acc;
+  }
+  __syncthreads();
+  double mean = 0.0;
+  if (singular && nf > 0) {
+    double t = 0.0;
+    for (int q = tid; q < nf; q += blockDim.x) t += xs[q];
+    mean = bsum_bcast(t, red) / nf;
+  }
+  const int n = C.nx * C.ny * C.nz;
+  for (int m = tid; m < n; m += blockDim.x) {
+    const int q = lexpos[m];
+    xout[lexcell[m]] = static_cast<T>(q >= 0 ? (singular ? xs[q] - mean : xs[q]) : 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // PCG vector kernels on level 0 (FP64).
 // ---------------------------------------------------------------------------
 struct DFetch {
@@ -1126,6 +1179,113 @@ void MgSolver::upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]) 
   D.h_poct = A.xf_oct;
 }
 
+// Exact coarsest-level operator for composite hierarchies: the fluid block of
+// the coarsest uniform level's -Laplacian (the rows k_coarse_cg applies),
+// plus alpha * 1 1^T on the constant mode when the system is singular, inverted
+// by Gauss-Jordan elimination with partial pivoting. Returns false (the CG
+// path stays) when the level is too large or the block is singular (e.g. a
+// fluid region split by solids).
+bool MgSolver::build_dense_coarse() {
+  const DevLevel& D = lv_.back();
+  if (D.v.amr) return false;
+  const HostLevel& h = D.h;
+  const int n = h.nx * h.ny * h.nz;
+  if (n > 1024 || h.solid.size() != static_cast<size_t>(n)) return false;
+  std::vector<int> pos(n, -1), fidx;
+  for (int m = 0; m < n; ++m)
+    if (!h.solid[m]) {
+      pos[m] = static_cast<int>(fidx.size());
+      fidx.push_back(m);
+    }
+  const int nf = static_cast<int>(fidx.size());
+  if (nf == 0) return false;
+  const int dims[3] = {h.nx, h.ny, h.nz};
+  const double h2[3] = {1.0 / (h.dx * h.dx), 1.0 / (h.dy * h.dy), 1.0 / (h.dz * h.dz)};
+  std::vector<double> A(static_cast<size_t>(nf) * nf, 0.0);
+  double diag_sum = 0.0;
+  for (int q = 0; q < nf; ++q) {
+    const int m = fidx[q];
+    const int ijk[3] = {m % h.nx, (m / h.nx) % h.ny, m / (h.nx * h.ny)};
+    double diag = 0.0;
+    for (int axis = 0; axis < 3; ++axis) {
+      if (axis == 2 && h.nz == 1) continue;
+      for (int side = -1; side <= 1; side += 2) {
+        int c[3] = {ijk[0], ijk[1], ijk[2]};
+        c[axis] += side;
+        if (c[axis] < 0 || c[axis] >= dims[axis]) {
+          const int bt = D.v.bc[2 * axis + (side > 0 ? 1 : 0)];
+          if (bt == NB_BC_OUTLET) {
+            diag += 2.0 * h2[axis];
+            continue;
+          }
+          if (bt != NB_BC_PERIODIC) continue;
+          c[axis] = (c[axis] + dims[axis]) % dims[axis];
+        }
+        const int nn = c[0] + h.nx * (c[1] + h.ny * c[2]);
+        if (h.solid[nn]) continue;
+        diag += h2[axis];
+        A[static_cast<size_t>(q) * nf + pos[nn]] -= h2[axis];
+      }
+    }
+    A[static_cast<size_t>(q) * nf + q] += diag;
+    diag_sum += diag;
+  }
+  if (singular_) {
+    const double alpha = diag_sum / nf / nf;
+    for (double& a : A) a += alpha;
+  }
+  // Gauss-Jordan with partial pivoting: [A | I] -> [I | A^-1]
+  std::vector<double> I(static_cast<size_t>(nf) * nf, 0.0);
+  for (int q = 0; q < nf; ++q) I[static_cast<size_t>(q) * nf + q] = 1.0;
+  double amax = 0.0;
+  for (double a : A) amax = std::max(amax, std::fabs(a));
+  for (int col = 0; col < nf; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < nf; ++r)
+      if (std::fabs(A[static_cast<size_t>(r) * nf + col]) > std::fabs(A[static_cast<size_t>(piv) * nf + col])) piv = r;
+    const double pv = A[static_cast<size_t>(piv) * nf + col];
+    if (!(std::fabs(pv) > 1e-12 * amax)) return false;
+    if (piv != col)
+      for (int c = 0; c < nf; ++c) {
+        std::swap(A[static_cast<size_t>(piv) * nf + c], A[static_cast<size_t>(col) * nf + c]);
+        std::swap(I[static_cast<size_t>(piv) * nf + c], I[static_cast<size_t>(col) * nf + c]);
+      }
+    const double inv = 1.0 / pv;
+    for (int c = 0; c < nf; ++c) {
+      A[static_cast<size_t>(col) * nf + c] *= inv;
+      I[static_cast<size_t>(col) * nf + c] *= inv;
+    }
+    for (int r = 0; r < nf; ++r) {
+      if (r == col) continue;
+      const double f = A[static_cast<size_t>(r) * nf + col];
+      if (f == 0.0) continue;
+      for (int c = 0; c < nf; ++c) {
+        A[static_cast<size_t>(r) * nf + c] -= f * A[static_cast<size_t>(col) * nf + c];
+        I[static_cast<size_t>(r) * nf + c] -= f * I[static_cast<size_t>(col) * nf + c];
+      }
+    }
+  }
+  auto cell = [&](int m) {
+    const int i = m % h.nx, j = (m / h.nx) % h.ny, k = m / (h.nx * h.ny);
+    const int b = h.lut[((k >> 3) * h.nby + (j >> 3)) * h.nbx + (i >> 3)];
+    return b * BR3 + (((k & 7) << 6) | ((j & 7) << 3) | (i & 7));
+  };
+  std::vector<int> fmap(nf), lexcell(n);
+  for (int q = 0; q < nf; ++q) fmap[q] = cell(fidx[q]);
+  for (int m = 0; m < n; ++m) lexcell[m] = cell(m);
+  dense_inv_ = static_cast<double*>(alloc(I.size() * sizeof(double)));
+  dense_fmap_ = static_cast<int*>(alloc(fmap.size() * sizeof(int)));
+  dense_lexpos_ = static_cast<int*>(alloc(pos.size() * sizeof(int)));
+  dense_lexcell_ = static_cast<int*>(alloc(lexcell.size() * sizeof(int)));
+  NB_CUDA(cudaMemcpy(dense_inv_, I.data(), I.size() * sizeof(double), cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(dense_fmap_, fmap.data(), fmap.size() * sizeof(int), cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(dense_lexpos_, pos.data(), pos.size() * sizeof(int), cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(dense_lexcell_, lexcell.data(), lexcell.size() * sizeof(int), cudaMemcpyHostToDevice));
+  dense_nf_ = nf;
+  dense_ = true;
+  return true;
+}
+
 // Per-brick maps that let a CTA stage a brick and its face halo (and the
 // parents of both, for the prolongation folded into the first post-smoothing
 // sweep) with one round of independent loads instead of chained LUT lookups.
@@ -1300,6 +1460,9 @@ MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc)
     upload_uniform(lv_[ncomp + l], geo.bc);
   }
   common_alloc();
+  // Below a multi-level mesh (no reference hierarchy to reproduce) the
+  // coarsest level is solved exactly instead of by CgPoisson(1e-6, 500).
+  if (fine.tree.nlev > 1) build_dense_coarse();
 }
 
 MgSolver::~MgSolver() {
@@ -1330,10 +1493,17 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double ncell = D.ncell;
   if (lvl + 1 == static_cast<int>(lv_.size())) {
     const size_t nco = static_cast<size_t>(L.nx) * L.ny * L.nz;
-    const size_t smem = coarse_smem(nco);
-    NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
-              (launch_pdl(k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0), singular_ ? 1 : 0,
-                                                  1e-6, 500, flags_, maxit_)));
+    if (dense_) {
+      NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1) + 8.0 * dense_nf_ * dense_nf_,
+                launch_pdl(k_coarse_direct<T>, dim3(1), dim3(NT), 2 * sizeof(double) * dense_nf_, s, L, b, bmean,
+                           static_cast<T*>(D.x0), dense_inv_, dense_fmap_, dense_lexpos_, dense_lexcell_,
+                           dense_nf_, singular_ ? 1 : 0, flags_, maxit_));
+    } else {
+      const size_t smem = coarse_smem(nco);
+      NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
+                (launch_pdl(k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0),
+                            singular_ ? 1 : 0, 1e-6, 500, flags_, maxit_)));
+    }
     *out_x = D.x0;
     *out_mean_slot = -1;
     return;

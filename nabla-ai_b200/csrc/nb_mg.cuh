@@ -94,8 +94,18 @@ class MgSolver {
   void upload_uniform(DevLevel& D, const int bcs[6]);
   void upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]);
   void build_halo_maps();
+  bool build_dense_coarse();
   void common_alloc();
   void* alloc(size_t bytes);
+  // Exact coarsest-level solve (composite hierarchies only): the inverse of the
+  // fluid block of the coarsest operator (regularised on the constant mode when
+  // singular), host-factored once.
+  bool dense_ = false;
+  int dense_nf_ = 0;
+  double* dense_inv_ = nullptr;   // [nf][nf]
+  int* dense_fmap_ = nullptr;     // fluid row q -> level cell (brick layout)
+  int* dense_lexpos_ = nullptr;   // level cell m (lexicographic) -> fluid row or -1
+  int* dense_lexcell_ = nullptr;  // level cell m (lexicographic) -> brick-layout index
   cudaStream_t side_ = nullptr;               // capture stream of the loop body
   unsigned long long* body_execs_ = nullptr;  // device counter
 
