@@ -81,8 +81,65 @@ class Restatement(_Common):
     def ns(self, grid, cfg):
         return _NS(self.lib, "orc", grid, cfg)
 
+    def amr(self, geom, leaves, cfg, solid=None):
+        return AmrStep(self.lib, geom, leaves, cfg, solid)
+
     def morton_encode(self, x, y, z):
         return self.lib.orc_morton_encode(x, y, z)
+
+
+class AmrStep:
+    """The oracle's octree MAC step (oracle/restate_amr.c). Faces and cells are
+    addressed by (level, i, j, k) index arrays, as AmrCase.face_index and
+    amr.cell_coords produce them."""
+
+    def __init__(self, lib, geom, leaves, cfg, solid=None):
+        self.lib = lib
+        I32 = C.POINTER(C.c_int32)
+        lib.orc_amr_create.restype = C.c_void_p
+        lib.orc_amr_create.argtypes = [C.POINTER(abi.AmrGeom), I32, C.c_int64, C.POINTER(C.c_uint8), FP]
+        lib.orc_amr_destroy.argtypes = [C.c_void_p]
+        lib.orc_amr_set.argtypes = [C.c_void_p, C.c_int, C.c_int64, I32, I32, I32, I32, DP]
+        lib.orc_amr_get.argtypes = [C.c_void_p, C.c_int, C.c_int64, I32, I32, I32, I32, DP]
+        lib.orc_amr_step.restype = C.c_double
+        lib.orc_amr_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_int)]
+        self._leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+        sp = None
+        if solid is not None:
+            self._solid = np.ascontiguousarray(solid, dtype=np.uint8)
+            sp = self._solid.ctypes.data_as(C.POINTER(C.c_uint8))
+        self._cfg = cfg
+        self.h = lib.orc_amr_create(C.byref(geom), self._leaves.ctypes.data_as(I32), self._leaves.shape[0], sp,
+                                    C.byref(cfg))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_amr_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def _idx(ix):
+        return [np.ascontiguousarray(a, dtype=np.int32) for a in ix]
+
+    def set(self, comp, index, values):
+        lev, i, j, k = self._idx(index)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        P = C.POINTER(C.c_int32)
+        self.lib.orc_amr_set(self.h, comp, v.size, lev.ctypes.data_as(P), i.ctypes.data_as(P), j.ctypes.data_as(P),
+                             k.ctypes.data_as(P), abi.dptr(v))
+
+    def get(self, comp, index):
+        lev, i, j, k = self._idx(index)
+        out = np.zeros(lev.size)
+        P = C.POINTER(C.c_int32)
+        self.lib.orc_amr_get(self.h, comp, lev.size, lev.ctypes.data_as(P), i.ctypes.data_as(P), j.ctypes.data_as(P),
+                             k.ctypes.data_as(P), abi.dptr(out))
+        return out
+
+    def step(self, dt, tol=1e-13):
+        it = C.c_int()
+        dmax = self.lib.orc_amr_step(self.h, dt, tol, C.byref(it))
+        return dmax, it.value
 
 
 class Reference(_Common):
