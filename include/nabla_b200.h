@@ -136,6 +136,17 @@ nb_status nb_step(nb_case* c, double dt, nb_step_report* rep);
 /* Runs `nsteps` fixed-dt steps without reading any report back (resident
  * throughput path); the last step's report is written to `rep` if non-NULL. */
 nb_status nb_step_many(nb_case* c, double dt, int nsteps, nb_step_report* rep);
+/* Batched stepping of independent cases (uniform or octree, FP64 or mixed)
+ * created on `ctx`: each of the `nsteps` steps of all `n` cases is ONE CUDA
+ * graph launch whose independent branches are the cases' own steps (their
+ * dt from their CFL condition when dt <= 0, else the fixed dt; their
+ * device-side MG-PCG loops), so the small kernels of different cases overlap
+ * on the GPU. `reports` (n entries, may be NULL) receives each case's last
+ * StepReport. The graph is built on first use for a given case list and
+ * reused; destroying a case drops the graphs that contain it. No reference
+ * counterpart: the reference steps one NSSolver at a time. */
+nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, int nsteps,
+                        nb_step_report* reports);
 /* Device bytes held by the case (admission control uses this). */
 uint64_t nb_case_device_bytes(const nb_case* c);
 /* Leaf cells of the case (Mcell-steps/s numerator). */

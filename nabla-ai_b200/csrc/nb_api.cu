@@ -431,6 +431,8 @@ void issue_step(nb_case& c, int cur, bool cfl_dt, bool direct) {
                           cudaMemcpyDeviceToDevice, c.stream));
 }
 
+void finish_step(nb_case& c, nb_step_report* rep);
+
 // One step. Without profiling the step runs as one CUDA graph (built on first
 // use per state parity and dt mode): one launch and one small read-back per step.
 void do_step(nb_case& c, double dt, nb_step_report* rep) {
@@ -466,13 +468,19 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
   }
   NB_CUDA(cudaMemcpyAsync(c.h_blk, c.d_blk, sizeof(StepBlock), cudaMemcpyDeviceToHost, c.stream));
   NB_CUDA(cudaStreamSynchronize(c.stream));
-  const StepBlock& hb = *c.h_blk;
   if (!direct) {
     const GraphSlot& gs = c.graphs[c.cur][cfl_dt ? 1 : 0];
-    c.ctx->launches += gs.fixed_kernels + (hb.execs - c.last_execs) * gs.body_kernels;
+    c.ctx->launches += gs.fixed_kernels + (c.h_blk->execs - c.last_execs) * gs.body_kernels;
   }
+  finish_step(c, rep);
+}
+
+// Host side of a finished step once c.h_blk holds its results: clock, state
+// parity and the StepReport (ns_solver.cpp:797-823).
+void finish_step(nb_case& c, nb_step_report* rep) {
+  const StepBlock& hb = *c.h_blk;
   c.last_execs = hb.execs;
-  dt = hb.dt;
+  const double dt = hb.dt;
   c.cur = 1 - c.cur;  // the stage-3 output is the new state
   c.step += 1;
   c.t += dt;
@@ -514,6 +522,88 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
   }
   rep->cell_count = c.amr ? static_cast<uint64_t>(c.fm.nbrick) * BR3 : static_cast<uint64_t>(g.nx) * g.ny * g.nz;
   rep->accepted = (rep->continuity_residual < c.cfg.tol_continuity && rep->mass_error < c.cfg.tol_mass) ? 1 : 0;
+}
+
+// ---- batches: one graph per step of a set of cases ---------------------------
+void destroy_batch(BatchGraph& bg) {
+  if (bg.exec) cudaGraphExecDestroy(bg.exec);
+  if (bg.graph) cudaGraphDestroy(bg.graph);
+  bg.exec = nullptr;
+  bg.graph = nullptr;
+}
+
+void drop_batches_with(nb_ctx* ctx, const nb_case* c) {
+  const uintptr_t id = reinterpret_cast<uintptr_t>(c);
+  for (auto it = ctx->batch_cache.begin(); it != ctx->batch_cache.end();) {
+    bool has = false;
+    for (size_t q = 0; q < it->first.size(); q += 3) has = has || it->first[q] == id;
+    if (has) {
+      destroy_batch(it->second);
+      it = ctx->batch_cache.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+// One step of every case, as one graph: each case's whole step (its CFL dt or
+// the fixed dt already in its step block, its three projections with their
+// device-side MG-PCG loops, the report copy) is a branch captured from the
+// case's own stream between a fork and a join on the context stream.
+void batch_step(nb_ctx* ctx, nb_case* const* cs, int n, bool cfl_dt, nb_step_report* reps) {
+  std::vector<uintptr_t> key;
+  key.reserve(3 * static_cast<size_t>(n));
+  for (int q = 0; q < n; ++q) {
+    key.push_back(reinterpret_cast<uintptr_t>(cs[q]));
+    key.push_back(static_cast<uintptr_t>(cs[q]->cur));
+    key.push_back(cfl_dt ? 1u : 0u);
+  }
+  auto it = ctx->batch_cache.find(key);
+  if (it == ctx->batch_cache.end()) {
+    BatchGraph bg;
+    cudaEvent_t ev = nullptr;
+    NB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    const uint64_t before = ctx->launches;
+    NB_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      NB_CUDA(cudaEventRecord(ev, ctx->stream));
+      for (int q = 0; q < n; ++q) {
+        nb_case& c = *cs[q];
+        NB_CUDA(cudaStreamWaitEvent(c.stream, ev, 0));
+        issue_step(c, c.cur, cfl_dt, false);
+        bg.body_kernels.push_back(c.body_kernels);
+        NB_CUDA(cudaMemcpyAsync(c.h_blk, c.d_blk, sizeof(StepBlock), cudaMemcpyDeviceToHost, c.stream));
+      }
+      for (int q = 0; q < n; ++q) {
+        NB_CUDA(cudaEventRecord(ev, cs[q]->stream));
+        NB_CUDA(cudaStreamWaitEvent(ctx->stream, ev, 0));
+      }
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(ctx->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaEventDestroy(ev);
+      ctx->launches = before;
+      throw;
+    }
+    NB_CUDA(cudaStreamEndCapture(ctx->stream, &bg.graph));
+    cudaEventDestroy(ev);
+    const cudaError_t e = cudaGraphInstantiate(&bg.exec, bg.graph, 0);
+    if (e != cudaSuccess) {
+      destroy_batch(bg);
+      ctx->launches = before;
+      NB_CUDA(e);
+    }
+    bg.fixed_kernels = ctx->launches - before;
+    ctx->launches = before;
+    it = ctx->batch_cache.emplace(key, std::move(bg)).first;
+  }
+  NB_CUDA(cudaGraphLaunch(it->second.exec, ctx->stream));
+  NB_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->launches += it->second.fixed_kernels;
+  for (int q = 0; q < n; ++q)
+    ctx->launches += (cs[q]->h_blk->execs - cs[q]->last_execs) * it->second.body_kernels[q];
+  for (int q = 0; q < n; ++q) finish_step(*cs[q], reps ? &reps[q] : nullptr);
 }
 
 MgSolver& ctx_solver(nb_ctx* ctx, const nb_grid_desc& g, int precision) {
@@ -583,6 +673,8 @@ void nb_ctx_destroy(nb_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->batch_cache) destroy_batch(kv.second);
+  ctx->batch_cache.clear();
   ctx->mg_cache.clear();
   if (ctx->stage_a) cudaFree(ctx->stage_a);
   if (ctx->stage_b) cudaFree(ctx->stage_b);
@@ -694,7 +786,39 @@ nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_co
 void nb_case_destroy(nb_case* c) {
   if (!c) return;
   cudaSetDevice(c->ctx->device);
+  if (c->ctx->stream) cudaStreamSynchronize(c->ctx->stream);
+  drop_batches_with(c->ctx, c);
   delete c;
+}
+
+// Steps every case of `cases` nsteps times; each step of all of them is one
+// CUDA graph launch (see batch_step).
+nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, int nsteps,
+                        nb_step_report* reports) {
+  if (!ctx || !cases || n <= 0 || nsteps < 0) return NB_ERR_BAD_ARG;
+  for (int q = 0; q < n; ++q) {
+    if (!cases[q] || cases[q]->ctx != ctx) return fail(ctx, NB_ERR_BAD_ARG, "batch cases must belong to the context");
+    for (int r = 0; r < q; ++r)
+      if (cases[r] == cases[q]) return fail(ctx, NB_ERR_BAD_ARG, "a case appears twice in the batch");
+  }
+  if (!ctx->prof.family.empty()) return fail(ctx, NB_ERR_UNSUPPORTED, "batch steps run as graphs: switch profiling off");
+  return guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    const bool cfl_dt = dt <= 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+      if (!cfl_dt)
+        for (int q = 0; q < n; ++q) {
+          cases[q]->h_dt[0] = dt;
+          NB_CUDA(cudaMemcpyAsync(&cases[q]->d_blk->dt, cases[q]->h_dt, sizeof(double), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+        }
+      batch_step(ctx, cases, n, cfl_dt, reports);
+    }
+    if (reports)
+      for (int q = 0; q < n; ++q)
+        if (std::isnan(reports[q].momentum_residual)) return fail(ctx, NB_ERR_NAN, "NaN in the step diagnostics");
+    return NB_OK;
+  });
 }
 
 uint64_t nb_case_device_bytes(const nb_case* c) {

@@ -7,12 +7,26 @@
 #include "nb_internal.h"
 #include "nb_mg.cuh"
 
+namespace nb {
+// One step of a set of cases as a single CUDA graph: every case's step is an
+// independent branch (captured from the case's own stream), so one launch
+// advances all of them and their kernels overlap on the device.
+struct BatchGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t fixed_kernels = 0;        // kernels outside the MG-PCG loop bodies
+  std::vector<uint64_t> body_kernels;  // per case: kernels per loop-body execution
+};
+}  // namespace nb
+
 struct nb_ctx {
   int device = 0;
   std::string err;
   uint64_t launches = 0;
   nb::Profiler prof;
   cudaStream_t stream = nullptr;
+  // batch graphs keyed by (case, state parity) pairs
+  std::map<std::vector<uintptr_t>, nb::BatchGraph> batch_cache;
   // MgPoisson-style cache for the host-array Poisson seam (multigrid.cpp:211-220)
   std::map<std::pair<uint64_t, int>, std::unique_ptr<nb::MgSolver>> mg_cache;
   double* stage_a = nullptr;

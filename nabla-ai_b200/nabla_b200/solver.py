@@ -178,3 +178,19 @@ class NSSolver:
     @property
     def cell_count(self) -> int:
         return self.ctx.lib.nb_case_cell_count(self.h)
+
+
+def batch_step(cases, dt: float = 0.0, nsteps: int = 1):
+    """Steps independent cases (NSSolver or amr.AmrCase objects of one
+    context) together: each step of all of them is one CUDA graph launch
+    (nb_batch_step). Returns each case's last StepReport."""
+    cases = list(cases)
+    if not cases:
+        return []
+    ctx = cases[0].ctx
+    if any(c.ctx is not ctx for c in cases):
+        raise ValueError("batch cases must share one context")
+    hs = (C.c_void_p * len(cases))(*[c.h.value if isinstance(c.h, C.c_void_p) else c.h for c in cases])
+    reps = (abi.StepReport * len(cases))()
+    ctx.check(ctx.lib.nb_batch_step(ctx.h, hs, len(cases), dt, nsteps, reps), "nb_batch_step")
+    return list(reps)
