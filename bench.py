@@ -355,6 +355,123 @@ def stream_of(ctx, run):
 
 
 # ---------------------------------------------------------------------------
+# batched workload: 96 independent octree TGV boxes stepped together
+# ---------------------------------------------------------------------------
+def make_batch(ctx, prec, n):
+    from nabla_b200 import amr, workloads
+    runs = []
+    for seed in range(n):
+        w = workloads.tgv_box_case(seed)
+        mesh = amr.AmrMesh(w.geom, w.leaves, solid=w.solid, ctx=ctx)
+        case = amr.AmrCase(mesh, w.config, precision=prec)
+        case.set_state(*w.initial_state(case))
+        case._mesh_keepalive = mesh
+        runs.append(case)
+    return runs
+
+
+def run_batch(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from nabla_b200 import abi, solver
+
+    device = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    ctx = solver.Context(local_rank)
+    precision = args.precision or "mixed"
+    prec = abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64
+    t0 = time.perf_counter()
+    batch = make_batch(ctx, prec, args.batch)
+    setup_s = time.perf_counter() - t0
+    cells = sum(c.cell_count for c in batch)
+    stream = torch.cuda.ExternalStream(ctx.lib.nb_ctx_stream(ctx.h))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    t0 = time.perf_counter()
+    solver.batch_step(batch, 0.0, max(1, args.warmup))
+    warm_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = ctx.launches
+    elapsed = 0.0
+    reps = None
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            reps = solver.batch_step(batch, 0.0, 1)
+            e1.record(stream)
+            e1.synchronize()
+            elapsed += e0.elapsed_time(e1)
+    launches = ctx.launches - launches0
+    elapsed_max = max_over_ranks(elapsed, world, device)
+    value = world * cells * args.steps / (elapsed_max * 1e-3) / 1e6
+    # end to end: every case's state from pinned host memory, one batch step, back to host
+    pinned = [[torch.from_numpy(a.copy()).pin_memory().numpy() for a in c.get_state()] for c in batch]
+    n_e2e = 2
+    e2e_ms = 0.0
+    for _ in range(n_e2e):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for c, st in zip(batch, pinned):
+            c.set_state(*st)
+        solver.batch_step(batch, 0.0, 1)
+        for c, st in zip(batch, pinned):
+            for o, s in zip(st, c.get_state()):
+                o[:] = s
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    e2e_value = world * cells * n_e2e / (max_over_ranks(e2e_ms, world, device) * 1e-3) / 1e6
+    nbytes = sum(a.nbytes for st in pinned for a in st)
+    # kernel shares and roofline: direct-launch profiled steps of the largest case
+    big = max(batch, key=lambda c: c.cell_count)
+
+    class _Big:
+        h = big.h
+
+        @staticmethod
+        def step():
+            return big.step(0.0)
+
+    shares = {fam: dict(zip(("ms", "launches", "bytes"), profile_step(ctx, _Big, fam))) for fam in FAMILIES}
+    total = sum(v["ms"] for v in shares.values()) or 1.0
+    top = max(shares, key=lambda k: shares[k]["ms"])
+    ms, nl, nb = shares[top]["ms"], shares[top]["launches"], shares[top]["bytes"]
+    hbm, peak_kind = peaks()
+    achieved = nb / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    return {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(elapsed_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == abi.PRECISION_FP64 else "f32+f64",
+        "data": "synthetic (96 seeded Taylor-Green boxes with seeded obstacles)",
+        "config": {"workload": f"batched: {args.batch} independent octree TGV boxes, base grids in {{16..64}}^3, "
+                               "1-3 levels, 0-6 boxes each, nu=1/1600, WENO-5, CFL 0.4, MG-PCG to 1e-10; "
+                               "each step of all cases is one CUDA graph launch",
+                   "cases": args.batch, "cells": cells, "precision": precision,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "setup_s": round(setup_s, 1), "first_steps_s": round(warm_s, 1)},
+        "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(nbytes),
+                "d2h_bytes_per_step": int(nbytes)},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 5),
+                     "case": "largest case of the batch, direct-launch profiled step",
+                     "bytes_per_launch": nb / max(nl, 1), "launches": int(nl), "traffic": None},
+        "kernel_shares": {k: round(v["ms"] / total, 4) for k, v in sorted(shares.items(), key=lambda kv: -kv[1]["ms"])},
+        "divergence_max": max(r.divergence_max for r in reps),
+        "converged": all(bool(r.converged) for r in reps),
+        "clocks": clk.summary(),
+    }
+
+
+# ---------------------------------------------------------------------------
 # CPU baselines (the reference's own code, oracle/_ref)
 # ---------------------------------------------------------------------------
 def reference_case(name):
@@ -363,6 +480,10 @@ def reference_case(name):
     if name == "tgv64":
         g, cfg = cases.taylor_green(64)
         return g, cfg, cases.taylor_green_state(g), None, "the same case"
+    if name == "batch96":
+        g, cfg = cases.taylor_green(64)
+        return g, cfg, cases.taylor_green_state(g), None, \
+            "the reference NSSolver on the uniform 64^3 TGV box (the reference has no octree or batched path)"
     import numpy as np
 
     from nabla_b200 import abi, workloads
@@ -448,7 +569,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64"])
+    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96"])
+    ap.add_argument("--batch", type=int, default=96, help="cases of the batch96 workload")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)
@@ -469,7 +591,7 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
-    out = run_ours(args, rank, world, local_rank)
+    out = (run_batch if args.workload == "batch96" else run_ours)(args, rank, world, local_rank)
     if rank == 0:
         if args.cpu_steps > 0:
             s, cells, sample = cpu_sample(args.workload, args.cpu_steps)

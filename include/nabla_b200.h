@@ -109,6 +109,8 @@ const char* nb_last_error(const nb_ctx* ctx);
 const char* nb_status_string(nb_status s);
 /* Kernel launches issued by this context since creation (evidence counter). */
 uint64_t nb_ctx_launch_count(const nb_ctx* ctx);
+/* The context's cudaStream_t (batch graphs launch on it; for caller-side events). */
+void* nb_ctx_stream(const nb_ctx* ctx);
 nb_status nb_ctx_synchronize(nb_ctx* ctx);
 
 /* ---- cases: one NS problem resident on the device ----------------------- */

@@ -686,6 +686,8 @@ const char* nb_last_error(const nb_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 
 uint64_t nb_ctx_launch_count(const nb_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+void* nb_ctx_stream(const nb_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
 nb_status nb_ctx_synchronize(nb_ctx* ctx) {
   if (!ctx) return NB_ERR_BAD_ARG;
   return guarded(ctx, [&] {

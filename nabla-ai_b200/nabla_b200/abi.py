@@ -131,6 +131,7 @@ PROTOTYPES = [
     ("nb_status_string", C.c_char_p, [C.c_int]),
     ("nb_ctx_launch_count", C.c_uint64, [VP]),
     ("nb_ctx_synchronize", C.c_int, [VP]),
+    ("nb_ctx_stream", VP, [VP]),
     ("nb_case_create", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(FlowConfig), C.c_int, C.POINTER(VP)]),
     ("nb_case_destroy", None, [VP]),
     ("nb_case_initialize", C.c_int, [VP]),

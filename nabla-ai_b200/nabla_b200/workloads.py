@@ -137,6 +137,81 @@ def _leaf_metric(modes, boxes, leaves, h0, lmax, near):
     return out_w, out_near
 
 
+def _tgv_vorticity(x, y, z):
+    """|curl u| of u = sin x cos y cos z, v = -cos x sin y cos z, w = 0."""
+    wx = -np.cos(x) * np.sin(y) * np.sin(z)
+    wy = -np.sin(x) * np.cos(y) * np.sin(z)
+    wz = 2.0 * np.sin(x) * np.sin(y) * np.cos(z)
+    return np.sqrt(wx * wx + wy * wy + wz * wz)
+
+
+@dataclass
+class TgvBoxWorkload:
+    geom: abi.AmrGeom
+    leaves: np.ndarray
+    solid: np.ndarray
+    config: abi.FlowConfig
+    base: int
+    levels: int
+    n_boxes: int
+
+    def initial_state(self, case: amr.AmrCase):
+        st = []
+        for a in range(3):
+            x, y, z = case.face_positions(a)
+            if a == 0:
+                st.append(np.sin(x) * np.cos(y) * np.cos(z))
+            elif a == 1:
+                st.append(-np.cos(x) * np.sin(y) * np.cos(z))
+            else:
+                st.append(np.zeros_like(x))
+        st.append(np.zeros(case.sizes[3]))
+        return st
+
+
+def tgv_box_case(seed: int) -> TgvBoxWorkload:
+    """One case of the batched workload: the Taylor-Green box [0, 2 pi]^3 on a
+    base grid drawn from {16, 24, 32, 48, 64}^3 with 1 to 3 octree levels and
+    0 to 6 seeded boxes (sides U[0.05, 0.2] x 2 pi), refined at brick
+    granularity where the TGV vorticity is in its top fifth or near a box."""
+    rng = np.random.default_rng(1000 + seed)
+    base = int(rng.choice([16, 24, 32, 48, 64]))
+    levels = int(rng.integers(1, 4))
+    n_boxes = int(rng.integers(0, 7))
+    L = 2.0 * np.pi
+    h0 = L / base
+    nb0 = (base // 8,) * 3
+    geom = amr.make_geom(nb0, (h0, h0, h0), levels - 1, cases.periodic_faces())
+    side = rng.uniform(0.05, 0.2, (n_boxes, 3)) * L
+    centre = rng.uniform(0.0, L, (n_boxes, 3))
+    boxes = np.stack([centre - side / 2, centre + side / 2], axis=1) if n_boxes else np.zeros((0, 2, 3))
+    leaves = amr.base_leaves(nb0)
+    for lev in range(levels - 1):
+        at = leaves[:, 0] == lev
+        w = np.zeros(len(leaves))
+        near = np.zeros(len(leaves), dtype=bool)
+        for q in np.nonzero(at)[0]:
+            lv, bx, by, bz = leaves[q]
+            h = h0 / (1 << lv)
+            c = (np.arange(8) + 0.5) * h
+            X, Y, Z = np.meshgrid(bx * 8 * h + c, by * 8 * h + c, bz * 8 * h + c, indexing="ij")
+            w[q] = _tgv_vorticity(X, Y, Z).max()
+            if n_boxes:
+                near[q] = (box_distance(boxes, X.ravel(), Y.ravel(), Z.ravel()) <= 0.05 * L).any()
+        thr = np.percentile(w[at], 80.0)
+        flags = (at & ((w > thr) | near)).astype(np.uint8)
+        if not flags.any():
+            break
+        leaves = amr.refine(geom, leaves, flags)
+    lev, i, j, k = amr.cell_coords(leaves)
+    h = h0 / (2.0 ** lev)
+    solid = inside_boxes(boxes, (i + 0.5) * h, (j + 0.5) * h, (k + 0.5) * h).astype(np.uint8) if n_boxes else \
+        np.zeros(lev.size, dtype=np.uint8)
+    cfg = cases.flow_config(reynolds=1600.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
+                            convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
+    return TgvBoxWorkload(geom, leaves, solid, cfg, base, int(leaves[:, 0].max()) + 1, n_boxes)
+
+
 def obstacle_channel(seed: int = 0, lmax: int = 2, n_boxes: int = 6, precision_note: str = "") -> AmrWorkload:
     rng = np.random.default_rng(seed)
     h0 = 1.0 / 16.0
