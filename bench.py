@@ -472,6 +472,78 @@ def run_batch(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+# serving: open-loop Poisson arrivals through the continuous-batching loop
+# ---------------------------------------------------------------------------
+def serve_requests(args, seed):
+    import numpy as np
+
+    from nabla_b200 import amr, serving, workloads
+    rng = np.random.default_rng(seed)
+    arrivals = serving.poisson_arrivals(args.rate, args.serve_seconds, seed)
+    # request payloads (mesh leaves, solids, config) exist before the clock
+    # starts, as a client's case description would
+    pool = []
+    s = 0
+    while len(pool) < 64:
+        w = workloads.tgv_box_case(s)
+        if len(w.leaves) * 512 <= args.max_cells:
+            pool.append(w)
+        s += 1
+
+    def builder(w):
+        def build(ctx, precision):
+            mesh = amr.AmrMesh(w.geom, w.leaves, solid=w.solid, ctx=ctx)
+            case = amr.AmrCase(mesh, w.config, precision=precision)
+            case.set_state(*w.initial_state(case))
+            case._mesh_keepalive = mesh
+            return case
+        return build
+
+    reqs = []
+    for i, t in enumerate(arrivals):
+        w = pool[int(rng.integers(len(pool)))]
+        steps = int(rng.integers(args.min_steps, args.max_steps + 1))
+        reqs.append(serving.Request(i, float(t), steps, builder(w), len(w.leaves) * 512))
+    return reqs
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+
+    from nabla_b200 import abi, serving, solver
+    torch.cuda.set_device(local_rank)
+    ctx = solver.Context(local_rank)
+    forms = {}
+    for name, prec in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
+        reqs = serve_requests(args, 7 + rank)
+        with ClockSampler(local_rank) as clk:
+            st = serving.Server(ctx, hbm_budget=150e9, precision=prec, slots=args.slots).run(
+                reqs, time_limit=args.serve_seconds * 2)
+        s = st.summary()
+        s["clocks"] = clk.summary()
+        s["divergence_max"] = None
+        forms[name] = s
+    primary = forms[args.precision or "mixed"]
+    return {
+        "metric": METRIC, "value": round(primary["mcell_steps_per_s"], 4), "unit": UNIT, "n_gpus": world,
+        "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if (args.precision or "mixed") == "mixed" else "f64",
+        "data": "synthetic (seeded Poisson arrivals of seeded octree TGV boxes)",
+        "config": {"workload": f"serving: Poisson arrivals at {args.rate}/s for {args.serve_seconds} s, each request "
+                               f"an octree TGV box (<= {args.max_cells} leaf cells) for {args.min_steps}-"
+                               f"{args.max_steps} steps, HBM budget 150 GB, continuous batching "
+                               f"(per-case step graphs overlapped on the device, {args.slots} slots); the loop "
+                               "runs for twice the arrival window",
+                   "precision": args.precision or "mixed"},
+        "latency": {"p50_s": round(primary["p50_latency_s"], 4), "p99_s": round(primary["p99_latency_s"], 4)},
+        "forms": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items() if kk != "clocks"}
+                  for k, v in forms.items()},
+        "gpu_launches": int(ctx.launches),
+        "clocks": forms["mixed"]["clocks"],
+    }
+
+
+# ---------------------------------------------------------------------------
 # CPU baselines (the reference's own code, oracle/_ref)
 # ---------------------------------------------------------------------------
 def reference_case(name):
@@ -480,7 +552,7 @@ def reference_case(name):
     if name == "tgv64":
         g, cfg = cases.taylor_green(64)
         return g, cfg, cases.taylor_green_state(g), None, "the same case"
-    if name == "batch96":
+    if name in ("batch96", "serve"):
         g, cfg = cases.taylor_green(64)
         return g, cfg, cases.taylor_green_state(g), None, \
             "the reference NSSolver on the uniform 64^3 TGV box (the reference has no octree or batched path)"
@@ -569,8 +641,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96"])
+    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96", "serve"])
     ap.add_argument("--batch", type=int, default=96, help="cases of the batch96 workload")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="serve: arrival window")
+    ap.add_argument("--min-steps", type=int, default=10)
+    ap.add_argument("--max-steps", type=int, default=40)
+    ap.add_argument("--max-cells", type=int, default=300_000, help="serve: leaf-cell cap per request")
+    ap.add_argument("--slots", type=int, default=32, help="serve: cases in flight at most")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)
@@ -591,7 +669,8 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
-    out = (run_batch if args.workload == "batch96" else run_ours)(args, rank, world, local_rank)
+    runner = {"batch96": run_batch, "serve": run_serve}.get(args.workload, run_ours)
+    out = runner(args, rank, world, local_rank)
     if rank == 0:
         if args.cpu_steps > 0:
             s, cells, sample = cpu_sample(args.workload, args.cpu_steps)

@@ -149,6 +149,12 @@ nb_status nb_step_many(nb_case* c, double dt, int nsteps, nb_step_report* rep);
  * counterpart: the reference steps one NSSolver at a time. */
 nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, int nsteps,
                         nb_step_report* reports);
+/* Split form of nb_step for continuous batching: nb_step_async launches the
+ * case's step graph on its stream and returns; nb_step_wait waits for it and
+ * fills `rep` (may be NULL). Steps of different cases launched this way run
+ * concurrently. One step in flight per case; not available while profiling. */
+nb_status nb_step_async(nb_case* c, double dt);
+nb_status nb_step_wait(nb_case* c, nb_step_report* rep);
 /* Device bytes held by the case (admission control uses this). */
 uint64_t nb_case_device_bytes(const nb_case* c);
 /* Leaf cells of the case (Mcell-steps/s numerator). */

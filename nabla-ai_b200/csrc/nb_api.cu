@@ -76,6 +76,8 @@ struct nb_case {
   AmrFlowView AF{};
   long long* d_sync[3] = {nullptr, nullptr, nullptr};
   int nsync[3] = {0, 0, 0};
+  // a step launched and not yet waited for (nb_step_async / nb_step_wait)
+  bool pending = false, pend_cfl = false, pend_direct = false;
 
   void* alloc(size_t n) {
     void* q = nullptr;
@@ -435,7 +437,8 @@ void finish_step(nb_case& c, nb_step_report* rep);
 
 // One step. Without profiling the step runs as one CUDA graph (built on first
 // use per state parity and dt mode): one launch and one small read-back per step.
-void do_step(nb_case& c, double dt, nb_step_report* rep) {
+// launch_step issues it on the case stream; complete_step waits and finishes.
+void launch_step(nb_case& c, double dt) {
   const bool cfl_dt = dt <= 0.0;
   if (!cfl_dt) {
     c.h_dt[0] = dt;
@@ -467,12 +470,24 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
     NB_CUDA(cudaGraphLaunch(gs.exec, c.stream));
   }
   NB_CUDA(cudaMemcpyAsync(c.h_blk, c.d_blk, sizeof(StepBlock), cudaMemcpyDeviceToHost, c.stream));
+  c.pending = true;
+  c.pend_cfl = cfl_dt;
+  c.pend_direct = direct;
+}
+
+void complete_step(nb_case& c, nb_step_report* rep) {
   NB_CUDA(cudaStreamSynchronize(c.stream));
-  if (!direct) {
-    const GraphSlot& gs = c.graphs[c.cur][cfl_dt ? 1 : 0];
+  c.pending = false;
+  if (!c.pend_direct) {
+    const GraphSlot& gs = c.graphs[c.cur][c.pend_cfl ? 1 : 0];
     c.ctx->launches += gs.fixed_kernels + (c.h_blk->execs - c.last_execs) * gs.body_kernels;
   }
   finish_step(c, rep);
+}
+
+void do_step(nb_case& c, double dt, nb_step_report* rep) {
+  launch_step(c, dt);
+  complete_step(c, rep);
 }
 
 // Host side of a finished step once c.h_blk holds its results: clock, state
@@ -800,6 +815,7 @@ nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, in
   if (!ctx || !cases || n <= 0 || nsteps < 0) return NB_ERR_BAD_ARG;
   for (int q = 0; q < n; ++q) {
     if (!cases[q] || cases[q]->ctx != ctx) return fail(ctx, NB_ERR_BAD_ARG, "batch cases must belong to the context");
+    if (cases[q]->pending) return fail(ctx, NB_ERR_BAD_ARG, "a batch case has a step in flight");
     for (int r = 0; r < q; ++r)
       if (cases[r] == cases[q]) return fail(ctx, NB_ERR_BAD_ARG, "a case appears twice in the batch");
   }
@@ -950,10 +966,36 @@ nb_status nb_case_compute_dt(nb_case* c, double* dt) {
 
 nb_status nb_step(nb_case* c, double dt, nb_step_report* rep) {
   if (!c) return NB_ERR_BAD_ARG;
+  if (c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "a step of this case is in flight (nb_step_wait)");
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
     nb_step_report r{};
     do_step(*c, dt, &r);
+    if (rep) *rep = r;
+    if (std::isnan(r.momentum_residual) || std::isnan(r.continuity_residual))
+      return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");
+    return NB_OK;
+  });
+}
+
+nb_status nb_step_async(nb_case* c, double dt) {
+  if (!c) return NB_ERR_BAD_ARG;
+  if (c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "a step of this case is already in flight");
+  if (!c->ctx->prof.family.empty()) return fail(c->ctx, NB_ERR_UNSUPPORTED, "asynchronous steps need profiling off");
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    launch_step(*c, dt);
+    return NB_OK;
+  });
+}
+
+nb_status nb_step_wait(nb_case* c, nb_step_report* rep) {
+  if (!c) return NB_ERR_BAD_ARG;
+  if (!c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "no step of this case is in flight");
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    nb_step_report r{};
+    complete_step(*c, &r);
     if (rep) *rep = r;
     if (std::isnan(r.momentum_residual) || std::isnan(r.continuity_residual))
       return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");

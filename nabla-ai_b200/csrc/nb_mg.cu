@@ -1190,7 +1190,9 @@ bool MgSolver::build_dense_coarse() {
   if (D.v.amr) return false;
   const HostLevel& h = D.h;
   const int n = h.nx * h.ny * h.nz;
-  if (n > 1024 || h.solid.size() != static_cast<size_t>(n)) return false;
+  // Gauss-Jordan costs ~2 n^3 on the host; larger coarsest levels here are
+  // the cubic 8^3 ones, on which the CG path converges in a few iterations.
+  if (n > 256 || h.solid.size() != static_cast<size_t>(n)) return false;
   std::vector<int> pos(n, -1), fidx;
   for (int m = 0; m < n; ++m)
     if (!h.solid[m]) {

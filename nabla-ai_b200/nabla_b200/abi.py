@@ -142,6 +142,8 @@ PROTOTYPES = [
     ("nb_step", C.c_int, [VP, C.c_double, C.POINTER(StepReport)]),
     ("nb_step_many", C.c_int, [VP, C.c_double, C.c_int, C.POINTER(StepReport)]),
     ("nb_batch_step", C.c_int, [VP, C.POINTER(VP), C.c_int, C.c_double, C.c_int, C.POINTER(StepReport)]),
+    ("nb_step_async", C.c_int, [VP, C.c_double]),
+    ("nb_step_wait", C.c_int, [VP, C.POINTER(StepReport)]),
     ("nb_case_device_bytes", C.c_uint64, [VP]),
     ("nb_case_cell_count", C.c_uint64, [VP]),
     ("nb_case_stream", VP, [VP]),

@@ -194,3 +194,15 @@ def batch_step(cases, dt: float = 0.0, nsteps: int = 1):
     reps = (abi.StepReport * len(cases))()
     ctx.check(ctx.lib.nb_batch_step(ctx.h, hs, len(cases), dt, nsteps, reps), "nb_batch_step")
     return list(reps)
+
+
+def step_async(case, dt: float = 0.0):
+    """Launches one step of `case` (NSSolver or amr.AmrCase) without waiting."""
+    case.ctx.check(case.ctx.lib.nb_step_async(case.h, dt), "nb_step_async")
+
+
+def step_wait(case) -> abi.StepReport:
+    """Waits for the step launched by step_async and returns its report."""
+    rep = abi.StepReport()
+    case.ctx.check(case.ctx.lib.nb_step_wait(case.h, C.byref(rep)), "nb_step_wait")
+    return rep
