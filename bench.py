@@ -40,6 +40,10 @@ sys.path.insert(0, os.path.join(REPO, "nabla-ai_b200"))
 
 METRIC = "Mcell-steps/s (mixed vs FP64 plain, div<1e-8) on 1 B200; p50/p99 solve latency"
 UNIT = "Mcell-steps/s"
+# DRAM bytes (read + write) per launch of a kernel family, averaged over the
+# same launches the roofline averages, from one ncu capture of this workload
+# (profiles/channel3_launches_and_captures.md: 40 consecutive k_smooth launches).
+NCU_TRAFFIC = {("channel3", "smooth"): 1.295e6}
 FAMILIES = ["rhs_rk", "smooth", "resid_restrict", "coarse_cg", "pcg_matvec", "pcg_update",
             "pcg_center", "pcg_mean", "pcg_dots", "pcg_dir", "div", "correct", "diag", "sync"]
 
@@ -305,7 +309,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 5),
                      "bytes_per_launch": nb.value / max(nl.value, 1), "launches": int(nl.value),
-                     "avg_launch_us": round(ms.value * 1e3 / max(nl.value, 1), 3), "traffic": None},
+                     "avg_launch_us": round(ms.value * 1e3 / max(nl.value, 1), 3),
+                     "traffic": NCU_TRAFFIC.get((args.workload, top))},
         "kernel_shares": {k: round(v["ms"] / total, 4) for k, v in sorted(shares.items(),
                                                                          key=lambda kv: -kv[1]["ms"])},
         "divergence_max": max(r.divergence_max for r in reps),
