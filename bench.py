@@ -477,6 +477,51 @@ def run_batch(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+# pressure-solve precision stress: single projections on 3-level octrees
+# ---------------------------------------------------------------------------
+def run_poisson(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from nabla_b200 import abi, amr, solver, workloads
+    torch.cuda.set_device(local_rank)
+    ctx = solver.Context(local_rank)
+    sizes = []
+    for base in args.poisson_bases:
+        geom, leaves = workloads.tgv_octree(base)
+        mesh = amr.AmrMesh(geom, leaves, ctx=ctx)
+        b = np.random.default_rng(base).standard_normal(mesh.ncell)
+        hx, hy, hz = mesh.cell_size()
+        vol = hx * hy * hz
+        b -= np.sum(vol * b) / vol.sum()  # zero volume-weighted mean
+        out = {"effective": base * 4, "leaf_cells": mesh.ncell}
+        sol = {}
+        for name, prec in (("fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+            mesh.solve(b, 1e-12, 400, precision=prec)  # hierarchy set-up and warm-up
+            t0 = time.perf_counter()
+            x, rep = mesh.solve(b, 1e-12, 400, precision=prec)
+            wall = time.perf_counter() - t0
+            sol[name] = x
+            out[name] = {"iterations": rep.iterations, "residual": rep.residual, "converged": rep.converged,
+                         "wall_s": round(wall, 4), "mcells_per_s": round(mesh.ncell / wall / 1e6, 3)}
+        d = sol["mixed"] - sol["fp64"]
+        scale = np.abs(sol["fp64"]).max()
+        r = mesh.apply_a(sol["mixed"]) - b
+        out["mixed_vs_fp64"] = {"max_pressure_rel_err": float(np.abs(d).max() / scale),
+                                "rms_pressure_rel_err": float(np.sqrt(np.mean(d * d)) / scale),
+                                "divergence_rel_residual": float(np.sqrt(np.sum(vol * r * r) / np.sum(vol * b * b)))}
+        sizes.append(out)
+        mesh.close()
+    return {"metric": "pressure-solve precision stress (3-level octrees, rhs N(0,1), tol 1e-12)",
+            "unit": "iterations / s", "n_gpus": world, "data": "synthetic (seeded N(0,1) right-hand sides)",
+            "config": {"workload": "3-level octrees of the periodic TGV box refined where the brick-mean vorticity "
+                                   "is in its top fifth; FP32 V-cycle inside FP64 flexible PCG (mixed) vs FP64 "
+                                   "MG-PCG; wall time of nb_amr_poisson_solve incl. the host copies of b and x; "
+                                   "the FP64 GPU solution is the reference of the mixed errors"},
+            "sizes": sizes, "gpu_launches": int(ctx.launches)}
+
+
+# ---------------------------------------------------------------------------
 # serving: open-loop Poisson arrivals through the continuous-batching loop
 # ---------------------------------------------------------------------------
 def serve_requests(args, seed):
@@ -646,7 +691,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96", "serve"])
+    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96", "serve", "poisson3"])
+    ap.add_argument("--poisson-bases", type=int, nargs="+", default=[32, 64, 128],
+                    help="poisson3: base grids (effective = 4x)")
     ap.add_argument("--batch", type=int, default=96, help="cases of the batch96 workload")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serve: arrival window")
@@ -674,10 +721,10 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
-    runner = {"batch96": run_batch, "serve": run_serve}.get(args.workload, run_ours)
+    runner = {"batch96": run_batch, "serve": run_serve, "poisson3": run_poisson}.get(args.workload, run_ours)
     out = runner(args, rank, world, local_rank)
     if rank == 0:
-        if args.cpu_steps > 0:
+        if args.cpu_steps > 0 and args.workload != "poisson3":
             s, cells, sample = cpu_sample(args.workload, args.cpu_steps)
             out["cpu_baseline"] = {"value": round(cells / s / 1e6, 5), "unit": UNIT, "cores": 1,
                                    "kind": "reference",

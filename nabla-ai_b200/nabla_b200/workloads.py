@@ -212,6 +212,33 @@ def tgv_box_case(seed: int) -> TgvBoxWorkload:
     return TgvBoxWorkload(geom, leaves, solid, cfg, base, int(leaves[:, 0].max()) + 1, n_boxes)
 
 
+def tgv_octree(base: int, levels: int = 3):
+    """3-level octree of the periodic Taylor-Green box [0, 2 pi]^3 on a base^3
+    grid (effective (base * 2^(levels-1))^3), refined at brick granularity
+    where the brick-mean TGV vorticity is in its top fifth (the pressure-solve stress
+    meshes). Returns (geom, leaves)."""
+    L = 2.0 * np.pi
+    h0 = L / base
+    nb0 = (base // 8,) * 3
+    geom = amr.make_geom(nb0, (h0, h0, h0), levels - 1, cases.periodic_faces())
+    leaves = amr.base_leaves(nb0)
+    c = np.arange(8) + 0.5
+    for lev in range(levels - 1):
+        at = np.nonzero(leaves[:, 0] == lev)[0]
+        h = h0 / (1 << lev)
+        b = leaves[at, 1:4].astype(np.float64)
+        X = (b[:, 0:1, None, None] * 8 + c[None, :, None, None]) * h
+        Y = (b[:, 1:2, None, None] * 8 + c[None, None, :, None]) * h
+        Z = (b[:, 2:3, None, None] * 8 + c[None, None, None, :]) * h
+        # brick mean of |omega| (the brick maxima of this symmetric field tie)
+        w = _tgv_vorticity(X, Y, Z).reshape(len(at), -1).mean(axis=1)
+        thr = np.percentile(w, 80.0)
+        flags = np.zeros(len(leaves), dtype=np.uint8)
+        flags[at[w > thr]] = 1
+        leaves = amr.refine(geom, leaves, flags)
+    return geom, leaves
+
+
 def obstacle_channel(seed: int = 0, lmax: int = 2, n_boxes: int = 6, precision_note: str = "") -> AmrWorkload:
     rng = np.random.default_rng(seed)
     h0 = 1.0 / 16.0
