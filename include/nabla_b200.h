@@ -104,6 +104,8 @@ typedef struct nb_case nb_case;
 /* Binds CUDA device `device`. Fails with NB_ERR_CUDA when no sm_100 device is
  * present: there is no CPU fallback. */
 nb_status nb_ctx_create(int device, nb_ctx** out);
+/* Releases the caller's handle. Cases and meshes hold the context too, so they
+ * may be destroyed after it, in any order: it is freed with the last of them. */
 void nb_ctx_destroy(nb_ctx* ctx);
 const char* nb_last_error(const nb_ctx* ctx);
 const char* nb_status_string(nb_status s);

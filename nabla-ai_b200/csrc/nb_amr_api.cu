@@ -116,14 +116,17 @@ nb_status nb_amr_mesh_create(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* l
     return NB_OK;
   });
   if (s != NB_OK) return s;
+  ctx_retain(ctx);
   *out = m.release();
   return NB_OK;
 }
 
 void nb_amr_mesh_destroy(nb_amr_mesh* m) {
   if (!m) return;
-  cudaSetDevice(m->ctx->device);
+  nb_ctx* ctx = m->ctx;
+  cudaSetDevice(ctx->device);
   delete m;
+  ctx_release(ctx);
 }
 
 int64_t nb_amr_mesh_leaf_count(const nb_amr_mesh* m) {

@@ -640,6 +640,19 @@ FlowView cell_view(const MgSolver& mg) {
 
 }  // namespace
 
+void nb::ctx_release(nb_ctx* ctx) {
+  if (ctx->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->batch_cache) destroy_batch(kv.second);
+  ctx->batch_cache.clear();
+  ctx->mg_cache.clear();
+  if (ctx->stage_a) cudaFree(ctx->stage_a);
+  if (ctx->stage_b) cudaFree(ctx->stage_b);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
 extern "C" {
 
 const char* nb_status_string(nb_status s) {
@@ -685,16 +698,7 @@ nb_status nb_ctx_create(int device, nb_ctx** out) {
 }
 
 void nb_ctx_destroy(nb_ctx* ctx) {
-  if (!ctx) return;
-  cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (auto& kv : ctx->batch_cache) destroy_batch(kv.second);
-  ctx->batch_cache.clear();
-  ctx->mg_cache.clear();
-  if (ctx->stage_a) cudaFree(ctx->stage_a);
-  if (ctx->stage_b) cudaFree(ctx->stage_b);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  if (ctx) ctx_release(ctx);
 }
 
 const char* nb_last_error(const nb_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
@@ -796,6 +800,7 @@ nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_co
     return NB_OK;
   });
   if (s != NB_OK) return s;
+  ctx_retain(ctx);
   *out = c.release();
   return NB_OK;
 }
@@ -805,7 +810,9 @@ void nb_case_destroy(nb_case* c) {
   cudaSetDevice(c->ctx->device);
   if (c->ctx->stream) cudaStreamSynchronize(c->ctx->stream);
   drop_batches_with(c->ctx, c);
+  nb_ctx* ctx = c->ctx;
   delete c;
+  ctx_release(ctx);
 }
 
 // Steps every case of `cases` nsteps times; each step of all of them is one
@@ -1206,6 +1213,7 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     return NB_OK;
   });
   if (s != NB_OK) return s;
+  ctx_retain(ctx);
   *out = c.release();
   return NB_OK;
 }

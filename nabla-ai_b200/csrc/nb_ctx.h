@@ -1,5 +1,6 @@
 // nb_ctx.h — the context object behind the C ABI and its error plumbing.
 #pragma once
+#include <atomic>
 #include <map>
 #include <memory>
 #include <string>
@@ -21,6 +22,10 @@ struct BatchGraph {
 
 struct nb_ctx {
   int device = 0;
+  // the caller's handle plus one per live case and mesh: nb_ctx_destroy drops
+  // the first, and the context is freed when the last of its objects goes, in
+  // whatever order the caller (or a garbage collector) destroys them
+  std::atomic<int> refs{1};
   std::string err;
   uint64_t launches = 0;
   nb::Profiler prof;
@@ -53,6 +58,10 @@ nb_status guarded(nb_ctx* ctx, Fn&& fn) {
     return fail(ctx, NB_ERR_BAD_ARG, e.what());
   }
 }
+
+inline void ctx_retain(nb_ctx* ctx) { ctx->refs.fetch_add(1, std::memory_order_relaxed); }
+// Frees the context when this was its last reference.
+void ctx_release(nb_ctx* ctx);
 
 // Grows the context's two staging buffers to at least `elems` doubles each.
 void ensure_staging(nb_ctx* ctx, size_t elems);

@@ -77,3 +77,18 @@ def test_batch_fixed_dt_and_bad_arguments(ctx):
     assert all(r.dt == pytest.approx(0.05) for r in reps)
     with pytest.raises(solver.NablaError):
         solver.batch_step([a[0], a[0]], 0.0, 1)
+
+
+def test_context_destroyed_before_its_cases():
+    """Cases and meshes hold their context: destroying the context handle first
+    (as a garbage collector may at interpreter exit) leaves them usable to
+    destroy, and the batch graphs that name them are released with them."""
+    own = solver.Context(0)
+    a, b = _channel(own, seed=0), _channel(own, seed=1)
+    solver.batch_step([a, b], nsteps=1)
+    mesh = a._mesh_keepalive
+    own.close()
+    a.close()
+    mesh.close()
+    b.close()
+    b._mesh_keepalive.close()
