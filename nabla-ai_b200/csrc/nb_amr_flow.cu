@@ -335,71 +335,98 @@ __global__ void __launch_bounds__(RHS_NT) k_amr_rhs_rk(AmrFlowView F, int stage,
   const double* in[3] = {u, v, w};
   const double* in0[3] = {u0, v0, w0};
   double* out[3] = {uo, vo, wo};
+  // Same-level leaves of the 27 brick positions around (and at) the brick,
+  // -1 where the position is outside the mesh or covered at another level.
+  __shared__ int nb27[27];
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
     const int lev = L.blevel[brick];
     const int o[3] = {L.bcoord[3 * brick] * BR, L.bcoord[3 * brick + 1] * BR, L.bcoord[3 * brick + 2] * BR};
+    const int N[3] = {L.lcells[lev][0], L.lcells[lev][1], L.lcells[lev][2]};
+    if (threadIdx.x < 27) {
+      const int q = threadIdx.x;
+      nb27[q] = lut_at(L, lev, L.bcoord[3 * brick] + q % 3 - 1, L.bcoord[3 * brick + 1] + (q / 3) % 3 - 1,
+                       L.bcoord[3 * brick + 2] + q / 9 - 1);
+    }
+    __syncthreads();
     for (int p = threadIdx.x; p < TN; p += blockDim.x) {
       const int ti = p % TW - 3, tj = (p / TW) % TW - 3, tk = p / (TW * TW) - 3;
       const int far = (ti < -1 || ti > 9) + (tj < -1 || tj > 9) + (tk < -1 || tk > 9);
       if (far > 1) continue;  // never read by a stencil
       const bool inner = ti >= 0 && ti < 8 && tj >= 0 && tj < 8 && tk >= 0 && tk < 8;
+      const int g[3] = {o[0] + ti, o[1] + tj, o[2] + tk};
+      // A halo point strictly inside the domain whose leaf is at this level is
+      // that leaf's stored cell slot: the ghost walker applies no domain rule
+      // there and its face lookup returns the slot (the minus-side slab is
+      // read only across a periodic low boundary, excluded per component).
+      int r = -1;
+      if (!inner && g[0] >= 0 && g[1] >= 0 && g[2] >= 0 && g[0] < N[0] && g[1] < N[1] && g[2] < N[2])
+        r = nb27[(ti < 0 ? 0 : (ti < 8 ? 1 : 2)) + 3 * (tj < 0 ? 0 : (tj < 8 ? 1 : 2)) +
+                 9 * (tk < 0 ? 0 : (tk < 8 ? 1 : 2))];
+      const long long slot = ((tk & 7) << 6) | ((tj & 7) << 3) | (ti & 7);
       for (int a = 0; a < 3; ++a) {
         double val;
-        if (inner) val = in[a][brick * static_cast<long long>(BR3) + ((tk << 6) | (tj << 3) | ti)];
-        else val = amr_acc(F, a, in[a], lev, o[0] + ti, o[1] + tj, o[2] + tk);
+        if (inner) val = in[a][brick * static_cast<long long>(BR3) + slot];
+        else if (r >= 0 && (g[a] >= 1 || !F.per[a])) val = in[a][r * static_cast<long long>(BR3) + slot];
+        else val = amr_acc(F, a, in[a], lev, g[0], g[1], g[2]);
         tile[a][p] = static_cast<T>(val);
       }
     }
     __syncthreads();
-    const T dx = T(F.h[lev][0]), dy = T(F.h[lev][1]), dz = T(F.h[lev][2]);
+    const T hx = T(F.h[lev][0]), hy = T(F.h[lev][1]), hz = T(F.h[lev][2]);
     const T nu = T(F.nu);
-    const TileRef<T> TU{tile[0]}, TV{tile[1]}, TWW{tile[2]};
-    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
-      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+    // Face jobs: the 3 x 512 low faces, then 3 x 64 high slab faces (a brick
+    // with a slab owns its high faces at a coarser neighbour or the domain
+    // boundary). One RHS call site for every component and position.
+    for (int job = threadIdx.x; job < 3 * BR3 + 3 * 64; job += blockDim.x) {
+      const bool high = job >= 3 * BR3;
+      const int a = high ? (job - 3 * BR3) >> 6 : job >> 9;
+      int loc[3];
+      if (high) {
+        const int m = (job - 3 * BR3) & 63;
+        loc[a] = 7;
+        loc[a == 0 ? 1 : 0] = m & 7;
+        loc[a == 2 ? 1 : 2] = m >> 3;
+      } else {
+        loc[0] = job & 7;
+        loc[1] = (job >> 3) & 7;
+        loc[2] = (job >> 6) & 7;
+      }
+      const int l = (loc[2] << 6) | (loc[1] << 3) | loc[0];
+      const int sid = F.slab_id[3 * brick + a];
+      const int rel_hi = F.rel_hi[3 * brick + a];
+      // low face (derived when the -a side is finer: synced afterwards);
+      // high slab face: RHS at a coarser neighbour, R = 0 at the domain boundary
+      if (high ? (sid < 0 || rel_hi == R_FINER) : (loc[a] == 0 && F.rel_lo[3 * brick + a] == R_FINER)) continue;
       const int p[3] = {o[0] + loc[0], o[1] + loc[1], o[2] + loc[2]};
       const long long c = brick * static_cast<long long>(BR3) + l;
-      const bool sc = L.type[c] == CELL_SOLID;
-      for (int a = 0; a < 3; ++a) {
-        const int stride = a == 0 ? 1 : (a == 1 ? 8 : 64);
-        const T bf = T(F.bf[a]);
-        // low face (derived when the -a side is finer: synced afterwards)
-        if (!(loc[a] == 0 && F.rel_lo[3 * brick + a] == R_FINER)) {
-          double r = 0.0;
-          if (p[a] != 0 && !sc) {
-            bool sn;
-            if (loc[a] > 0) {
-              sn = L.type[c - stride] == CELL_SOLID;
-            } else {
-              int q[3] = {p[0], p[1], p[2]};
-              q[a] -= 1;
-              sn = solid_at(F, lev, q);
-            }
-            if (!sn)
-              r = static_cast<double>(a == 0   ? rhs_u<T>(TU, TV, TWW, loc[0], loc[1], loc[2], F.weno, dx, dy, dz, nu, bf)
-                                      : a == 1 ? rhs_v<T>(TU, TV, TWW, loc[0], loc[1], loc[2], F.weno, dx, dy, dz, nu, bf)
-                                               : rhs_w<T>(TU, TV, TWW, loc[0], loc[1], loc[2], F.weno, dx, dy, dz, nu, bf));
-          }
-          out[a][c] = comb(in0[a][c], in[a][c], r);
+      const long long dst = high ? F.nb + sid * 64LL + slab_local(a, loc[0], loc[1], loc[2]) : c;
+      bool live = L.type[c] != CELL_SOLID;
+      if (high) {
+        live = live && rel_hi == R_COARSER;
+        if (live) {
+          int q[3] = {p[0], p[1], p[2]};
+          q[a] += 1;
+          live = !solid_at(F, lev, q);
         }
-        // high slab face: owned at a coarser neighbour (RHS) or the domain boundary (R = 0)
-        const int sid = F.slab_id[3 * brick + a];
-        if (loc[a] == 7 && sid >= 0 && F.rel_hi[3 * brick + a] != R_FINER) {
-          const long long s = F.nb + sid * 64LL + slab_local(a, loc[0], loc[1], loc[2]);
-          double r = 0.0;
-          if (F.rel_hi[3 * brick + a] == R_COARSER && !sc) {
+      } else {
+        live = live && p[a] != 0;
+        if (live) {
+          if (loc[a] > 0) {
+            live = L.type[c - (a == 0 ? 1 : (a == 1 ? 8 : 64))] != CELL_SOLID;
+          } else {
             int q[3] = {p[0], p[1], p[2]};
-            q[a] += 1;
-            if (!solid_at(F, lev, q)) {
-              int e[3] = {loc[0], loc[1], loc[2]};
-              e[a] = 8;
-              r = static_cast<double>(a == 0   ? rhs_u<T>(TU, TV, TWW, e[0], e[1], e[2], F.weno, dx, dy, dz, nu, bf)
-                                      : a == 1 ? rhs_v<T>(TU, TV, TWW, e[0], e[1], e[2], F.weno, dx, dy, dz, nu, bf)
-                                               : rhs_w<T>(TU, TV, TWW, e[0], e[1], e[2], F.weno, dx, dy, dz, nu, bf));
-            }
+            q[a] -= 1;
+            live = !solid_at(F, lev, q);
           }
-          out[a][s] = comb(in0[a][s], in[a][s], r);
         }
       }
+      double r = 0.0;
+      if (live) {
+        const int e = tix(loc[0] + (high && a == 0), loc[1] + (high && a == 1), loc[2] + (high && a == 2));
+        r = static_cast<double>(
+            rhs_face<T, TW, TW * TW>(tile[0], tile[1], tile[2], a, e, F.weno, hx, hy, hz, nu, T(F.bf[a])));
+      }
+      out[a][dst] = comb(in0[a][dst], in[a][dst], r);
     }
     __syncthreads();
   }

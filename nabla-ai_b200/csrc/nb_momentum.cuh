@@ -27,10 +27,49 @@ __device__ __forceinline__ T weno5_t(T v0, T v1, T v2, T v3, T v4) {
   return (a0 * p0 + a1 * p1 + a2 * p2) / s;
 }
 
+// Upwind-biased face value: the stencil is mirrored for a negative advecting
+// velocity. The five inputs are selected first so that one WENO evaluation is
+// emitted per call site (same value as evaluating the chosen branch).
 template <typename T>
 __device__ __forceinline__ T recon_t(int weno, T adv, T qm2, T qm1, T q0, T qp1, T qp2, T qp3) {
   if (!weno) return T(0.5) * (q0 + qp1);
-  return (adv >= T(0)) ? weno5_t<T>(qm2, qm1, q0, qp1, qp2) : weno5_t<T>(qp3, qp2, qp1, q0, qm1);
+  const bool up = adv >= T(0);
+  return weno5_t<T>(up ? qm2 : qp3, up ? qm1 : qp2, up ? q0 : qp1, up ? qp1 : q0, up ? qp2 : qm1);
+}
+
+// Momentum RHS of component a at the a-face (i,j,k) of a staged tile, for any
+// a: the normal direction convects component a with its own face average, each
+// transverse direction d with the average of component d's two faces on
+// either side of the a-face (ns_solver.cpp:322-472 written once for all three
+// components). Component tiles t0, t1, t2 are indexed base + n*stride, with
+// strides 1, SY, SZ along x, y, z; the flux and Laplacian terms are summed in
+// x, y, z order as in rhs_u/v/w.
+template <typename T, int SY, int SZ>
+__device__ __forceinline__ T rhs_face(const T* t0, const T* t1, const T* t2, int a, int c, int weno, T hx, T hy,
+                                      T hz, T nu, T bf) {
+  const T half = T(0.5);
+  const T* A = a == 0 ? t0 : (a == 1 ? t1 : t2);
+  const int sa = a == 0 ? 1 : (a == 1 ? SY : SZ);
+  T dF[3], lap[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int sd = d == 0 ? 1 : (d == 1 ? SY : SZ);
+    const T hd = d == 0 ? hx : (d == 1 ? hy : hz);
+    T advB, advT;
+    if (d == a) {
+      advB = half * (A[c - sa] + A[c]);
+      advT = half * (A[c] + A[c + sa]);
+    } else {
+      const T* D = d == 0 ? t0 : (d == 1 ? t1 : t2);
+      advT = half * (D[c - sa + sd] + D[c + sd]);
+      advB = half * (D[c - sa] + D[c]);
+    }
+    const T qB = recon_t<T>(weno, advB, A[c - 3 * sd], A[c - 2 * sd], A[c - sd], A[c], A[c + sd], A[c + 2 * sd]);
+    const T qT = recon_t<T>(weno, advT, A[c - 2 * sd], A[c - sd], A[c], A[c + sd], A[c + 2 * sd], A[c + 3 * sd]);
+    dF[d] = (advT * qT - advB * qB) / hd;
+    lap[d] = (A[c + sd] - T(2) * A[c] + A[c - sd]) / (hd * hd);
+  }
+  return -(dF[0] + dF[1] + dF[2]) + nu * ((lap[0] + lap[1]) + lap[2]) + bf;
 }
 
 // u-momentum at the x-face (i,j,k) (ns_solver.cpp:322-374).
