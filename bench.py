@@ -362,11 +362,15 @@ def stream_of(ctx, run):
 # ---------------------------------------------------------------------------
 # batched workload: 96 independent octree TGV boxes stepped together
 # ---------------------------------------------------------------------------
-def make_batch(ctx, prec, n):
-    from nabla_b200 import amr, workloads
+def batch_specs(n):
+    from nabla_b200 import workloads
+    return [workloads.tgv_box_case(seed) for seed in range(n)]
+
+
+def make_batch(ctx, prec, specs):
+    from nabla_b200 import amr
     runs = []
-    for seed in range(n):
-        w = workloads.tgv_box_case(seed)
+    for w in specs:
         mesh = amr.AmrMesh(w.geom, w.leaves, solid=w.solid, ctx=ctx)
         case = amr.AmrCase(mesh, w.config, precision=prec)
         case.set_state(*w.initial_state(case))
@@ -375,24 +379,29 @@ def make_batch(ctx, prec, n):
     return runs
 
 
-def run_batch(args, rank, world, local_rank):
-    import ctypes as C
+def close_batch(batch):
+    for c in batch:
+        mesh = c._mesh_keepalive
+        c.close()
+        mesh.close()
 
+
+def tune_for(ctx, prec, spec, steps=2):
+    """Autotunes the context on one case built from `spec` (cache per GPU)."""
+    from nabla_b200 import solver
+    (case,) = make_batch(ctx, prec, [spec])
+    t0 = time.perf_counter()
+    rep = solver.autotune(case, steps=steps)
+    rep["tune_s"] = round(time.perf_counter() - t0, 1)
+    close_batch([case])
+    return rep
+
+
+def time_batch(ctx, batch, args, stream, flush, world, device):
+    """Warm-up steps, then args.steps timed batch steps (L2 flushed before each)."""
     import torch
 
-    from nabla_b200 import abi, solver
-
-    device = f"cuda:{local_rank}"
-    torch.cuda.set_device(local_rank)
-    ctx = solver.Context(local_rank)
-    precision = args.precision or "mixed"
-    prec = abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64
-    t0 = time.perf_counter()
-    batch = make_batch(ctx, prec, args.batch)
-    setup_s = time.perf_counter() - t0
-    cells = sum(c.cell_count for c in batch)
-    stream = torch.cuda.ExternalStream(ctx.lib.nb_ctx_stream(ctx.h))
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    from nabla_b200 import solver
     t0 = time.perf_counter()
     solver.batch_step(batch, 0.0, max(1, args.warmup))
     warm_s = time.perf_counter() - t0
@@ -402,18 +411,44 @@ def run_batch(args, rank, world, local_rank):
     launches0 = ctx.launches
     elapsed = 0.0
     reps = None
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        reps = solver.batch_step(batch, 0.0, 1)
+        e1.record(stream)
+        e1.synchronize()
+        elapsed += e0.elapsed_time(e1)
+    return dict(elapsed_max=max_over_ranks(elapsed, world, device), launches=ctx.launches - launches0,
+                reps=reps, warm_s=warm_s)
+
+
+def run_batch(args, rank, world, local_rank):
+    import torch
+
+    from nabla_b200 import abi, solver
+
+    device = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    ctx = solver.Context(local_rank)
+    precision = args.precision or "mixed"
+    prec = abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64
+    other = abi.PRECISION_FP64 if prec == abi.PRECISION_MIXED else abi.PRECISION_MIXED
+    specs = batch_specs(args.batch)
+    largest = max(specs, key=lambda w: len(w.leaves))
+    tuning = {}
+    if not args.no_autotune:
+        tuning[precision] = tune_for(ctx, prec, largest)
+    t0 = time.perf_counter()
+    batch = make_batch(ctx, prec, specs)
+    setup_s = time.perf_counter() - t0
+    cells = sum(c.cell_count for c in batch)
+    stream = torch.cuda.ExternalStream(ctx.lib.nb_ctx_stream(ctx.h))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     with ClockSampler(local_rank) as clk:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            reps = solver.batch_step(batch, 0.0, 1)
-            e1.record(stream)
-            e1.synchronize()
-            elapsed += e0.elapsed_time(e1)
-    launches = ctx.launches - launches0
-    elapsed_max = max_over_ranks(elapsed, world, device)
+        main = time_batch(ctx, batch, args, stream, flush, world, device)
+    elapsed_max, launches, reps = main["elapsed_max"], main["launches"], main["reps"]
     value = world * cells * args.steps / (elapsed_max * 1e-3) / 1e6
     # end to end: every case's state from pinned host memory, one batch step, back to host
     pinned = [[torch.from_numpy(a.copy()).pin_memory().numpy() for a in c.get_state()] for c in batch]
@@ -433,17 +468,28 @@ def run_batch(args, rank, world, local_rank):
         e2e_ms += e0.elapsed_time(e1)
     e2e_value = world * cells * n_e2e / (max_over_ranks(e2e_ms, world, device) * 1e-3) / 1e6
     nbytes = sum(a.nbytes for st in pinned for a in st)
+    del pinned
     # kernel shares and roofline: direct-launch profiled steps of the largest case
     big = max(batch, key=lambda c: c.cell_count)
-
-    class _Big:
-        h = big.h
-
-        @staticmethod
-        def step():
-            return big.step(0.0)
-
-    shares = {fam: dict(zip(("ms", "launches", "bytes"), profile_step(ctx, _Big, fam))) for fam in FAMILIES}
+    shares = {fam: dict(zip(("ms", "launches", "bytes"), profile_step(ctx, big, fam))) for fam in FAMILIES}
+    big = None
+    div_max = max(r.divergence_max for r in reps)
+    converged = all(bool(r.converged) for r in reps)
+    close_batch(batch)
+    batch = None
+    # the other form on the same cases (same seeds), tuned for its precision
+    other_name = "fp64" if other == abi.PRECISION_FP64 else "mixed"
+    forms = {precision: round(value, 4)}
+    if not args.single_form:
+        if not args.no_autotune:
+            tuning[other_name] = tune_for(ctx, other, largest)
+        batch2 = make_batch(ctx, other, specs)
+        sec = time_batch(ctx, batch2, args, stream, flush, world, device)
+        forms[other_name] = round(world * cells * args.steps / (sec["elapsed_max"] * 1e-3) / 1e6, 4)
+        div_max = max(div_max, max(r.divergence_max for r in sec["reps"]))
+        converged = converged and all(bool(r.converged) for r in sec["reps"])
+        close_batch(batch2)
+        forms["mixed_over_fp64"] = round(forms["mixed"] / forms["fp64"], 3)
     total = sum(v["ms"] for v in shares.values()) or 1.0
     top = max(shares, key=lambda k: shares[k]["ms"])
     ms, nl, nb = shares[top]["ms"], shares[top]["launches"], shares[top]["bytes"]
@@ -461,7 +507,9 @@ def run_batch(args, rank, world, local_rank):
                    "cases": args.batch, "cells": cells, "precision": precision,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed between timed steps (256 MiB write)",
-                   "setup_s": round(setup_s, 1), "first_steps_s": round(warm_s, 1)},
+                   "setup_s": round(setup_s, 1), "first_steps_s": round(main["warm_s"], 1),
+                   "autotune": tuning or "off"},
+        "forms": forms,
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(nbytes),
                 "d2h_bytes_per_step": int(nbytes)},
         "gpu_launches": int(launches),
@@ -470,8 +518,8 @@ def run_batch(args, rank, world, local_rank):
                      "case": "largest case of the batch, direct-launch profiled step",
                      "bytes_per_launch": nb / max(nl, 1), "launches": int(nl), "traffic": None},
         "kernel_shares": {k: round(v["ms"] / total, 4) for k, v in sorted(shares.items(), key=lambda kv: -kv[1]["ms"])},
-        "divergence_max": max(r.divergence_max for r in reps),
-        "converged": all(bool(r.converged) for r in reps),
+        "divergence_max": div_max,
+        "converged": converged,
         "clocks": clk.summary(),
     }
 
@@ -695,6 +743,8 @@ def main():
     ap.add_argument("--poisson-bases", type=int, nargs="+", default=[32, 64, 128],
                     help="poisson3: base grids (effective = 4x)")
     ap.add_argument("--batch", type=int, default=96, help="cases of the batch96 workload")
+    ap.add_argument("--no-autotune", action="store_true", help="batch96: default tuning instead of the autotuner")
+    ap.add_argument("--single-form", action="store_true", help="batch96: time the primary precision only")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serve: arrival window")
     ap.add_argument("--min-steps", type=int, default=10)

@@ -174,6 +174,50 @@ void* nb_case_stream(const nb_case* c);
 nb_status nb_ctx_profile(nb_ctx* ctx, const char* family);
 nb_status nb_ctx_profile_read(nb_ctx* ctx, double* total_ms, uint64_t* launches, double* bytes);
 
+/* ---- launch tuning and the autotuner ---------------------------------------
+ * No counterpart in the reference. A context's tuning applies to the cases,
+ * meshes and Poisson hierarchies created after it is set; objects keep the
+ * tuning they were created with. Bricks are fixed at 8^3 cells, one thread
+ * per cell in the multigrid kernels. */
+typedef struct nb_tuning {
+  int32_t mg_ctas_per_sm;    /* multigrid brick kernels: grid <= this x SMs (1..4) */
+  int32_t rhs_ctas_per_sm;   /* momentum kernel: grid <= this x SMs (1..4) */
+  int32_t halo_mode;         /* multigrid halo staging: 0 per-brick neighbour maps
+                                (one round of independent loads), 1 per-cell walk */
+  int32_t sweeps;            /* smoothing sweeps before and after each coarse
+                                correction (1..3), mixed form; FP64 keeps 2 */
+  int32_t coarse_direct_max; /* below multi-level meshes, solve coarsest levels of
+                                up to this many cells exactly (0..512; 0 = CG) */
+  int32_t pdl;               /* 1: multigrid chains use programmatic dependent launch */
+} nb_tuning;
+
+typedef struct nb_tune_report {
+  nb_tuning best;
+  double best_ms;            /* per step, fastest candidate */
+  double default_ms;         /* per step, nb_tuning_default */
+  int32_t candidates;        /* candidates timed (0 when taken from the cache) */
+  int32_t rejected;          /* candidates whose steps did not converge */
+  int32_t from_cache;
+  char key[128];             /* cache key: GPU, SM count, mesh kind, precision, size class */
+} nb_tune_report;
+
+void nb_tuning_default(nb_tuning* t);
+nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t);
+nb_status nb_ctx_get_tuning(const nb_ctx* ctx, nb_tuning* t);
+/* Picks the tuning for cases like `sample` and sets it on the context:
+ * coordinate descent over the fields of nb_tuning from the default, each
+ * candidate timed over `steps` fixed-dt steps (CUDA events, after one warm-up
+ * step) on a scratch copy of `sample` (same mesh or grid, configuration,
+ * precision and current state); a candidate is kept only if it is at least 2%
+ * faster and its steps converge with divergence <= 1e-8. With `cache_path`
+ * (a text file, one line per key) a cached entry for the key is used without
+ * timing, and a new result is written back. `sample` is not modified. */
+nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache_path, nb_tune_report* rep);
+/* Cache file access (host only): 1 if `key` was found, 0 if not; negative on
+ * an unreadable or malformed file. */
+int nb_tune_cache_lookup(const char* cache_path, const char* key, nb_tuning* t, double* ms);
+nb_status nb_tune_cache_store(const char* cache_path, const char* key, const nb_tuning* t, double ms);
+
 /* ---- pressure Poisson: the PoissonSolver seam ---------------------------- */
 /* Replaces MgPoisson::solve (core/src/flow/multigrid.cpp:206-355) behind
  * PoissonSolver::solve(const UniformGrid&, const std::vector<double>& b,

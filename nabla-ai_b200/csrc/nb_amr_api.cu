@@ -54,7 +54,8 @@ std::vector<AmrLeaf> to_leaves(const int32_t* leaves, int64_t n) {
 
 MgSolver& mesh_solver(nb_amr_mesh* m, int precision) {
   auto& s = m->mg[precision == NB_PRECISION_MIXED ? 1 : 0];
-  if (!s) s = std::make_unique<MgSolver>(m->lvl, precision, LaunchCounter{&m->ctx->launches, &m->ctx->prof});
+  if (!s)
+    s = std::make_unique<MgSolver>(m->lvl, precision, LaunchCounter{&m->ctx->launches, &m->ctx->prof}, &m->ctx->tune);
   return *s;
 }
 

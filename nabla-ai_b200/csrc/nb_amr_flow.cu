@@ -636,8 +636,8 @@ void amr_flow_setup() {
 
 void launch_amr_rhs_rk(cudaStream_t s, const AmrFlowView& F, int stage, const double* dtp, const double* u,
                        const double* v, const double* w, const double* u0, const double* v0,
-                       const double* w0, double* uo, double* vo, double* wo, int mixed) {
-  const int grid = std::min(F.L.nbrick, 148 * 2);
+                       const double* w0, double* uo, double* vo, double* wo, int mixed, int grid_cap) {
+  const int grid = std::min(F.L.nbrick, std::max(grid_cap, 1));
   if (mixed)
     k_amr_rhs_rk<float><<<grid, RHS_NT, 3 * TN * sizeof(float), s>>>(F, stage, dtp, u, v, w, u0, v0, w0, uo, vo,
                                                                      wo);

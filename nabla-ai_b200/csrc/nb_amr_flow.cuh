@@ -32,7 +32,7 @@ struct AmrStepScalars {
 void amr_flow_setup();
 void launch_amr_rhs_rk(cudaStream_t s, const AmrFlowView& F, int stage, const double* dtp, const double* u,
                        const double* v, const double* w, const double* u0, const double* v0,
-                       const double* w0, double* uo, double* vo, double* wo, int mixed);
+                       const double* w0, double* uo, double* vo, double* wo, int mixed, int grid_cap);
 void launch_amr_sync(cudaStream_t s, const long long* list, int n, double* f);
 void launch_amr_div(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v, const double* w,
                     double* b);

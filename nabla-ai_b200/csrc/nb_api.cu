@@ -67,6 +67,7 @@ struct nb_case {
   uint64_t bytes = 0;
   bool has_solid = false;
   uint64_t nfluid = 0;
+  int rhs_grid = 296;  // CTAs of the momentum kernel (tuning)
   int step = 0;
   double t = 0.0, dt_last = 0.0;
   // ---- octree-AMR cases (the mesh outlives the case) ----
@@ -386,7 +387,7 @@ void issue_step_amr(nb_case& c, int cur, bool cfl_dt, bool direct) {
     double** out = (stage == 2) ? A : B;
     flow_launch(c, "rhs_rk", ncell_of(c) * 73, [&] {
       launch_amr_rhs_rk(c.stream, c.AF, stage, &blk->dt, in[0], in[1], in[2], c.uvw0[0], c.uvw0[1], c.uvw0[2],
-                        out[0], out[1], out[2], mixed);
+                        out[0], out[1], out[2], mixed, c.rhs_grid);
     });
     amr_sync(c, out);
     project_amr(c, out, stage - 1, direct);
@@ -422,7 +423,7 @@ void issue_step(nb_case& c, int cur, bool cfl_dt, bool direct) {
     double** out = (stage == 2) ? A : B;
     flow_launch(c, "rhs_rk", ncell_of(c) * 73, [&] {
       launch_rhs_rk(c.stream, c.F, stage, &blk->dt, in[0], in[1], in[2], c.uvw0[0], c.uvw0[1], c.uvw0[2],
-                    out[0], out[1], out[2], mixed);
+                    out[0], out[1], out[2], mixed, c.rhs_grid);
     });
     project(c, out, stage - 1, direct);
   }
@@ -625,7 +626,7 @@ MgSolver& ctx_solver(nb_ctx* ctx, const nb_grid_desc& g, int precision) {
   const auto key = std::make_pair(grid_signature(g), precision);
   auto it = ctx->mg_cache.find(key);
   if (it == ctx->mg_cache.end()) {
-    auto s = std::make_unique<MgSolver>(g, precision, LaunchCounter{&ctx->launches, &ctx->prof});
+    auto s = std::make_unique<MgSolver>(g, precision, LaunchCounter{&ctx->launches, &ctx->prof}, &ctx->tune);
     it = ctx->mg_cache.emplace(key, std::move(s)).first;
   }
   return *it->second;
@@ -651,6 +652,44 @@ void nb::ctx_release(nb_ctx* ctx) {
   if (ctx->stage_b) cudaFree(ctx->stage_b);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+
+void nb::case_kind(const nb_case* c, int* amr, int* precision, int* levels) {
+  *amr = c->amr ? 1 : 0;
+  *precision = c->precision;
+  *levels = c->amr ? c->mesh->lvl.tree.nlev : 1;
+}
+
+nb_status nb::clone_case(nb_case* src, nb_case** out) {
+  nb_ctx* ctx = src->ctx;
+  nb_case* c = nullptr;
+  nb_status st = src->amr ? nb_amr_case_create(ctx, src->mesh, &src->cfg, src->precision, &c)
+                          : nb_case_create(ctx, &src->grid, &src->cfg, src->precision, &c);
+  if (st != NB_OK) return st;
+  // the current state, through the public accessors (host round trip)
+  std::vector<double> f[4];
+  if (src->amr) {
+    int64_t sz[4];
+    st = nb_amr_case_sizes(src, sz);
+    for (int q = 0; q < 4 && st == NB_OK; ++q) f[q].resize(static_cast<size_t>(sz[q]));
+    if (st == NB_OK) st = nb_amr_case_get_state(src, f[0].data(), f[1].data(), f[2].data(), f[3].data());
+    if (st == NB_OK) st = nb_amr_case_set_state(c, f[0].data(), f[1].data(), f[2].data(), f[3].data());
+  } else {
+    const size_t nx = src->grid.nx, ny = src->grid.ny, nz = src->grid.nz;
+    f[0].resize((nx + 1) * ny * nz);
+    f[1].resize(nx * (ny + 1) * nz);
+    f[2].resize(nx * ny * (nz + 1));
+    f[3].resize(nx * ny * nz);
+    st = nb_case_get_state(src, f[0].data(), f[1].data(), f[2].data(), f[3].data());
+    if (st == NB_OK)
+      st = nb_case_set_state(c, f[0].data(), f[1].data(), f[2].data(), f[3].data(), src->step, src->t, src->dt_last);
+  }
+  if (st != NB_OK) {
+    nb_case_destroy(c);
+    return st;
+  }
+  *out = c;
+  return NB_OK;
 }
 
 extern "C" {
@@ -683,7 +722,9 @@ nb_status nb_ctx_create(int device, nb_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return NB_ERR_CUDA;
   auto* ctx = new nb_ctx();
   ctx->device = device;
+  nb_tuning_default(&ctx->tune);
   const nb_status s = guarded(ctx, [&] {
+    NB_CUDA(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device));
     NB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     flow_kernel_setup();
     amr_flow_setup();
@@ -740,7 +781,8 @@ nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_co
     c->nu = cfg->velocity_scale * cfg->ref_length / cfg->reynolds;  // ns_solver.cpp:54
     for (uint8_t v : c->solid)
       if (v) { c->has_solid = true; break; }
-    c->mg = std::make_unique<MgSolver>(c->grid, precision, LaunchCounter{&ctx->launches, &ctx->prof});
+    c->mg = std::make_unique<MgSolver>(c->grid, precision, LaunchCounter{&ctx->launches, &ctx->prof}, &ctx->tune);
+    c->rhs_grid = std::min(std::max(ctx->tune.rhs_ctas_per_sm, 1), 4) * ctx->nsm;
     c->nfluid = c->mg->host0().nfluid;
     FlowView& F = c->F;
     F.L = c->mg->view0();
@@ -1114,7 +1156,8 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
         break;
       }
     c->nfluid = lv.nfluid;
-    c->mg = std::make_unique<MgSolver>(lv, precision, LaunchCounter{&ctx->launches, &ctx->prof});
+    c->mg = std::make_unique<MgSolver>(lv, precision, LaunchCounter{&ctx->launches, &ctx->prof}, &ctx->tune);
+    c->rhs_grid = std::min(std::max(ctx->tune.rhs_ctas_per_sm, 1), 4) * ctx->nsm;
     build_face_maps(t, c->fm);
     AmrFlowView& F = c->AF;
     auto up = [&](const void* src, size_t bytes) {

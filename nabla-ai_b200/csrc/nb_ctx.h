@@ -30,6 +30,8 @@ struct nb_ctx {
   uint64_t launches = 0;
   nb::Profiler prof;
   cudaStream_t stream = nullptr;
+  int nsm = 148;     // SMs of the device
+  nb_tuning tune{};  // applies to objects created after it is set
   // batch graphs keyed by (case, state parity) pairs
   std::map<std::vector<uintptr_t>, nb::BatchGraph> batch_cache;
   // MgPoisson-style cache for the host-array Poisson seam (multigrid.cpp:211-220)
@@ -62,6 +64,12 @@ nb_status guarded(nb_ctx* ctx, Fn&& fn) {
 inline void ctx_retain(nb_ctx* ctx) { ctx->refs.fetch_add(1, std::memory_order_relaxed); }
 // Frees the context when this was its last reference.
 void ctx_release(nb_ctx* ctx);
+
+// A scratch case with `sample`'s mesh or grid, configuration, precision and
+// current state, built with the context's current tuning (autotuner).
+nb_status clone_case(nb_case* sample, nb_case** out);
+// Kind of a case for the tuning cache key.
+void case_kind(const nb_case* c, int* amr, int* precision, int* levels);
 
 // Grows the context's two staging buffers to at least `elems` doubles each.
 void ensure_staging(nb_ctx* ctx, size_t elems);

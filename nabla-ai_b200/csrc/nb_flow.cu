@@ -15,6 +15,7 @@
 #include <cmath>
 
 #include "nb_flow.cuh"
+#include "nb_momentum.cuh"
 #include "nb_reduce.cuh"
 
 namespace nb {
@@ -188,33 +189,6 @@ __device__ double acc_w(const FlowView& F, const double* __restrict__ w, int i, 
   return term;
 }
 
-// Jiang-Shu WENO-5 at the right face of the middle cell (ns_solver.cpp:15-31).
-template <typename T>
-__device__ __forceinline__ T weno5(T v0, T v1, T v2, T v3, T v4) {
-  const T eps = T(1e-12);
-  const T c1312 = T(13.0 / 12.0), q = T(0.25);
-  const T b0 = c1312 * (v0 - T(2) * v1 + v2) * (v0 - T(2) * v1 + v2) +
-               q * (v0 - T(4) * v1 + T(3) * v2) * (v0 - T(4) * v1 + T(3) * v2);
-  const T b1 = c1312 * (v1 - T(2) * v2 + v3) * (v1 - T(2) * v2 + v3) + q * (v1 - v3) * (v1 - v3);
-  const T b2 = c1312 * (v2 - T(2) * v3 + v4) * (v2 - T(2) * v3 + v4) +
-               q * (T(3) * v2 - T(4) * v3 + v4) * (T(3) * v2 - T(4) * v3 + v4);
-  const T a0 = T(0.1) / ((eps + b0) * (eps + b0));
-  const T a1 = T(0.6) / ((eps + b1) * (eps + b1));
-  const T a2 = T(0.3) / ((eps + b2) * (eps + b2));
-  const T s = a0 + a1 + a2;
-  const T p0 = (T(2) * v0 - T(7) * v1 + T(11) * v2) / T(6.0);
-  const T p1 = (-v1 + T(5) * v2 + T(2) * v3) / T(6.0);
-  const T p2 = (T(2) * v2 + T(5) * v3 - v4) / T(6.0);
-  return (a0 * p0 + a1 * p1 + a2 * p2) / s;
-}
-
-// reconstruct (ns_solver.cpp:35-42): q[-2..3] around the face between 0 and +1.
-template <typename T>
-__device__ __forceinline__ T recon(int weno, T adv, T qm2, T qm1, T q0, T qp1, T qp2, T qp3) {
-  if (!weno) return T(0.5) * (q0 + qp1);
-  return (adv >= T(0)) ? weno5<T>(qm2, qm1, q0, qp1, qp2) : weno5<T>(qp3, qp2, qp1, q0, qm1);
-}
-
 __device__ __forceinline__ int tix(int a, int b, int c) { return ((c + 3) * TW + (b + 3)) * TW + (a + 3); }
 
 // ---------------------------------------------------------------------------
@@ -241,11 +215,8 @@ __global__ void __launch_bounds__(RHS_NT) k_rhs_rk(FlowView F, int stage, const 
   const LevelView& L = F.L;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const int twoD = L.twoD;
-  const T idx_ = T(1.0 / L.dxyz[0]);
-  (void)idx_;
   const T dx = T(L.dxyz[0]), dy = T(L.dxyz[1]), dz = T(L.dxyz[2]);
   const T nu = T(F.nu);
-  const T h = T(0.5);
   const double c1 = 1.0 / 3.0, c2 = 2.0 / 3.0;
   const double dt = *dtp;
   auto comb = [&](double a0, double a, double r) -> double {
@@ -266,133 +237,29 @@ __global__ void __launch_bounds__(RHS_NT) k_rhs_rk(FlowView F, int stage, const 
       tw[p] = static_cast<T>(acc_w(F, w, gi, gj, gk));
     }
     __syncthreads();
-#define TU(a, b, c) tu[tix((a), (b), (c))]
-#define TV(a, b, c) tv[tix((a), (b), (c))]
-#define TWW(a, b, c) tw[tix((a), (b), (c))]
-    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
-      const int i = l & 7, j = (l >> 3) & 7, k = l >> 6;
-      const int gi = ox + i, gj = oy + j, gk = oz + k;
-      if (gi >= nx || gj >= ny || gk >= nz) continue;  // void cell
+    // Face jobs: component a's low face of every cell (one RHS call site).
+    for (int job = threadIdx.x; job < 3 * BR3; job += blockDim.x) {
+      const int a = job >> 9, l = job & (BR3 - 1);
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      const int g[3] = {ox + loc[0], oy + loc[1], oz + loc[2]};
+      if (g[0] >= nx || g[1] >= ny || g[2] >= nz) continue;  // void cell
       const int c = brick * BR3 + l;
-      const bool sc = L.type[c] == CELL_SOLID;
-      // ---- u-momentum at x-face gi (ns_solver.cpp:322-374) ----
-      {
-        double ru = 0.0;
-        if (gi >= 1 && !sc && !is_solid_g(L, gi - 1, gj, gk)) {
-          const T ucL = h * (TU(i - 1, j, k) + TU(i, j, k));
-          const T ucR = h * (TU(i, j, k) + TU(i + 1, j, k));
-          const T uxL = recon<T>(F.weno, ucL, TU(i - 3, j, k), TU(i - 2, j, k), TU(i - 1, j, k), TU(i, j, k),
-                                 TU(i + 1, j, k), TU(i + 2, j, k));
-          const T uxR = recon<T>(F.weno, ucR, TU(i - 2, j, k), TU(i - 1, j, k), TU(i, j, k), TU(i + 1, j, k),
-                                 TU(i + 2, j, k), TU(i + 3, j, k));
-          const T dFx = (ucR * uxR - ucL * uxL) / dx;
-          const T vT = h * (TV(i - 1, j + 1, k) + TV(i, j + 1, k));
-          const T vB = h * (TV(i - 1, j, k) + TV(i, j, k));
-          const T uyT = recon<T>(F.weno, vT, TU(i, j - 2, k), TU(i, j - 1, k), TU(i, j, k), TU(i, j + 1, k),
-                                 TU(i, j + 2, k), TU(i, j + 3, k));
-          const T uyB = recon<T>(F.weno, vB, TU(i, j - 3, k), TU(i, j - 2, k), TU(i, j - 1, k), TU(i, j, k),
-                                 TU(i, j + 1, k), TU(i, j + 2, k));
-          const T dFy = (vT * uyT - vB * uyB) / dy;
-          T dFz = T(0);
-          if (!twoD) {
-            const T wT = h * (TWW(i - 1, j, k + 1) + TWW(i, j, k + 1));
-            const T wB = h * (TWW(i - 1, j, k) + TWW(i, j, k));
-            const T uzT = recon<T>(F.weno, wT, TU(i, j, k - 2), TU(i, j, k - 1), TU(i, j, k), TU(i, j, k + 1),
-                                   TU(i, j, k + 2), TU(i, j, k + 3));
-            const T uzB = recon<T>(F.weno, wB, TU(i, j, k - 3), TU(i, j, k - 2), TU(i, j, k - 1), TU(i, j, k),
-                                   TU(i, j, k + 1), TU(i, j, k + 2));
-            dFz = (wT * uzT - wB * uzB) / dz;
-          }
-          T lap = (TU(i + 1, j, k) - T(2) * TU(i, j, k) + TU(i - 1, j, k)) / (dx * dx) +
-                  (TU(i, j + 1, k) - T(2) * TU(i, j, k) + TU(i, j - 1, k)) / (dy * dy);
-          if (!twoD) lap += (TU(i, j, k + 1) - T(2) * TU(i, j, k) + TU(i, j, k - 1)) / (dz * dz);
-          ru = static_cast<double>(-(dFx + dFy + dFz) + nu * lap + T(F.bf[0]));
-        }
-        uo[c] = comb(u0[c], u[c], ru);
-        if (gi == nx - 1) {
-          const long long s = uidx(F, nx, gj, gk);
-          uo[s] = comb(u0[s], u[s], 0.0);
-        }
-      }
-      // ---- v-momentum at y-face gj (ns_solver.cpp:376-424) ----
-      {
-        double rv = 0.0;
-        if (gj >= 1 && !sc && !is_solid_g(L, gi, gj - 1, gk)) {
-          const T vcB = h * (TV(i, j - 1, k) + TV(i, j, k));
-          const T vcT = h * (TV(i, j, k) + TV(i, j + 1, k));
-          const T vyB = recon<T>(F.weno, vcB, TV(i, j - 3, k), TV(i, j - 2, k), TV(i, j - 1, k), TV(i, j, k),
-                                 TV(i, j + 1, k), TV(i, j + 2, k));
-          const T vyT = recon<T>(F.weno, vcT, TV(i, j - 2, k), TV(i, j - 1, k), TV(i, j, k), TV(i, j + 1, k),
-                                 TV(i, j + 2, k), TV(i, j + 3, k));
-          const T dFy = (vcT * vyT - vcB * vyB) / dy;
-          const T uR = h * (TU(i + 1, j - 1, k) + TU(i + 1, j, k));
-          const T uL = h * (TU(i, j - 1, k) + TU(i, j, k));
-          const T vxR = recon<T>(F.weno, uR, TV(i - 2, j, k), TV(i - 1, j, k), TV(i, j, k), TV(i + 1, j, k),
-                                 TV(i + 2, j, k), TV(i + 3, j, k));
-          const T vxL = recon<T>(F.weno, uL, TV(i - 3, j, k), TV(i - 2, j, k), TV(i - 1, j, k), TV(i, j, k),
-                                 TV(i + 1, j, k), TV(i + 2, j, k));
-          const T dFx = (uR * vxR - uL * vxL) / dx;
-          T dFz = T(0);
-          if (!twoD) {
-            const T wR = h * (TWW(i, j - 1, k + 1) + TWW(i, j, k + 1));
-            const T wL = h * (TWW(i, j - 1, k) + TWW(i, j, k));
-            const T vzR = recon<T>(F.weno, wR, TV(i, j, k - 2), TV(i, j, k - 1), TV(i, j, k), TV(i, j, k + 1),
-                                   TV(i, j, k + 2), TV(i, j, k + 3));
-            const T vzL = recon<T>(F.weno, wL, TV(i, j, k - 3), TV(i, j, k - 2), TV(i, j, k - 1), TV(i, j, k),
-                                   TV(i, j, k + 1), TV(i, j, k + 2));
-            dFz = (wR * vzR - wL * vzL) / dz;
-          }
-          T lap = (TV(i + 1, j, k) - T(2) * TV(i, j, k) + TV(i - 1, j, k)) / (dx * dx) +
-                  (TV(i, j + 1, k) - T(2) * TV(i, j, k) + TV(i, j - 1, k)) / (dy * dy);
-          if (!twoD) lap += (TV(i, j, k + 1) - T(2) * TV(i, j, k) + TV(i, j, k - 1)) / (dz * dz);
-          rv = static_cast<double>(-(dFx + dFy + dFz) + nu * lap + T(F.bf[1]));
-        }
-        vo[c] = comb(v0[c], v[c], rv);
-        if (gj == ny - 1) {
-          const long long s = vidx(F, gi, ny, gk);
-          vo[s] = comb(v0[s], v[s], 0.0);
-        }
-      }
-      // ---- w-momentum at z-face gk (ns_solver.cpp:426-472), 3-D only ----
-      {
-        double rw = 0.0;
-        if (!twoD && gk >= 1 && !sc && !is_solid_g(L, gi, gj, gk - 1)) {
-          const T wcB = h * (TWW(i, j, k - 1) + TWW(i, j, k));
-          const T wcT = h * (TWW(i, j, k) + TWW(i, j, k + 1));
-          const T wzB = recon<T>(F.weno, wcB, TWW(i, j, k - 3), TWW(i, j, k - 2), TWW(i, j, k - 1),
-                                 TWW(i, j, k), TWW(i, j, k + 1), TWW(i, j, k + 2));
-          const T wzT = recon<T>(F.weno, wcT, TWW(i, j, k - 2), TWW(i, j, k - 1), TWW(i, j, k),
-                                 TWW(i, j, k + 1), TWW(i, j, k + 2), TWW(i, j, k + 3));
-          const T dFz = (wcT * wzT - wcB * wzB) / dz;
-          const T uR = h * (TU(i + 1, j, k - 1) + TU(i + 1, j, k));
-          const T uL = h * (TU(i, j, k - 1) + TU(i, j, k));
-          const T wxR = recon<T>(F.weno, uR, TWW(i - 2, j, k), TWW(i - 1, j, k), TWW(i, j, k),
-                                 TWW(i + 1, j, k), TWW(i + 2, j, k), TWW(i + 3, j, k));
-          const T wxL = recon<T>(F.weno, uL, TWW(i - 3, j, k), TWW(i - 2, j, k), TWW(i - 1, j, k),
-                                 TWW(i, j, k), TWW(i + 1, j, k), TWW(i + 2, j, k));
-          const T dFx = (uR * wxR - uL * wxL) / dx;
-          const T vR = h * (TV(i, j + 1, k - 1) + TV(i, j + 1, k));
-          const T vL = h * (TV(i, j, k - 1) + TV(i, j, k));
-          const T wyR = recon<T>(F.weno, vR, TWW(i, j - 2, k), TWW(i, j - 1, k), TWW(i, j, k),
-                                 TWW(i, j + 1, k), TWW(i, j + 2, k), TWW(i, j + 3, k));
-          const T wyL = recon<T>(F.weno, vL, TWW(i, j - 3, k), TWW(i, j - 2, k), TWW(i, j - 1, k),
-                                 TWW(i, j, k), TWW(i, j + 1, k), TWW(i, j + 2, k));
-          const T dFy = (vR * wyR - vL * wyL) / dy;
-          const T lap = (TWW(i + 1, j, k) - T(2) * TWW(i, j, k) + TWW(i - 1, j, k)) / (dx * dx) +
-                        (TWW(i, j + 1, k) - T(2) * TWW(i, j, k) + TWW(i, j - 1, k)) / (dy * dy) +
-                        (TWW(i, j, k + 1) - T(2) * TWW(i, j, k) + TWW(i, j, k - 1)) / (dz * dz);
-          rw = static_cast<double>(-(dFx + dFy + dFz) + nu * lap + T(F.bf[2]));
-        }
-        wo[c] = comb(w0[c], w[c], rw);
-        if (gk == nz - 1) {
-          const long long s = widx(F, gi, gj, nz);
-          wo[s] = comb(w0[s], w[s], 0.0);
-        }
+      // faces touching a solid, the domain's low boundary faces and (2-D) w get R = 0
+      double r = 0.0;
+      if (g[a] >= 1 && !(a == 2 && twoD) && L.type[c] != CELL_SOLID &&
+          !is_solid_g(L, g[0] - (a == 0), g[1] - (a == 1), g[2] - (a == 2)))
+        r = static_cast<double>(rhs_face<T, TW, TW * TW>(tu, tv, tw, a, tix(loc[0], loc[1], loc[2]), F.weno, dx, dy,
+                                                         dz, nu, T(F.bf[a]), twoD != 0));
+      const double* f = a == 0 ? u : (a == 1 ? v : w);
+      const double* f0 = a == 0 ? u0 : (a == 1 ? v0 : w0);
+      double* o = a == 0 ? uo : (a == 1 ? vo : wo);
+      o[c] = comb(f0[c], f[c], r);
+      // the domain's high boundary face (no RHS)
+      if (g[a] == (a == 0 ? nx : (a == 1 ? ny : nz)) - 1) {
+        const long long s = a == 0 ? uidx(F, nx, g[1], g[2]) : (a == 1 ? vidx(F, g[0], ny, g[2]) : widx(F, g[0], g[1], nz));
+        o[s] = comb(f0[s], f[s], 0.0);
       }
     }
-#undef TU
-#undef TV
-#undef TWW
     __syncthreads();
   }
 }
@@ -665,8 +532,8 @@ void launch_bc(cudaStream_t s, const BcOp* ops, int n, int serial, double* u, do
 
 void launch_rhs_rk(cudaStream_t s, const FlowView& F, int stage, const double* dtp, const double* u,
                    const double* v, const double* w, const double* u0, const double* v0,
-                   const double* w0, double* uo, double* vo, double* wo, int mixed) {
-  const int grid = std::min(F.L.nbrick, 148 * 2);
+                   const double* w0, double* uo, double* vo, double* wo, int mixed, int grid_cap) {
+  const int grid = std::min(F.L.nbrick, std::max(grid_cap, 1));
   if (mixed)
     k_rhs_rk<float><<<grid, RHS_NT, 3 * TN * sizeof(float), s>>>(F, stage, dtp, u, v, w, u0, v0, w0, uo,
                                                                  vo, wo);

@@ -38,7 +38,7 @@ struct StepScalars {  // per-step diagnostics (device), ns_solver.cpp:797-823
 void launch_bc(cudaStream_t s, const BcOp* ops, int n, int serial, double* u, double* v, double* w);
 void launch_rhs_rk(cudaStream_t s, const FlowView& F, int stage, const double* dtp, const double* u,
                    const double* v, const double* w, const double* u0, const double* v0,
-                   const double* w0, double* uo, double* vo, double* wo, int mixed);
+                   const double* w0, double* uo, double* vo, double* wo, int mixed, int grid_cap);
 void launch_div(cudaStream_t s, const FlowView& F, const double* u, const double* v, const double* w,
                 double* b);
 void launch_correct(cudaStream_t s, const FlowView& F, const double* phi, const double* dtp, double* u,

@@ -34,8 +34,6 @@ inline size_t coarse_smem(size_t n) {
   return n * (6 * sizeof(double) + 1) + (n <= static_cast<size_t>(COARSE_PRE_CELLS) ? n * 6 * sizeof(int16_t) : 0);
 }
 
-inline int grid_for(int nbrick) { return nbrick < MAX_GRID ? nbrick : MAX_GRID; }
-
 __device__ __forceinline__ bool stopped(const SolveFlags* f, int maxit) {
   return f != nullptr && (f->stop != 0 || f->iters >= maxit);
 }
@@ -1190,9 +1188,9 @@ bool MgSolver::build_dense_coarse() {
   if (D.v.amr) return false;
   const HostLevel& h = D.h;
   const int n = h.nx * h.ny * h.nz;
-  // Gauss-Jordan costs ~2 n^3 on the host; larger coarsest levels here are
-  // the cubic 8^3 ones, on which the CG path converges in a few iterations.
-  if (n > 256 || h.solid.size() != static_cast<size_t>(n)) return false;
+  // Gauss-Jordan costs ~2 n^3 on the host (the default limit of 256 cells
+  // keeps set-up cheap; larger coarsest levels converge in a few CG iterations).
+  if (n > direct_max_ || h.solid.size() != static_cast<size_t>(n)) return false;
   std::vector<int> pos(n, -1), fidx;
   for (int m = 0; m < n; ++m)
     if (!h.solid[m]) {
@@ -1355,7 +1353,7 @@ void MgSolver::common_alloc() {
     throw ApiError{NB_ERR_UNSUPPORTED, "coarsest multigrid level exceeds 4096 cells"};
   if (lv_.size() > static_cast<size_t>(MAX_LEVELS))
     throw ApiError{NB_ERR_UNSUPPORTED, "multigrid hierarchy deeper than " + std::to_string(MAX_LEVELS) + " levels"};
-  build_halo_maps();
+  if (halo_mode_ == 0) build_halo_maps();
   n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
   double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
   for (double** v : vecs) {
@@ -1384,8 +1382,24 @@ void MgSolver::common_alloc() {
   NB_CUDA(cudaFuncSetAttribute(k_coarse_cg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
 }
 
-MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
+void MgSolver::set_tuning(const nb_tuning* tune) {
+  nb_tuning t;
+  nb_tuning_default(&t);
+  if (tune) t = *tune;
+  int dev = 0, nsm = 148;
+  NB_CUDA(cudaGetDevice(&dev));
+  NB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int per_sm = std::min(std::max(t.mg_ctas_per_sm, 1), 4);
+  grid_cap_ = std::min(per_sm * nsm, MAX_GRID);  // the reduction buffer holds MAX_GRID partials
+  pdl_ = t.pdl != 0;
+  sweeps_ = precision_ == NB_PRECISION_MIXED ? std::min(std::max(t.sweeps, 1), 3) : 2;  // FP64: V(2,2) as the reference
+  halo_mode_ = t.halo_mode == 1 ? 1 : 0;
+  direct_max_ = std::min(std::max(t.coarse_direct_max, 0), 512);
+}
+
+MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc, const nb_tuning* tune)
     : precision_(precision), lc_(lc) {
+  set_tuning(tune);
   std::vector<HostLevel> H = build_hierarchy(g);
   singular_ = true;
   for (int f = 0; f < 6; ++f)
@@ -1404,8 +1418,9 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc)
 // into its parents (cells fluid if any child is); once a single octree level
 // remains the grid is uniform and coarsens as MgPoisson does
 // (core/src/flow/multigrid.cpp:211-266).
-MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc)
+MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc, const nb_tuning* tune)
     : precision_(precision), lc_(lc) {
+  set_tuning(tune);
   const AmrGeom& geo = fine.tree.geom;
   singular_ = true;
   for (int f = 0; f < 6; ++f)
@@ -1477,7 +1492,7 @@ MgSolver::~MgSolver() {
 void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
   const LevelView& L = lv_[0].v;
   NB_LAUNCH(lc_, "apply_a", s, lv_[0].ncell * 17,
-            launch_pdl(k_apply_a, dim3(grid_for(L.nbrick)), dim3(NT), 0, s, L, x, out));
+            launch_pdl(pdl_, k_apply_a, dim3(grid_of(L.nbrick)), dim3(NT), 0, s, L, x, out));
   NB_CUDA(cudaGetLastError());
 }
 
@@ -1490,20 +1505,20 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const LevelView& L = D.v;
   const T* b = static_cast<const T*>(bv);
   const double* bmean = (singular_ && bmean_slot >= 0) ? S_ + bmean_slot : nullptr;
-  const int grid = grid_for(L.nbrick);
+  const int grid = grid_of(L.nbrick);
   const double tsz = sizeof(T);
   const double ncell = D.ncell;
   if (lvl + 1 == static_cast<int>(lv_.size())) {
     const size_t nco = static_cast<size_t>(L.nx) * L.ny * L.nz;
     if (dense_) {
       NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1) + 8.0 * dense_nf_ * dense_nf_,
-                launch_pdl(k_coarse_direct<T>, dim3(1), dim3(NT), 2 * sizeof(double) * dense_nf_, s, L, b, bmean,
+                launch_pdl(pdl_, k_coarse_direct<T>, dim3(1), dim3(NT), 2 * sizeof(double) * dense_nf_, s, L, b, bmean,
                            static_cast<T*>(D.x0), dense_inv_, dense_fmap_, dense_lexpos_, dense_lexcell_,
                            dense_nf_, singular_ ? 1 : 0, flags_, maxit_));
     } else {
       const size_t smem = coarse_smem(nco);
       NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
-                (launch_pdl(k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0),
+                (launch_pdl(pdl_, k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0),
                             singular_ ? 1 : 0, 1e-6, 500, flags_, maxit_)));
     }
     *out_x = D.x0;
@@ -1520,45 +1535,53 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   DevLevel& Cd = lv_[lvl + 1];
   const LevelView& C = Cd.v;
   const double ncoarse = Cd.ncell;
-  // pre-smoothing (2 sweeps), first from x = 0
+  // Ping-pong buffers with their pending means: xa <-> slot 0, xb <-> slot 1.
+  T* buf[2] = {xa, xb};
+  double* mean[2] = {mA, mB};
+  int cur = 0;
+  // pre-smoothing (sweeps_ sweeps; 2 as the reference), the first from x = 0
   NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
-            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean,
-                                             XFetch<T>{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1}, xa,
-                                             rb_, mA, inv_nf, flags_, maxit_)));
-  NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
-                                             xb, rb_, mB, inv_nf, flags_, maxit_)));
+            (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+                        XFetch<T>{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1}, buf[cur], rb_, mean[cur],
+                        inv_nf, flags_, maxit_)));
+  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
+    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
+              (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+                          XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, buf[cur ^ 1], rb_,
+                          mean[cur ^ 1], inv_nf, flags_, maxit_)));
   // residual + restriction
   const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
   double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
   NB_LAUNCH(lc_, "resid_restrict", s, ncell * (2 * tsz + 1) + ncoarse * tsz,
-            (launch_pdl(k_resid_restrict<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean,
-                                                     XFetch<T>{xb, mB, nullptr, nullptr, dummy, 1, 1, 1}, C,
-                                                     Cd.h.fx, Cd.h.fy, Cd.h.fz, static_cast<T*>(Cd.b), rb_,
-                                                     cmean, inv_nfc, flags_, maxit_)));
+            (launch_pdl(pdl_, k_resid_restrict<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+                        XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, C, Cd.h.fx, Cd.h.fy,
+                        Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_)));
   void* ec = nullptr;
   int ec_slot = -1;
   vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec);
   const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
-  // post-smoothing: first sweep folds in the prolongation x += P e
+  // post-smoothing: the first sweep folds in the prolongation x += P e
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
-            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,
-                L, b, bmean,
-                XFetch<T>{xb, mB, static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy, Cd.h.fz, D.d_xfb, D.d_xfo}, xa, rb_,
-                mA, inv_nf, flags_, maxit_)));
-  NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-            (launch_pdl(k_smooth<T>, dim3(grid), dim3(NT), 0, s,L, b, bmean, XFetch<T>{xa, mA, nullptr, nullptr, dummy, 1, 1, 1},
-                                             xb, rb_, mB, inv_nf, flags_, maxit_)));
-  *out_x = xb;
-  *out_mean_slot = sing ? lvl_slot(lvl, 1) : -1;
+            (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+                        XFetch<T>{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
+                                  Cd.h.fz, D.d_xfb, D.d_xfo},
+                        buf[cur ^ 1], rb_, mean[cur ^ 1], inv_nf, flags_, maxit_)));
+  cur ^= 1;
+  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
+    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
+              (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+                          XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, buf[cur ^ 1], rb_,
+                          mean[cur ^ 1], inv_nf, flags_, maxit_)));
+  *out_x = buf[cur];
+  *out_mean_slot = sing ? lvl_slot(lvl, cur) : -1;
 }
 
 // Minv: z = V-cycle(r) (+ Minv's removeMean), then either p = z, rz = r.z
 // (first) or the flexible-beta dots, then p = z + beta p.
 void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   const LevelView& L = lv_[0].v;
-  const int grid = grid_for(L.nbrick);
+  const int grid = grid_of(L.nbrick);
   const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   const bool sing = singular_ && lv_[0].h.nfluid > 0;
   const bool mixed = precision_ == NB_PRECISION_MIXED;
@@ -1566,13 +1589,13 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   const double zsz = mixed ? 4.0 : 8.0;
   for (int k = 0; k < count; ++k) {
     NB_LAUNCH(lc_, "pcg_matvec", s, n * 17,
-              launch_pdl(k_pcg_matvec, dim3(grid), dim3(NT), 0, s, L, p_, Ap_, rb_, S_, flags_, maxit));
+              launch_pdl(pdl_, k_pcg_matvec, dim3(grid), dim3(NT), 0, s, L, p_, Ap_, rb_, S_, flags_, maxit));
     NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0)),
-              (launch_pdl(k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
+              (launch_pdl(pdl_, k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
                                                 sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol)));
     if (sing) {
       NB_LAUNCH(lc_, "pcg_center", s, n * (17 + (mixed ? 4 : 0)),
-                (launch_pdl(k_pcg_center, dim3(grid), dim3(NT), 0, s, L, rnew_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, maxit,
+                (launch_pdl(pdl_, k_pcg_center, dim3(grid), dim3(NT), 0, s, L, rnew_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, maxit,
                                                   tol)));
     }
     void* zx = nullptr;
@@ -1584,22 +1607,22 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
     if (sing) {
       if (mixed)
         NB_LAUNCH(lc_, "pcg_mean", s, n * (zsz + 1),
-                  (launch_pdl(k_fluid_mean_f, dim3(grid), dim3(NT), 0, s,L, static_cast<const float*>(zx), m1, rb_, S_ + S_ZMEAN2,
+                  (launch_pdl(pdl_, k_fluid_mean_f, dim3(grid), dim3(NT), 0, s,L, static_cast<const float*>(zx), m1, rb_, S_ + S_ZMEAN2,
                                                       inv_nf, flags_, maxit)));
       else
         NB_LAUNCH(lc_, "pcg_mean", s, n * (zsz + 1),
-                  (launch_pdl(k_fluid_mean, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, rb_, S_ + S_ZMEAN2,
+                  (launch_pdl(pdl_, k_fluid_mean, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, rb_, S_ + S_ZMEAN2,
                                                     inv_nf, flags_, maxit)));
     }
     if (mixed)
       NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
-                (launch_pdl(k_pcg_dots<float>, dim3(grid), dim3(NT), 0, s,L, static_cast<const float*>(zx), m1, m2, z_, p_, rnew_,
+                (launch_pdl(pdl_, k_pcg_dots<float>, dim3(grid), dim3(NT), 0, s,L, static_cast<const float*>(zx), m1, m2, z_, p_, rnew_,
                                                        r_, 0, rb_, S_, flags_, maxit)));
     else
       NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
-                (launch_pdl(k_pcg_dots<double>, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, m2, z_, p_,
+                (launch_pdl(pdl_, k_pcg_dots<double>, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, m2, z_, p_,
                                                         rnew_, r_, 0, rb_, S_, flags_, maxit)));
-    NB_LAUNCH(lc_, "pcg_dir", s, n * 24, launch_pdl(k_pcg_dir, dim3(grid), dim3(NT), 0, s, L, z_, p_, S_, flags_, maxit));
+    NB_LAUNCH(lc_, "pcg_dir", s, n * 24, launch_pdl(pdl_, k_pcg_dir, dim3(grid), dim3(NT), 0, s, L, z_, p_, S_, flags_, maxit));
     std::swap(r_, rnew_);
   }
   NB_CUDA(cudaGetLastError());
@@ -1662,7 +1685,7 @@ void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int ma
 
 void MgSolver::finish(cudaStream_t s, double* report) {
   const LevelView& L = lv_[0].v;
-  const int grid = grid_for(L.nbrick);
+  const int grid = grid_of(L.nbrick);
   const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   const bool sing = singular_ && lv_[0].h.nfluid > 0;
   // final removeMean(x) + true residual (multigrid.cpp:341-353)
@@ -1698,7 +1721,7 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit) {
   tol_ = tol;
   maxit_ = maxit;
   const LevelView& L = lv_[0].v;
-  const int grid = grid_for(L.nbrick);
+  const int grid = grid_of(L.nbrick);
   const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   const bool sing = singular_ && lv_[0].h.nfluid > 0;
   const bool mixed = precision_ == NB_PRECISION_MIXED;

@@ -39,10 +39,12 @@ struct DevLevel {
 
 class MgSolver {
  public:
-  MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc);
+  // `tune` sets launch shapes, halo staging, mixed-form sweeps, the exact
+  // coarse-solve threshold and PDL (nb_tuning; nullptr = defaults).
+  MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc, const nb_tuning* tune = nullptr);
   // Composite (octree-AMR) operator on the leaves of `fine` (types and codes
   // already built), with the composite-then-uniform MG hierarchy.
-  MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc);
+  MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc, const nb_tuning* tune = nullptr);
   ~MgSolver();
   MgSolver(const MgSolver&) = delete;
   MgSolver& operator=(const MgSolver&) = delete;
@@ -97,6 +99,13 @@ class MgSolver {
   bool build_dense_coarse();
   void common_alloc();
   void* alloc(size_t bytes);
+  void set_tuning(const nb_tuning* tune);
+  int grid_of(int nbrick) const { return nbrick < grid_cap_ ? nbrick : grid_cap_; }
+  int grid_cap_ = 0;   // CTAs of the brick kernels
+  bool pdl_ = true;    // programmatic dependent launch of the chains
+  int sweeps_ = 2;     // smoothing sweeps per side of the coarse correction
+  int halo_mode_ = 0;  // 0 per-brick neighbour maps, 1 per-cell walk
+  int direct_max_ = 256;  // exact coarsest solve up to this many cells
   // Exact coarsest-level solve (composite hierarchies only): the inverse of the
   // fluid block of the coarsest operator (regularised on the constant mode when
   // singular), host-factored once.

@@ -43,16 +43,21 @@ __device__ __forceinline__ T recon_t(int weno, T adv, T qm2, T qm1, T q0, T qp1,
 // either side of the a-face (ns_solver.cpp:322-472 written once for all three
 // components). Component tiles t0, t1, t2 are indexed base + n*stride, with
 // strides 1, SY, SZ along x, y, z; the flux and Laplacian terms are summed in
-// x, y, z order as in rhs_u/v/w.
+// x, y, z order as in rhs_u/v/w. With two_d the z terms are absent (the
+// reference's nz == 1 branches).
 template <typename T, int SY, int SZ>
 __device__ __forceinline__ T rhs_face(const T* t0, const T* t1, const T* t2, int a, int c, int weno, T hx, T hy,
-                                      T hz, T nu, T bf) {
+                                      T hz, T nu, T bf, bool two_d = false) {
   const T half = T(0.5);
   const T* A = a == 0 ? t0 : (a == 1 ? t1 : t2);
   const int sa = a == 0 ? 1 : (a == 1 ? SY : SZ);
   T dF[3], lap[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
+    if (d == 2 && two_d) {
+      dF[d] = lap[d] = T(0);
+      continue;
+    }
     const int sd = d == 0 ? 1 : (d == 1 ? SY : SZ);
     const T hd = d == 0 ? hx : (d == 1 ? hy : hz);
     T advB, advT;

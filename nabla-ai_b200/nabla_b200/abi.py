@@ -123,6 +123,34 @@ def dptr(a: np.ndarray | None):
     return a.ctypes.data_as(DP)
 
 
+class Tuning(C.Structure):
+    """nb_tuning: launch shapes, halo staging, mixed-form sweeps, exact
+    coarse-solve threshold and PDL of the objects a context creates."""
+    _fields_ = [
+        ("mg_ctas_per_sm", C.c_int32),
+        ("rhs_ctas_per_sm", C.c_int32),
+        ("halo_mode", C.c_int32),
+        ("sweeps", C.c_int32),
+        ("coarse_direct_max", C.c_int32),
+        ("pdl", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class TuneReport(C.Structure):
+    _fields_ = [
+        ("best", Tuning),
+        ("best_ms", C.c_double),
+        ("default_ms", C.c_double),
+        ("candidates", C.c_int32),
+        ("rejected", C.c_int32),
+        ("from_cache", C.c_int32),
+        ("key", C.c_char * 128),
+    ]
+
+
 # (name, restype, argtypes) for every symbol declared in include/nabla_b200.h
 PROTOTYPES = [
     ("nb_ctx_create", C.c_int, [C.c_int, C.POINTER(VP)]),
@@ -148,6 +176,12 @@ PROTOTYPES = [
     ("nb_case_cell_count", C.c_uint64, [VP]),
     ("nb_case_stream", VP, [VP]),
     ("nb_ctx_profile", C.c_int, [VP, C.c_char_p]),
+    ("nb_tuning_default", None, [C.POINTER(Tuning)]),
+    ("nb_ctx_set_tuning", C.c_int, [VP, C.POINTER(Tuning)]),
+    ("nb_ctx_get_tuning", C.c_int, [VP, C.POINTER(Tuning)]),
+    ("nb_autotune", C.c_int, [VP, VP, C.c_int, C.c_char_p, C.POINTER(TuneReport)]),
+    ("nb_tune_cache_lookup", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Tuning), DP]),
+    ("nb_tune_cache_store", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Tuning), C.c_double]),
     ("nb_ctx_profile_read", C.c_int, [VP, DP, C.POINTER(C.c_uint64), DP]),
     ("nb_poisson_solve", C.c_int, [VP, C.POINTER(GridDesc), DP, DP, C.c_double, C.c_int, C.c_int,
                                    C.POINTER(PoissonReport)]),

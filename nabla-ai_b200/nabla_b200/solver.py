@@ -16,6 +16,7 @@ Every call runs on the CUDA library; nothing here computes the solution.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -55,6 +56,23 @@ class Context:
     @property
     def launches(self) -> int:
         return self.lib.nb_ctx_launch_count(self.h)
+
+    @property
+    def tuning(self) -> dict:
+        """The nb_tuning applied to cases, meshes and Poisson hierarchies created next."""
+        t = abi.Tuning()
+        self.check(self.lib.nb_ctx_get_tuning(self.h, C.byref(t)), "nb_ctx_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, **fields):
+        """Sets nb_tuning fields (the others keep their current values)."""
+        t = abi.Tuning()
+        self.check(self.lib.nb_ctx_get_tuning(self.h, C.byref(t)), "nb_ctx_get_tuning")
+        for k, v in fields.items():
+            if k not in t.as_dict():
+                raise ValueError(f"unknown tuning field {k!r}")
+            setattr(t, k, int(v))
+        self.check(self.lib.nb_ctx_set_tuning(self.h, C.byref(t)), "nb_ctx_set_tuning")
 
     def close(self):
         if getattr(self, "h", None):
@@ -206,3 +224,34 @@ def step_wait(case) -> abi.StepReport:
     rep = abi.StepReport()
     case.ctx.check(case.ctx.lib.nb_step_wait(case.h, C.byref(rep)), "nb_step_wait")
     return rep
+
+
+def default_tuning() -> dict:
+    t = abi.Tuning()
+    abi.load().nb_tuning_default(C.byref(t))
+    return t.as_dict()
+
+
+def default_tune_cache() -> str:
+    """Per-user tuning cache: $NABLA_B200_TUNE_CACHE, else
+    ~/.cache/nabla_b200/tuning.txt (the directory is created)."""
+    path = os.environ.get("NABLA_B200_TUNE_CACHE")
+    if not path:
+        path = os.path.join(os.path.expanduser("~"), ".cache", "nabla_b200", "tuning.txt")
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    return path
+
+
+def autotune(case, steps: int = 3, cache: str | None = "default") -> dict:
+    """nb_autotune on `case` (NSSolver or amr.AmrCase): picks the fastest
+    converging tuning for cases like it and sets it on the case's context
+    (cases created afterwards use it). cache=None times without a cache;
+    "default" uses default_tune_cache()."""
+    ctx = case.ctx
+    path = default_tune_cache() if cache == "default" else cache
+    rep = abi.TuneReport()
+    ctx.check(ctx.lib.nb_autotune(ctx.h, case.h, steps, path.encode() if path else None, C.byref(rep)),
+              "nb_autotune")
+    return {"best": rep.best.as_dict(), "best_ms": rep.best_ms, "default_ms": rep.default_ms,
+            "candidates": rep.candidates, "rejected": rep.rejected, "from_cache": bool(rep.from_cache),
+            "key": rep.key.decode()}
