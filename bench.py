@@ -362,9 +362,9 @@ def stream_of(ctx, run):
 # ---------------------------------------------------------------------------
 # batched workload: 96 independent octree TGV boxes stepped together
 # ---------------------------------------------------------------------------
-def batch_specs(n):
+def batch_specs(n, seeds=None):
     from nabla_b200 import workloads
-    return [workloads.tgv_box_case(seed) for seed in range(n)]
+    return [workloads.tgv_box_case(seed) for seed in (seeds if seeds else range(n))]
 
 
 def make_batch(ctx, prec, specs):
@@ -435,10 +435,13 @@ def run_batch(args, rank, world, local_rank):
     precision = args.precision or "mixed"
     prec = abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64
     other = abi.PRECISION_FP64 if prec == abi.PRECISION_MIXED else abi.PRECISION_MIXED
-    specs = batch_specs(args.batch)
+    specs = batch_specs(args.batch, args.batch_seeds)
     largest = max(specs, key=lambda w: len(w.leaves))
     tuning = {}
-    if not args.no_autotune:
+    if args.tuning:
+        ctx.set_tuning(**args.tuning)
+        tuning["fixed"] = ctx.tuning
+    elif not args.no_autotune:
         tuning[precision] = tune_for(ctx, prec, largest)
     t0 = time.perf_counter()
     batch = make_batch(ctx, prec, specs)
@@ -481,7 +484,7 @@ def run_batch(args, rank, world, local_rank):
     other_name = "fp64" if other == abi.PRECISION_FP64 else "mixed"
     forms = {precision: round(value, 4)}
     if not args.single_form:
-        if not args.no_autotune:
+        if not args.no_autotune and not args.tuning:
             tuning[other_name] = tune_for(ctx, other, largest)
         batch2 = make_batch(ctx, other, specs)
         sec = time_batch(ctx, batch2, args, stream, flush, world, device)
@@ -501,10 +504,11 @@ def run_batch(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == abi.PRECISION_FP64 else "f32+f64",
         "data": "synthetic (96 seeded Taylor-Green boxes with seeded obstacles)",
-        "config": {"workload": f"batched: {args.batch} independent octree TGV boxes, base grids in {{16..64}}^3, "
+        "config": {"workload": f"batched: {len(specs)} independent octree TGV boxes, base grids in {{16..64}}^3, "
                                "1-3 levels, 0-6 boxes each, nu=1/1600, WENO-5, CFL 0.4, MG-PCG to 1e-10; "
                                "each step of all cases is one CUDA graph launch",
-                   "cases": args.batch, "cells": cells, "precision": precision,
+                   "cases": len(specs), "seeds": args.batch_seeds or f"0..{args.batch - 1}",
+                   "cells": cells, "precision": precision,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed between timed steps (256 MiB write)",
                    "setup_s": round(setup_s, 1), "first_steps_s": round(main["warm_s"], 1),
@@ -520,6 +524,7 @@ def run_batch(args, rank, world, local_rank):
         "kernel_shares": {k: round(v["ms"] / total, 4) for k, v in sorted(shares.items(), key=lambda kv: -kv[1]["ms"])},
         "divergence_max": div_max,
         "converged": converged,
+        "poisson_iters_mean": round(sum(r.poisson_iters for r in reps) / len(reps), 2),
         "clocks": clk.summary(),
     }
 
@@ -744,7 +749,11 @@ def main():
                     help="poisson3: base grids (effective = 4x)")
     ap.add_argument("--batch", type=int, default=96, help="cases of the batch96 workload")
     ap.add_argument("--no-autotune", action="store_true", help="batch96: default tuning instead of the autotuner")
+    ap.add_argument("--batch-seeds", type=int, nargs="+", default=None,
+                    help="batch96: build the batch from these case seeds instead of 0..batch-1")
     ap.add_argument("--single-form", action="store_true", help="batch96: time the primary precision only")
+    ap.add_argument("--tuning", type=lambda t: {k: int(v) for k, v in (kv.split("=") for kv in t.split(","))},
+                    default=None, help="batch96: fixed nb_tuning fields, e.g. threads_per_brick=128,mg_ctas_per_sm=9")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serve: arrival window")
     ap.add_argument("--min-steps", type=int, default=10)

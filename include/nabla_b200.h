@@ -177,10 +177,9 @@ nb_status nb_ctx_profile_read(nb_ctx* ctx, double* total_ms, uint64_t* launches,
 /* ---- launch tuning and the autotuner ---------------------------------------
  * No counterpart in the reference. A context's tuning applies to the cases,
  * meshes and Poisson hierarchies created after it is set; objects keep the
- * tuning they were created with. Bricks are fixed at 8^3 cells, one thread
- * per cell in the multigrid kernels. */
+ * tuning they were created with. Bricks are fixed at 8^3 cells. */
 typedef struct nb_tuning {
-  int32_t mg_ctas_per_sm;    /* multigrid brick kernels: grid <= this x SMs (1..4) */
+  int32_t mg_ctas_per_sm;    /* multigrid brick kernels: grid <= this x SMs (1..16) */
   int32_t rhs_ctas_per_sm;   /* momentum kernel: grid <= this x SMs (1..4) */
   int32_t halo_mode;         /* multigrid halo staging: 0 per-brick neighbour maps
                                 (one round of independent loads), 1 per-cell walk */
@@ -189,6 +188,9 @@ typedef struct nb_tuning {
   int32_t coarse_direct_max; /* below multi-level meshes, solve coarsest levels of
                                 up to this many cells exactly (0..512; 0 = CG) */
   int32_t pdl;               /* 1: multigrid chains use programmatic dependent launch */
+  int32_t threads_per_brick; /* CTA size of the smoother, residual-restriction and
+                                matvec kernels: 512, 256 or 128 (1, 2 or 4 cells
+                                per thread; smaller CTAs keep more bricks in flight) */
 } nb_tuning;
 
 typedef struct nb_tune_report {

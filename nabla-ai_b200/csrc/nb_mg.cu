@@ -24,7 +24,7 @@ namespace nb {
 namespace {
 
 constexpr int NT = 512;          // threads per CTA = cells per brick
-constexpr int MAX_GRID = 148 * 4;  // grid-stride CTA cap (4 CTAs of 512 per SM)
+constexpr int MAX_GRID = 148 * 16;  // grid-stride CTA cap (16 CTAs of 128 per SM)
 constexpr double kOmega = 0.8;   // multigrid.cpp:38
 constexpr int COARSE_MAX_CELLS = 4096;
 constexpr int COARSE_PRE_CELLS = 2048;  // coarsest levels up to this size keep a resolved stencil
@@ -176,40 +176,55 @@ __device__ __forceinline__ void fill_halo_amr(const LevelView& L, int brick, T* 
   }
 }
 
-// One-round staging (levels with per-brick maps, 512 threads): thread t loads
-// its own cell; threads 0..383 each load one face-halo cell from the
-// neighbour brick (6 faces x 64). All loads are independent.
-template <typename T, class F>
+// One-round staging (levels with per-brick maps): a CTA of NTH threads loads
+// the brick's 512 cells (512/NTH per thread) and the 384 face-halo cells from
+// the six neighbour bricks (6 faces x 64). Every load is issued before the
+// first store to shared memory, so all of them are in flight together.
+template <typename T, int NTH, class F>
 __device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T* tile, const F& fx) {
+  constexpr int CPT = BR3 / NTH;
+  constexpr int HPT = (384 + NTH - 1) / NTH;
   const int t = threadIdx.x;
   const bool pro = fx.prolongs();
   const int pb = pro ? L.par[brick] : 0, po = pro ? L.poct[brick] : -1;
-  const T own = fx.at(brick * BR3 + t, pb, po, L.amr);
-  T halo = T(0);
-  int hpos = -1;
-  if (t < 384) {
-    const int f = t >> 6, m = t & 63, u = m & 7, w = m >> 3, a = f >> 1, s = f & 1;
-    const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
-    int tc[3], lc[3];
-    tc[a] = s ? 8 : -1;
-    lc[a] = s ? 0 : 7;
-    tc[t1] = lc[t1] = u;
-    tc[t2] = lc[t2] = w;
-    hpos = tpos(tc[0], tc[1], tc[2]);
-    const int nb = L.nbr6[brick * 6 + f];
-    if (nb >= 0) {
-      const int npb = pro ? L.npar6[brick * 6 + f] : 0, npo = pro ? L.npoct6[brick * 6 + f] : -1;
-      halo = fx.at(nb * BR3 + ((lc[2] << 6) | (lc[1] << 3) | lc[0]), npb, npo, L.amr);
+  T own[CPT];
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) own[q] = fx.at(brick * BR3 + t + q * NTH, pb, po, L.amr);
+  T halo[HPT];
+  int hpos[HPT];
+#pragma unroll
+  for (int q = 0; q < HPT; ++q) {
+    const int h = t + q * NTH;
+    halo[q] = T(0);
+    hpos[q] = -1;
+    if (h < 384) {
+      const int f = h >> 6, m = h & 63, u = m & 7, w = m >> 3, a = f >> 1, s = f & 1;
+      const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
+      int tc[3], lc[3];
+      tc[a] = s ? 8 : -1;
+      lc[a] = s ? 0 : 7;
+      tc[t1] = lc[t1] = u;
+      tc[t2] = lc[t2] = w;
+      hpos[q] = tpos(tc[0], tc[1], tc[2]);
+      const int nb = L.nbr6[brick * 6 + f];
+      if (nb >= 0) {
+        const int npb = pro ? L.npar6[brick * 6 + f] : 0, npo = pro ? L.npoct6[brick * 6 + f] : -1;
+        halo[q] = fx.at(nb * BR3 + ((lc[2] << 6) | (lc[1] << 3) | lc[0]), npb, npo, L.amr);
+      }
     }
   }
-  tile[tpos_local(t)] = own;
-  if (hpos >= 0) tile[hpos] = halo;
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) tile[tpos_local(t + q * NTH)] = own[q];
+#pragma unroll
+  for (int q = 0; q < HPT; ++q)
+    if (hpos[q] >= 0) tile[hpos[q]] = halo[q];
 }
 
-template <typename T, class F>
+// Stages brick `brick` of L into `tile`; NTH is the CTA's thread count.
+template <typename T, int NTH = NT, class F>
 __device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile, const F& fx) {
-  if (L.fast && blockDim.x == BR3) {
-    fill_halo_fast<T>(L, brick, tile, fx);
+  if (L.fast) {
+    fill_halo_fast<T, NTH>(L, brick, tile, fx);
     return;
   }
   if (L.amr) {
@@ -288,49 +303,62 @@ __device__ __forceinline__ void full_row(const LevelView& L, uint32_t code, cons
 // where x' / b' include pending mean / prolongation. Optionally reduces the
 // fluid sum of xout into `mean_out` (= sum / nfluid) for the next removeMean.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict__ b,
-                                               const double* bmean, XFetch<T> X, T* __restrict__ xout,
-                                               RedBuf rb, double* mean_out, double inv_nfluid,
-                                               const SolveFlags* flags, int maxit) {
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b,
+                                                const double* bmean, XFetch<T> X, T* __restrict__ xout,
+                                                RedBuf rb, double* mean_out, double inv_nfluid,
+                                                const SolveFlags* flags, int maxit) {
+  constexpr int CPT = BR3 / NTH;  // cells per thread
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   double part[1] = {0.0};
+  const bool staged = X.x || X.ec;
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
-    if (X.x || X.ec) fill_halo<T>(L, brick, tile, X);
-    __syncthreads();
-    const int c = brick * BR3 + threadIdx.x;
-    const uint32_t code = L.code[c];
-    T out = T(0);
-    if (code_type(code) == CELL_FLUID) {
-      const int ctr = tpos_local(threadIdx.x);
-      T diag, off, xc;
-      if (X.x || X.ec) {
-        full_row<T>(L, code, tile, brick, c, X, diag, off);
-        xc = tile[ctr];
-      } else {  // first sweep from x = 0: A x = 0
-        const int lev = L.amr ? L.blevel[brick] : 0;
-        diag = T(0);
+    uint32_t code[CPT];
+    T bv[CPT];
 #pragma unroll
-        for (int f = 0; f < 6; ++f) {
-          const T h2 = static_cast<T>(L.amr ? L.lh2[lev][f >> 1] : L.h2[f >> 1]);
-          if (code & (1u << f)) diag += h2;
-          else if (code & (1u << (CODE_DIRICHLET + f))) diag += T(2) * h2;
-        }
-        if (L.amr && (code & (1u << CODE_HASCF)))
-          for (int q = L.cf_off[c]; q < L.cf_off[c + 1]; ++q) diag += static_cast<T>(L.cf_coef[q]);
-        off = T(0);
-        xc = T(0);
-      }
-      T bc = b[c];
-      if (bmean) bc = bc - static_cast<T>(*bmean);
-      const T Ax = diag * xc - off;
-      const T dM = diag > T(0) ? diag : T(1);
-      out = xc + static_cast<T>(kOmega) * (bc - Ax) / dM;
-      part[0] += cell_weight(L, brick) * static_cast<double>(out);
+    for (int q = 0; q < CPT; ++q) {
+      const int c = brick * BR3 + threadIdx.x + q * NTH;
+      code[q] = L.code[c];
+      bv[q] = b[c];
     }
-    xout[c] = out;
+    if (staged) fill_halo<T, NTH>(L, brick, tile, X);
+    __syncthreads();
+    const double wgt = cell_weight(L, brick);
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      const int l = threadIdx.x + q * NTH;
+      const int c = brick * BR3 + l;
+      T out = T(0);
+      if (code_type(code[q]) == CELL_FLUID) {
+        T diag, off, xc;
+        if (staged) {
+          full_row<T>(L, code[q], tile, brick, c, X, diag, off);
+          xc = tile[tpos_local(l)];
+        } else {  // first sweep from x = 0: A x = 0
+          const int lev = L.amr ? L.blevel[brick] : 0;
+          diag = T(0);
+#pragma unroll
+          for (int f = 0; f < 6; ++f) {
+            const T h2 = static_cast<T>(L.amr ? L.lh2[lev][f >> 1] : L.h2[f >> 1]);
+            if (code[q] & (1u << f)) diag += h2;
+            else if (code[q] & (1u << (CODE_DIRICHLET + f))) diag += T(2) * h2;
+          }
+          if (L.amr && (code[q] & (1u << CODE_HASCF)))
+            for (int k = L.cf_off[c]; k < L.cf_off[c + 1]; ++k) diag += static_cast<T>(L.cf_coef[k]);
+          off = T(0);
+          xc = T(0);
+        }
+        T bc = bv[q];
+        if (bmean) bc = bc - static_cast<T>(*bmean);
+        const T Ax = diag * xc - off;
+        const T dM = diag > T(0) ? diag : T(1);
+        out = xc + static_cast<T>(kOmega) * (bc - Ax) / dM;
+        part[0] += wgt * static_cast<double>(out);
+      }
+      xout[c] = out;
+    }
     __syncthreads();
   }
   if (mean_out) {
@@ -344,12 +372,13 @@ __global__ void __launch_bounds__(NT) k_smooth(LevelView L, const T* __restrict_
 // coarse cell covered by the brick averages its fluid children, summed in the
 // reference's lexicographic child order (k, then j, then i).
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __restrict__ b,
-                                                       const double* bmean, XFetch<T> X, LevelView C,
-                                                       int fx, int fy, int fz, T* __restrict__ rc,
-                                                       RedBuf rb, double* mean_out, double inv_nfluid_c,
-                                                       const SolveFlags* flags, int maxit) {
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __restrict__ b,
+                                                        const double* bmean, XFetch<T> X, LevelView C,
+                                                        int fx, int fy, int fz, T* __restrict__ rc,
+                                                        RedBuf rb, double* mean_out, double inv_nfluid_c,
+                                                        const SolveFlags* flags, int maxit) {
+  constexpr int CPT = BR3 / NTH;  // cells per thread
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
@@ -358,71 +387,86 @@ __global__ void __launch_bounds__(NT) k_resid_restrict(LevelView F, const T* __r
   double part[1] = {0.0};
   const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
   for (int brick = blockIdx.x; brick < F.nbrick; brick += gridDim.x) {
-    fill_halo<T>(F, brick, tile, X);
-    __syncthreads();
-    const int c = brick * BR3 + threadIdx.x;
-    const uint32_t code = F.code[c];
-    const bool fluid = code_type(code) == CELL_FLUID;
-    T r = T(0);
-    if (fluid) {
-      const int ctr = tpos_local(threadIdx.x);
-      T diag, off;
-      full_row<T>(F, code, tile, brick, c, X, diag, off);
-      T bc = b[c];
-      if (bmean) bc = bc - static_cast<T>(*bmean);
-      r = bc - (diag * tile[ctr] - off);
+    uint32_t code[CPT];
+    T bv[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      const int c = brick * BR3 + threadIdx.x + q * NTH;
+      code[q] = F.code[c];
+      bv[q] = b[c];
     }
-    rs[threadIdx.x] = r;
-    fl[threadIdx.x] = fluid;
+    fill_halo<T, NTH>(F, brick, tile, X);
     __syncthreads();
-    const int t = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      const int l = threadIdx.x + q * NTH;
+      const int c = brick * BR3 + l;
+      const bool fluid = code_type(code[q]) == CELL_FLUID;
+      T r = T(0);
+      if (fluid) {
+        T diag, off;
+        full_row<T>(F, code[q], tile, brick, c, X, diag, off);
+        T bc = bv[q];
+        if (bmean) bc = bc - static_cast<T>(*bmean);
+        r = bc - (diag * tile[tpos_local(l)] - off);
+      }
+      rs[l] = r;
+      fl[l] = fluid;
+    }
+    __syncthreads();
     if (F.amr) {
       // composite transfer: a kept brick maps cell-for-cell; a merged brick
       // fills one octant (4^3 cells) of its parent with child averages.
       const int cb = F.xf_brick[brick], oct = F.xf_oct[brick];
       const double wc = cell_weight(C, cb);
       if (oct < 0) {
-        const T val = fl[t] ? rs[t] : T(0);
-        rc[cb * BR3 + t] = val;
-        part[0] += wc * static_cast<double>(val);
-      } else if (t < 64) {
-        const int lci = t & 3, lcj = (t >> 2) & 3, lck = t >> 4;
-        T sum = T(0);
-        int count = 0;
-        for (int dk = 0; dk < 2; ++dk)
-          for (int dj = 0; dj < 2; ++dj)
-            for (int di = 0; di < 2; ++di) {
-              const int l = ((2 * lck + dk) << 6) | ((2 * lcj + dj) << 3) | (2 * lci + di);
-              if (fl[l]) {
-                sum += rs[l];
-                ++count;
+        for (int t = threadIdx.x; t < BR3; t += NTH) {
+          const T val = fl[t] ? rs[t] : T(0);
+          rc[cb * BR3 + t] = val;
+          part[0] += wc * static_cast<double>(val);
+        }
+      } else {
+        for (int t = threadIdx.x; t < 64; t += NTH) {
+          const int lci = t & 3, lcj = (t >> 2) & 3, lck = t >> 4;
+          T sum = T(0);
+          int count = 0;
+          for (int dk = 0; dk < 2; ++dk)
+            for (int dj = 0; dj < 2; ++dj)
+              for (int di = 0; di < 2; ++di) {
+                const int l = ((2 * lck + dk) << 6) | ((2 * lcj + dj) << 3) | (2 * lci + di);
+                if (fl[l]) {
+                  sum += rs[l];
+                  ++count;
+                }
               }
-            }
-        const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
-        const int ci = (oct & 1) * 4 + lci, cj = ((oct >> 1) & 1) * 4 + lcj, ck = (oct >> 2) * 4 + lck;
-        rc[cb * BR3 + ((ck << 6) | (cj << 3) | ci)] = val;
-        part[0] += wc * static_cast<double>(val);
+          const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
+          const int ci = (oct & 1) * 4 + lci, cj = ((oct >> 1) & 1) * 4 + lcj, ck = (oct >> 2) * 4 + lck;
+          rc[cb * BR3 + ((ck << 6) | (cj << 3) | ci)] = val;
+          part[0] += wc * static_cast<double>(val);
+        }
       }
-    } else if (t < cx * cy * cz) {
-      const int lci = t % cx, lcj = (t / cx) % cy, lck = t / (cx * cy);
-      const int gci = F.bcoord[3 * brick] * cx + lci;
-      const int gcj = F.bcoord[3 * brick + 1] * cy + lcj;
-      const int gck = F.bcoord[3 * brick + 2] * cz + lck;
-      if (gci < C.nx && gcj < C.ny && gck < C.nz) {
-        T sum = T(0);
-        int count = 0;
-        for (int dk = 0; dk < fz; ++dk)
-          for (int dj = 0; dj < fy; ++dj)
-            for (int di = 0; di < fx; ++di) {
-              const int l = ((lck * fz + dk) << 6) | ((lcj * fy + dj) << 3) | (lci * fx + di);
-              if (fl[l]) {
-                sum += rs[l];
-                ++count;
+    } else {
+      for (int t = threadIdx.x; t < cx * cy * cz; t += NTH) {
+        const int lci = t % cx, lcj = (t / cx) % cy, lck = t / (cx * cy);
+        const int gci = F.bcoord[3 * brick] * cx + lci;
+        const int gcj = F.bcoord[3 * brick + 1] * cy + lcj;
+        const int gck = F.bcoord[3 * brick + 2] * cz + lck;
+        if (gci < C.nx && gcj < C.ny && gck < C.nz) {
+          T sum = T(0);
+          int count = 0;
+          for (int dk = 0; dk < fz; ++dk)
+            for (int dj = 0; dj < fy; ++dj)
+              for (int di = 0; di < fx; ++di) {
+                const int l = ((lck * fz + dk) << 6) | ((lcj * fy + dj) << 3) | (lci * fx + di);
+                if (fl[l]) {
+                  sum += rs[l];
+                  ++count;
+                }
               }
-            }
-        const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
-        rc[cell_index(C, gci, gcj, gck)] = val;
-        part[0] += static_cast<double>(val);
+          const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
+          rc[cell_index(C, gci, gcj, gck)] = val;
+          part[0] += static_cast<double>(val);
+        }
       }
     }
     __syncthreads();
@@ -880,31 +924,44 @@ __global__ void __launch_bounds__(NT) k_pcg_dir(LevelView L, const double* __res
 }
 
 // Ap = A p ; S_PAP = p.Ap ; alpha = rz / pAp or breakdown (multigrid.cpp:303-308).
-__global__ void __launch_bounds__(NT) k_pcg_matvec(LevelView L, const double* __restrict__ p,
-                                                   double* __restrict__ Ap, RedBuf rb, double* S,
-                                                   SolveFlags* flags, int maxit) {
+template <int NTH>
+__global__ void __launch_bounds__(NTH) k_pcg_matvec(LevelView L, const double* __restrict__ p,
+                                                    double* __restrict__ Ap, RedBuf rb, double* S,
+                                                    SolveFlags* flags, int maxit) {
+  constexpr int CPT = BR3 / NTH;  // cells per thread
   pdl_wait();
   if (stopped(flags, maxit)) return;
   DFetch X{p, nullptr};
   __shared__ double tile[TSN];
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
-    fill_halo<double>(L, brick, tile, X);
-    __syncthreads();
-    const int c = brick * BR3 + threadIdx.x;
-    const uint32_t code = L.code[c];
-    const int ty = code_type(code);
-    const double pc = p[c];
-    double o = 0.0;
-    if (ty == CELL_SOLID) {
-      o = pc;
-    } else if (ty == CELL_FLUID) {
-      double diag, off;
-      full_row<double>(L, code, tile, brick, c, X, diag, off);
-      o = diag * pc - off;
+    uint32_t code[CPT];
+    double pv[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      code[q] = L.code[brick * BR3 + threadIdx.x + q * NTH];
+      pv[q] = p[brick * BR3 + threadIdx.x + q * NTH];
     }
-    Ap[c] = o;
-    part[0] += cell_weight(L, brick) * (pc * o);
+    fill_halo<double, NTH>(L, brick, tile, X);
+    __syncthreads();
+    const double wgt = cell_weight(L, brick);
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      const int l = threadIdx.x + q * NTH;
+      const int c = brick * BR3 + l;
+      const int ty = code_type(code[q]);
+      const double pc = pv[q];
+      double o = 0.0;
+      if (ty == CELL_SOLID) {
+        o = pc;
+      } else if (ty == CELL_FLUID) {
+        double diag, off;
+        full_row<double>(L, code[q], tile, brick, c, X, diag, off);
+        o = diag * pc - off;
+      }
+      Ap[c] = o;
+      part[0] += wgt * (pc * o);
+    }
     __syncthreads();
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) {
@@ -1389,7 +1446,8 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
   int dev = 0, nsm = 148;
   NB_CUDA(cudaGetDevice(&dev));
   NB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int per_sm = std::min(std::max(t.mg_ctas_per_sm, 1), 4);
+  tpb_ = (t.threads_per_brick == 128 || t.threads_per_brick == 256) ? t.threads_per_brick : 512;
+  const int per_sm = std::min(std::max(t.mg_ctas_per_sm, 1), 16);
   grid_cap_ = std::min(per_sm * nsm, MAX_GRID);  // the reduction buffer holds MAX_GRID partials
   pdl_ = t.pdl != 0;
   sweeps_ = precision_ == NB_PRECISION_MIXED ? std::min(std::max(t.sweeps, 1), 3) : 2;  // FP64: V(2,2) as the reference
@@ -1535,18 +1593,22 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   DevLevel& Cd = lv_[lvl + 1];
   const LevelView& C = Cd.v;
   const double ncoarse = Cd.ncell;
+  // kernels for the tuned CTA size (threads per brick)
+  const auto ks = tpb_ == 128 ? k_smooth<T, 128> : (tpb_ == 256 ? k_smooth<T, 256> : k_smooth<T, 512>);
+  const auto kr = tpb_ == 128 ? k_resid_restrict<T, 128>
+                              : (tpb_ == 256 ? k_resid_restrict<T, 256> : k_resid_restrict<T, 512>);
   // Ping-pong buffers with their pending means: xa <-> slot 0, xb <-> slot 1.
   T* buf[2] = {xa, xb};
   double* mean[2] = {mA, mB};
   int cur = 0;
   // pre-smoothing (sweeps_ sweeps; 2 as the reference), the first from x = 0
   NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
-            (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                         XFetch<T>{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1}, buf[cur], rb_, mean[cur],
                         inv_nf, flags_, maxit_)));
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
     NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-              (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                           XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, buf[cur ^ 1], rb_,
                           mean[cur ^ 1], inv_nf, flags_, maxit_)));
   // residual + restriction
@@ -1554,7 +1616,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const int cb_slot = lvl_slot(lvl + 1, 2);
   double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
   NB_LAUNCH(lc_, "resid_restrict", s, ncell * (2 * tsz + 1) + ncoarse * tsz,
-            (launch_pdl(pdl_, k_resid_restrict<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+            (launch_pdl(pdl_, kr, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                         XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, C, Cd.h.fx, Cd.h.fy,
                         Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_)));
   void* ec = nullptr;
@@ -1563,14 +1625,14 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
   // post-smoothing: the first sweep folds in the prolongation x += P e
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
-            (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                         XFetch<T>{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
                                   Cd.h.fz, D.d_xfb, D.d_xfo},
                         buf[cur ^ 1], rb_, mean[cur ^ 1], inv_nf, flags_, maxit_)));
   cur ^= 1;
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
     NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-              (launch_pdl(pdl_, k_smooth<T>, dim3(grid), dim3(NT), 0, s, L, b, bmean,
+              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                           XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, buf[cur ^ 1], rb_,
                           mean[cur ^ 1], inv_nf, flags_, maxit_)));
   *out_x = buf[cur];
@@ -1587,9 +1649,10 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   const bool mixed = precision_ == NB_PRECISION_MIXED;
   const double n = lv_[0].ncell;
   const double zsz = mixed ? 4.0 : 8.0;
+  const auto km = tpb_ == 128 ? k_pcg_matvec<128> : (tpb_ == 256 ? k_pcg_matvec<256> : k_pcg_matvec<512>);
   for (int k = 0; k < count; ++k) {
     NB_LAUNCH(lc_, "pcg_matvec", s, n * 17,
-              launch_pdl(pdl_, k_pcg_matvec, dim3(grid), dim3(NT), 0, s, L, p_, Ap_, rb_, S_, flags_, maxit));
+              launch_pdl(pdl_, km, dim3(grid), dim3(tpb_), 0, s, L, p_, Ap_, rb_, S_, flags_, maxit));
     NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0)),
               (launch_pdl(pdl_, k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
                                                 sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol)));

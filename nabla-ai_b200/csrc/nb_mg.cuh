@@ -102,6 +102,7 @@ class MgSolver {
   void set_tuning(const nb_tuning* tune);
   int grid_of(int nbrick) const { return nbrick < grid_cap_ ? nbrick : grid_cap_; }
   int grid_cap_ = 0;   // CTAs of the brick kernels
+  int tpb_ = 512;      // threads per CTA of the smoother, residual and matvec kernels
   bool pdl_ = true;    // programmatic dependent launch of the chains
   int sweeps_ = 2;     // smoothing sweeps per side of the coarse correction
   int halo_mode_ = 0;  // 0 per-brick neighbour maps, 1 per-cell walk

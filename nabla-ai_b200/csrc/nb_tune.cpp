@@ -1,8 +1,9 @@
 // nb_tune.cpp — launch tuning of a context and the autotuner (no reference
 // counterpart).
 //
-// The tuned choices change launch shapes, the multigrid halo staging, the
-// mixed form's smoothing sweeps, the exact coarse-solve threshold and PDL.
+// The tuned choices change launch shapes (threads per brick and CTAs per SM),
+// the multigrid halo staging, the mixed form's smoothing sweeps, the exact
+// coarse-solve threshold and PDL.
 // None of them changes the discretisation: FP64 results move only by the
 // summation order of the grid reductions (grid size), mixed results by the
 // preconditioner (sweeps, coarse solve) within the solve tolerance.
@@ -11,6 +12,7 @@
 // CUDA events on the case's stream, by coordinate descent from the default,
 // and caches the winner per (GPU, SM count, mesh kind, precision, levels,
 // size class) in a text file.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,12 +28,14 @@ using namespace nb;
 namespace {
 
 bool tuning_ok(const nb_tuning& t, std::string& why) {
-  if (t.mg_ctas_per_sm < 1 || t.mg_ctas_per_sm > 4) why = "mg_ctas_per_sm must be in 1..4";
+  if (t.mg_ctas_per_sm < 1 || t.mg_ctas_per_sm > 16) why = "mg_ctas_per_sm must be in 1..16";
   else if (t.rhs_ctas_per_sm < 1 || t.rhs_ctas_per_sm > 4) why = "rhs_ctas_per_sm must be in 1..4";
   else if (t.halo_mode != 0 && t.halo_mode != 1) why = "halo_mode must be 0 or 1";
   else if (t.sweeps < 1 || t.sweeps > 3) why = "sweeps must be in 1..3";
   else if (t.coarse_direct_max < 0 || t.coarse_direct_max > 512) why = "coarse_direct_max must be in 0..512";
   else if (t.pdl != 0 && t.pdl != 1) why = "pdl must be 0 or 1";
+  else if (t.threads_per_brick != 128 && t.threads_per_brick != 256 && t.threads_per_brick != 512)
+    why = "threads_per_brick must be 128, 256 or 512";
   else return true;
   return false;
 }
@@ -54,11 +58,11 @@ std::string tune_key(nb_ctx* ctx, const nb_case* c) {
   return s;
 }
 
-// One cache line: key and the six fields, then ms per step.
+// One cache line: key and the seven fields, then ms per step.
 bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double& ms) {
   std::istringstream in(line);
   if (!(in >> key >> t.mg_ctas_per_sm >> t.rhs_ctas_per_sm >> t.halo_mode >> t.sweeps >> t.coarse_direct_max >>
-        t.pdl >> ms))
+        t.pdl >> t.threads_per_brick >> ms))
     return false;
   std::string why;
   return tuning_ok(t, why);
@@ -66,8 +70,8 @@ bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double&
 
 std::string format_line(const std::string& key, const nb_tuning& t, double ms) {
   char buf[320];
-  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm, t.rhs_ctas_per_sm,
-                t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, ms);
+  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm, t.rhs_ctas_per_sm,
+                t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, ms);
   return buf;
 }
 
@@ -89,6 +93,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->sweeps = 2;
   t->coarse_direct_max = 256;
   t->pdl = 1;
+  t->threads_per_brick = 512;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {
@@ -232,12 +237,37 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
   if (best_ms < 0.0)
     return fail(ctx, NB_ERR_NOT_CONVERGED, "nb_autotune: the sample does not converge to divergence <= 1e-8");
   rep->default_ms = best_ms;
+  auto consider = [&](const nb_tuning& cand) -> nb_status {
+    double ms = 0.0;
+    const nb_status s = time_one(cand, &ms);
+    if (s == NB_OK && ms >= 0.0 && ms < 0.98 * best_ms) {
+      best = cand;
+      best_ms = ms;
+    }
+    return s;
+  };
+  // threads per brick, keeping the resident threads per SM
+  for (int32_t v : {256, 128}) {
+    nb_tuning cand = best;
+    cand.threads_per_brick = v;
+    cand.mg_ctas_per_sm = std::min(16, best.mg_ctas_per_sm * best.threads_per_brick / v);
+    if ((st = consider(cand)) != NB_OK) return st;
+  }
+  // multigrid CTAs per SM: 1/4 .. 1 of a full SM (2048 threads)
+  {
+    const int full = 2048 / best.threads_per_brick;
+    for (int32_t v : {full / 4, full / 2, 3 * full / 4, full}) {
+      if (v == best.mg_ctas_per_sm) continue;
+      nb_tuning cand = best;
+      cand.mg_ctas_per_sm = v;
+      if ((st = consider(cand)) != NB_OK) return st;
+    }
+  }
   struct Knob {
     int32_t nb_tuning::*field;
     std::vector<int32_t> values;
   };
-  std::vector<Knob> knobs = {{&nb_tuning::mg_ctas_per_sm, {1, 2, 3, 4}},
-                             {&nb_tuning::rhs_ctas_per_sm, {1, 2, 3, 4}},
+  std::vector<Knob> knobs = {{&nb_tuning::rhs_ctas_per_sm, {1, 2, 3, 4}},
                              {&nb_tuning::halo_mode, {0, 1}},
                              {&nb_tuning::pdl, {0, 1}}};
   if (prec == NB_PRECISION_MIXED) knobs.push_back({&nb_tuning::sweeps, {1, 2, 3}});
@@ -247,13 +277,7 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
       if (best.*(k.field) == v) continue;
       nb_tuning cand = best;
       cand.*(k.field) = v;
-      double ms = 0.0;
-      st = time_one(cand, &ms);
-      if (st != NB_OK) return st;
-      if (ms >= 0.0 && ms < 0.98 * best_ms) {
-        best = cand;
-        best_ms = ms;
-      }
+      if ((st = consider(cand)) != NB_OK) return st;
     }
   ctx->tune = best;
   rep->best = best;

@@ -44,7 +44,9 @@ def _run(ctx, precision, tuning, nsteps=3):
 
 
 VARIANTS = [dict(mg_ctas_per_sm=1, rhs_ctas_per_sm=1), dict(halo_mode=1), dict(pdl=0),
-            dict(coarse_direct_max=0), dict(coarse_direct_max=512), dict(mg_ctas_per_sm=3, rhs_ctas_per_sm=4)]
+            dict(coarse_direct_max=0), dict(coarse_direct_max=512), dict(mg_ctas_per_sm=3, rhs_ctas_per_sm=4),
+            dict(threads_per_brick=256, mg_ctas_per_sm=8), dict(threads_per_brick=128, mg_ctas_per_sm=16),
+            dict(threads_per_brick=128, mg_ctas_per_sm=5, halo_mode=1)]
 
 
 @pytest.mark.parametrize("tuning", VARIANTS)
@@ -87,3 +89,25 @@ def test_autotune_and_cache(ctx, tmp_path):
         assert rep.converged and rep.divergence_max <= 1e-8
     finally:
         ctx.set_tuning(**solver.default_tuning())
+
+
+@pytest.mark.parametrize("tpb", [128, 256])
+def test_uniform_threads_per_brick(ctx, tpb):
+    """Uniform periodic grid (Taylor-Green 16^3): the smaller CTAs give the
+    default's solution to 1e-10 relative."""
+    def run(tuning):
+        ctx.set_tuning(**tuning)
+        try:
+            g, cfg = cases.taylor_green(16)
+            ns = solver.NSSolver(g, cfg, ctx=ctx)
+            ns.set_state(*cases.taylor_green_state(g))
+            for _ in range(2):
+                rep = ns.step(0.05)
+                assert rep.converged
+            return ns.u_face(), ns.pressure()
+        finally:
+            ctx.set_tuning(**solver.default_tuning())
+    u0, p0 = run({})
+    u1, p1 = run(dict(threads_per_brick=tpb, mg_ctas_per_sm=2048 // tpb))
+    assert np.abs(u1 - u0).max() <= 1e-10 * np.abs(u0).max()
+    assert np.abs(p1 - p0).max() <= 1e-10 * max(np.abs(p0).max(), 1e-30)
