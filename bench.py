@@ -231,6 +231,8 @@ def run_ours(args, rank, world, local_rank):
     device = f"cuda:{local_rank}"
     torch.cuda.set_device(local_rank)
     ctx = solver.Context(local_rank)
+    if args.tuning:
+        ctx.set_tuning(**args.tuning)
     precision = args.precision or ("mixed" if args.workload == "channel3" else "fp64")
     prec = abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64
     run = make_run(args.workload, ctx, prec)
@@ -298,7 +300,7 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_step": round(elapsed_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == abi.PRECISION_FP64 else "f32+f64",
         "data": run.data,
-        "config": {"workload": run.desc, "cells": cells, "precision": precision,
+        "config": {"workload": run.desc, "cells": cells, "precision": precision, "tuning": ctx.tuning,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed between timed steps (256 MiB write); working set < L2",
                    "poisson_cycles_per_step": reps[-1].poisson_iters},
@@ -753,7 +755,8 @@ def main():
                     help="batch96: build the batch from these case seeds instead of 0..batch-1")
     ap.add_argument("--single-form", action="store_true", help="batch96: time the primary precision only")
     ap.add_argument("--tuning", type=lambda t: {k: int(v) for k, v in (kv.split("=") for kv in t.split(","))},
-                    default=None, help="batch96: fixed nb_tuning fields, e.g. threads_per_brick=128,mg_ctas_per_sm=9")
+                    default=None, help="fixed nb_tuning fields, e.g. threads_per_brick=128,mg_ctas_per_sm=9 "
+                    "(channel3, tgv64, batch96)")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="serve: arrival window")
     ap.add_argument("--min-steps", type=int, default=10)

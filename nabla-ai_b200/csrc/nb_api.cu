@@ -67,7 +67,7 @@ struct nb_case {
   uint64_t bytes = 0;
   bool has_solid = false;
   uint64_t nfluid = 0;
-  int rhs_grid = 296;  // CTAs of the momentum kernel (tuning)
+  int rhs_grid = 592;  // CTAs of the momentum kernel (tuning)
   int step = 0;
   double t = 0.0, dt_last = 0.0;
   // ---- octree-AMR cases (the mesh outlives the case) ----

@@ -88,7 +88,7 @@ extern "C" {
 void nb_tuning_default(nb_tuning* t) {
   if (!t) return;
   t->mg_ctas_per_sm = 4;
-  t->rhs_ctas_per_sm = 2;
+  t->rhs_ctas_per_sm = 4;
   t->halo_mode = 0;
   t->sweeps = 2;
   t->coarse_direct_max = 256;

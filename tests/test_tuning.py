@@ -12,7 +12,7 @@ def _lib():
 
 
 def test_default_tuning():
-    assert solver.default_tuning() == {"mg_ctas_per_sm": 4, "rhs_ctas_per_sm": 2, "halo_mode": 0, "sweeps": 2,
+    assert solver.default_tuning() == {"mg_ctas_per_sm": 4, "rhs_ctas_per_sm": 4, "halo_mode": 0, "sweeps": 2,
                                        "coarse_direct_max": 256, "pdl": 1, "threads_per_brick": 512}
 
 
@@ -57,7 +57,7 @@ def test_cache_rejects_bad_key_and_malformed_file(tmp_path):
     lib = _lib()
     path = tmp_path / "tune.txt"
     assert lib.nb_tune_cache_store(str(path).encode(), b"a key", C.byref(_tuning()), 1.0) == abi.NB_ERR_BAD_ARG
-    path.write_text("# comment\n\ngpu/a 4 2 0 2 256 1 512 1.0\ngpu/b 4 2\n")
+    path.write_text("# comment\n\ngpu/a 4 4 0 2 256 1 512 1.0\ngpu/b 4 2\n")
     out = abi.Tuning()
     assert lib.nb_tune_cache_lookup(str(path).encode(), b"gpu/a", C.byref(out), None) == 1
     assert lib.nb_tune_cache_lookup(str(path).encode(), b"gpu/b", C.byref(out), None) == -1
