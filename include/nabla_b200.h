@@ -303,6 +303,25 @@ nb_status nb_amr_case_set_state(nb_case* c, const double* u, const double* v, co
 /* Any pointer may be NULL to skip that field. */
 nb_status nb_amr_case_get_state(nb_case* c, double* u, double* v, double* w, double* p);
 
+/* ---- checkpoints ------------------------------------------------------------
+ * Replace writeCheckpoint / readCheckpoint (core/src/flow/case.cpp:244-319).
+ * Uniform cases use the reference's NBFCK01 layout: 8 magic bytes "NBFCK01\0",
+ * int32 nx, ny, nz, int32 step, FP64 t, FP64 dt, then u, v, w, p each as a
+ * uint64 count and that many FP64 values in the reference's lexicographic MAC
+ * layout, host byte order; a file moves between the reference and this library
+ * in either direction. Octree cases (no reference counterpart) use NBFAMR1:
+ * magic, int32 leaf count, the leaves (4 int32 each, rank order), int32 step,
+ * FP64 t, FP64 dt, then the u, v, w face arrays in storage order and p, each
+ * count-prefixed. Reading checks the magic, the grid dimensions or leaf list
+ * and every array size (NB_ERR_BAD_ARG otherwise) and restores the step clock:
+ * a restart continues bit for bit. */
+nb_status nb_case_write_checkpoint(nb_case* c, const char* path);
+nb_status nb_case_read_checkpoint(nb_case* c, const char* path);
+/* Host only: header of a checkpoint file. kind 0 = NBFCK01 (dims set),
+ * 1 = NBFAMR1 (nleaf set). Returns 0, or -1 for an unreadable or foreign file. */
+int nb_checkpoint_info(const char* path, int32_t* kind, int32_t dims[3], int64_t* nleaf, int32_t* step,
+                       double* t, double* dt);
+
 /* ---- allocation-free operator ---------------------------------------------
  * No counterpart in the reference. The same -Laplacian as nb_apply_laplacian,
  * for callers that cannot call cudaMalloc: code issuing work while a stream is

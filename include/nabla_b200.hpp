@@ -156,6 +156,14 @@ class NSSolver {
   }
   [[nodiscard]] uint64_t deviceBytes() const { return nb_case_device_bytes(h_.get()); }
   [[nodiscard]] nb_case* handle() const { return h_.get(); }
+  // writeCheckpoint / readCheckpoint (core/src/flow/case.cpp:274-319): the NBFCK01 file.
+  void writeCheckpoint(const std::string& path) const {
+    ctx_->check(nb_case_write_checkpoint(h_.get(), path.c_str()), "writeCheckpoint");
+  }
+  void readCheckpoint(const std::string& path) {
+    ctx_->check(nb_case_read_checkpoint(h_.get(), path.c_str()), "readCheckpoint");
+    invalidate();
+  }
 
  private:
   struct Clock {

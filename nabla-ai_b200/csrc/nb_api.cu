@@ -660,6 +660,22 @@ void nb::case_kind(const nb_case* c, int* amr, int* precision, int* levels) {
   *levels = c->amr ? c->mesh->lvl.tree.nlev : 1;
 }
 
+nb_ctx* nb::case_ctx(const nb_case* c) { return c->ctx; }
+
+void nb::case_dims(const nb_case* c, int dims[3]) {
+  dims[0] = c->grid.nx;
+  dims[1] = c->grid.ny;
+  dims[2] = c->grid.nz;
+}
+
+nb_amr_mesh* nb::case_mesh(const nb_case* c) { return c->amr ? c->mesh : nullptr; }
+
+void nb::case_set_clock(nb_case* c, int step, double t, double dt_last) {
+  c->step = step;
+  c->t = t;
+  c->dt_last = dt_last;
+}
+
 nb_status nb::clone_case(nb_case* src, nb_case** out) {
   nb_ctx* ctx = src->ctx;
   nb_case* c = nullptr;

@@ -70,6 +70,12 @@ void ctx_release(nb_ctx* ctx);
 nb_status clone_case(nb_case* sample, nb_case** out);
 // Kind of a case for the tuning cache key.
 void case_kind(const nb_case* c, int* amr, int* precision, int* levels);
+// Case internals for the checkpoint files: owning context, uniform grid
+// dimensions, octree mesh (nullptr for uniform cases), and the step clock.
+nb_ctx* case_ctx(const nb_case* c);
+void case_dims(const nb_case* c, int dims[3]);
+nb_amr_mesh* case_mesh(const nb_case* c);
+void case_set_clock(nb_case* c, int step, double t, double dt_last);
 
 // Grows the context's two staging buffers to at least `elems` doubles each.
 void ensure_staging(nb_ctx* ctx, size_t elems);

@@ -177,6 +177,10 @@ PROTOTYPES = [
     ("nb_case_cell_count", C.c_uint64, [VP]),
     ("nb_case_stream", VP, [VP]),
     ("nb_ctx_profile", C.c_int, [VP, C.c_char_p]),
+    ("nb_case_write_checkpoint", C.c_int, [VP, C.c_char_p]),
+    ("nb_case_read_checkpoint", C.c_int, [VP, C.c_char_p]),
+    ("nb_checkpoint_info", C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_int32), DP, DP]),
     ("nb_tuning_default", None, [C.POINTER(Tuning)]),
     ("nb_ctx_set_tuning", C.c_int, [VP, C.POINTER(Tuning)]),
     ("nb_ctx_get_tuning", C.c_int, [VP, C.POINTER(Tuning)]),

@@ -156,6 +156,14 @@ class AmrCase:
             self.ctx.lib.nb_case_destroy(self.h)
             self.h = None
 
+    def write_checkpoint(self, path):
+        """Octree checkpoint (NBFAMR1): leaf list, step clock, u, v, w, p."""
+        self.ctx.check(self.ctx.lib.nb_case_write_checkpoint(self.h, str(path).encode()), "write_checkpoint")
+
+    def read_checkpoint(self, path):
+        """Restores state and step clock from an NBFAMR1 file of the same mesh."""
+        self.ctx.check(self.ctx.lib.nb_case_read_checkpoint(self.h, str(path).encode()), "read_checkpoint")
+
     def __del__(self):
         self.close()
 

@@ -147,6 +147,14 @@ class NSSolver:
     def initialize(self):
         self.ctx.check(self.ctx.lib.nb_case_initialize(self.h), "initialize")
 
+    def write_checkpoint(self, path):
+        """writeCheckpoint (core/src/flow/case.cpp:274-294): the reference's NBFCK01 file."""
+        self.ctx.check(self.ctx.lib.nb_case_write_checkpoint(self.h, str(path).encode()), "write_checkpoint")
+
+    def read_checkpoint(self, path):
+        """readCheckpoint (core/src/flow/case.cpp:296-319): state and step clock from an NBFCK01 file."""
+        self.ctx.check(self.ctx.lib.nb_case_read_checkpoint(self.h, str(path).encode()), "read_checkpoint")
+
     def set_state(self, u, v, w, p, step=0, t=0.0, dt_last=0.0):
         nu, nv, nw, np_ = self.grid.sizes()
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, p)]
@@ -255,3 +263,19 @@ def autotune(case, steps: int = 3, cache: str | None = "default") -> dict:
     return {"best": rep.best.as_dict(), "best_ms": rep.best_ms, "default_ms": rep.default_ms,
             "candidates": rep.candidates, "rejected": rep.rejected, "from_cache": bool(rep.from_cache),
             "key": rep.key.decode()}
+
+
+def checkpoint_info(path) -> dict | None:
+    """Header of a checkpoint file (host only): kind "uniform" (NBFCK01, dims)
+    or "octree" (NBFAMR1, leaf count), step, t, dt; None if unreadable."""
+    kind, dims = C.c_int32(), (C.c_int32 * 3)()
+    nleaf, step, t, dt = C.c_int64(), C.c_int32(), C.c_double(), C.c_double()
+    if abi.load().nb_checkpoint_info(str(path).encode(), C.byref(kind), dims, C.byref(nleaf), C.byref(step),
+                                     C.byref(t), C.byref(dt)) != 0:
+        return None
+    out = {"kind": "uniform" if kind.value == 0 else "octree", "step": step.value, "t": t.value, "dt": dt.value}
+    if kind.value == 0:
+        out["dims"] = tuple(dims)
+    else:
+        out["leaves"] = nleaf.value
+    return out

@@ -321,6 +321,16 @@ class _NS:
         getattr(self.lib, f"{self.p}_ns_step")(self.h, dt, C.byref(rep))
         return rep
 
+    def write_checkpoint(self, path):
+        """The reference's writeCheckpoint (core/src/flow/case.cpp:274-294)."""
+        if getattr(self.lib, f"{self.p}_ns_write_checkpoint")(self.h, str(path).encode()):
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def read_checkpoint(self, path):
+        """The reference's readCheckpoint (core/src/flow/case.cpp:296-319)."""
+        if getattr(self.lib, f"{self.p}_ns_read_checkpoint")(self.h, str(path).encode()):
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
 
 class Dropin:
     """The reference's own NSSolver / PoissonSolver seams with the B200 library
