@@ -322,6 +322,36 @@ nb_status nb_case_read_checkpoint(nb_case* c, const char* path);
 int nb_checkpoint_info(const char* path, int32_t* kind, int32_t dims[3], int64_t* nleaf, int32_t* step,
                        double* t, double* dt);
 
+/* ---- case run loop ------------------------------------------------------------
+ * Replaces runCase (core/src/flow/case.cpp:349-401), the loop behind
+ * `nabla_solve run`: create and initialize the case, optionally restart from
+ * a checkpoint, then step (dt from computeDt) up to max_steps times, appending
+ * one diagnostics.jsonl record per step in the reference's schema and number
+ * formatting (a provenance line first in a fresh file), writing
+ * checkpoint_<step>.ckpt every checkpoint_every steps and final.ckpt at the
+ * end, stopping at stop_time or when the momentum residual falls below
+ * steady_tol after step 20. No .vtu snapshots are written. */
+typedef struct nb_run_options {
+  const char* run_dir;        /* RunOptions::runDir (created if missing) */
+  int32_t max_steps;          /* RunOptions::maxSteps */
+  int32_t checkpoint_every;   /* RunOptions::checkpointEvery (0: final only) */
+  double stop_time;           /* RunOptions::stopTime (0: ignore) */
+  double steady_tol;          /* RunOptions::steadyTol (0: ignore) */
+  const char* restart_from;   /* RunOptions::restartFrom (NULL or "": fresh run) */
+  int32_t precision;          /* NB_PRECISION_* */
+  int32_t reserved;
+} nb_run_options;
+
+typedef struct nb_run_summary {  /* mirrors RunSummary (case.hpp:29-40) */
+  int32_t steps;
+  int32_t steady;
+  double time, momentum_residual, continuity_residual, mass_error, cd, cl;
+  uint64_t cells;
+} nb_run_summary;
+
+nb_status nb_run_case(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_config* cfg, const nb_run_options* opt,
+                      nb_run_summary* out);
+
 /* ---- allocation-free operator ---------------------------------------------
  * No counterpart in the reference. The same -Laplacian as nb_apply_laplacian,
  * for callers that cannot call cudaMalloc: code issuing work while a stream is

@@ -205,4 +205,13 @@ class NSSolver {
   mutable std::unique_ptr<Fields> cache_;
 };
 
+// runCase (core/src/flow/case.cpp:349-401) on the GPU: the run loop of
+// `nabla_solve run` with diagnostics.jsonl and checkpoints in opt.run_dir.
+inline nb_run_summary runCase(const std::shared_ptr<Context>& ctx, const nb_grid_desc& grid,
+                              const nb_flow_config& flow, const nb_run_options& opt) {
+  nb_run_summary s{};
+  ctx->check(nb_run_case(ctx->get(), &grid, &flow, &opt, &s), "runCase");
+  return s;
+}
+
 }  // namespace nabla_b200

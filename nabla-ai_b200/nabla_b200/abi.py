@@ -152,6 +152,23 @@ class TuneReport(C.Structure):
     ]
 
 
+class RunOptions(C.Structure):
+    _fields_ = [("run_dir", C.c_char_p), ("max_steps", C.c_int32), ("checkpoint_every", C.c_int32),
+                ("stop_time", C.c_double), ("steady_tol", C.c_double), ("restart_from", C.c_char_p),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]
+
+
+class RunSummary(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("steady", C.c_int32), ("time", C.c_double),
+                ("momentum_residual", C.c_double), ("continuity_residual", C.c_double),
+                ("mass_error", C.c_double), ("cd", C.c_double), ("cl", C.c_double), ("cells", C.c_uint64)]
+
+    def as_dict(self):
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["steady"] = bool(d["steady"])
+        return d
+
+
 # (name, restype, argtypes) for every symbol declared in include/nabla_b200.h
 PROTOTYPES = [
     ("nb_ctx_create", C.c_int, [C.c_int, C.POINTER(VP)]),
@@ -177,6 +194,8 @@ PROTOTYPES = [
     ("nb_case_cell_count", C.c_uint64, [VP]),
     ("nb_case_stream", VP, [VP]),
     ("nb_ctx_profile", C.c_int, [VP, C.c_char_p]),
+    ("nb_run_case", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(FlowConfig), C.POINTER(RunOptions),
+                              C.POINTER(RunSummary)]),
     ("nb_case_write_checkpoint", C.c_int, [VP, C.c_char_p]),
     ("nb_case_read_checkpoint", C.c_int, [VP, C.c_char_p]),
     ("nb_checkpoint_info", C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),

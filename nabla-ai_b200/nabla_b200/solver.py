@@ -279,3 +279,17 @@ def checkpoint_info(path) -> dict | None:
     else:
         out["leaves"] = nleaf.value
     return out
+
+
+def run_case(grid: Grid, config: abi.FlowConfig, run_dir, max_steps: int, *, checkpoint_every: int = 0,
+             stop_time: float = 0.0, steady_tol: float = 0.0, restart_from=None,
+             precision: int = abi.PRECISION_FP64, ctx: Context | None = None) -> dict:
+    """nb_run_case: runCase (core/src/flow/case.cpp:349-401) on the GPU, writing
+    diagnostics.jsonl and checkpoints into run_dir. Returns the RunSummary."""
+    ctx = ctx or default_context()
+    opt = abi.RunOptions(str(run_dir).encode(), max_steps, checkpoint_every, stop_time, steady_tol,
+                         str(restart_from).encode() if restart_from else None, precision, 0)
+    out = abi.RunSummary()
+    ctx.check(ctx.lib.nb_run_case(ctx.h, C.byref(grid.desc()), C.byref(config), C.byref(opt), C.byref(out)),
+              "nb_run_case")
+    return out.as_dict()

@@ -160,6 +160,8 @@ class Reference(_Common):
         L.ref_ns_step.argtypes = [C.c_void_p, C.c_double, RP]
         L.ref_ns_write_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_ns_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
+        L.ref_run_case.argtypes = [GP, FP, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_char_p,
+                                   DP, C.POINTER(C.c_int)]
         L.ref_morton_encode.restype = C.c_uint64
         L.ref_morton_encode.argtypes = [C.c_uint32] * 3
         L.ref_morton_decode.argtypes = [C.c_uint64] + [C.POINTER(C.c_uint32)] * 3
@@ -201,6 +203,23 @@ class Reference(_Common):
 
     def ns(self, grid, cfg):
         return _NS(self.lib, "ref", grid, cfg)
+
+    def run_case(self, grid, cfg, run_dir, max_steps, stop_time=0.0, steady_tol=0.0, checkpoint_every=0,
+                 restart_from=None):
+        """The reference's runCase (core/src/flow/case.cpp:349-401): diagnostics.jsonl,
+        checkpoints and final.vtu in run_dir. Returns its RunSummary as a dict."""
+        out, steady = np.zeros(7), C.c_int()
+        rc = self.lib.ref_run_case(C.byref(grid.desc()), C.byref(cfg), str(run_dir).encode(), max_steps,
+                                   stop_time, steady_tol, checkpoint_every,
+                                   str(restart_from).encode() if restart_from else None, abi.dptr(out),
+                                   C.byref(steady))
+        if rc:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        keys = ("steps", "time", "momentum_residual", "continuity_residual", "mass_error", "cd", "cl")
+        d = dict(zip(keys, out.tolist()))
+        d["steps"] = int(d["steps"])
+        d["steady"] = bool(steady.value)
+        return d
 
     def morton_encode(self, x, y, z):
         return self.lib.ref_morton_encode(x, y, z)

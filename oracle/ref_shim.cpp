@@ -266,6 +266,31 @@ int ref_ns_read_checkpoint(void* h, const char* path) {
   SHIM_CATCH
 }
 
+// runCase (core/src/flow/case.cpp:349-401) with the given grid, flow config
+// and run options; summary = steps, time, momentum, continuity, mass, cd, cl.
+int ref_run_case(const nb_grid_desc* grid, const nb_flow_config* cfg, const char* run_dir, int max_steps,
+                 double stop_time, double steady_tol, int checkpoint_every, const char* restart_from,
+                 double* summary, int* steady) {
+  SHIM_TRY
+  flow::CaseSpec spec;
+  spec.grid = toGrid(grid);
+  spec.flow = toCfg(cfg);
+  spec.run.runDir = run_dir;
+  spec.run.maxSteps = max_steps;
+  spec.run.stopTime = stop_time;
+  spec.run.steadyTol = steady_tol;
+  spec.run.checkpointEvery = checkpoint_every;
+  spec.run.restartFrom = restart_from ? restart_from : "";
+  spec.run.quiet = true;
+  const flow::RunSummary s = flow::runCase(spec);
+  const double v[7] = {static_cast<double>(s.steps), s.time, s.momentumResidual, s.continuityResidual,
+                       s.massError, s.cd, s.cl};
+  for (int q = 0; q < 7; ++q) summary[q] = v[q];
+  *steady = s.steady ? 1 : 0;
+  return 0;
+  SHIM_CATCH
+}
+
 // ---- Poisson ----
 int ref_apply_a(const nb_grid_desc* grid, const double* x, double* out) {
   SHIM_TRY

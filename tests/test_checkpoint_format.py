@@ -50,3 +50,20 @@ def test_checkpoint_info_rejects_foreign_files(tmp_path):
     short.write_bytes(b"NBFCK01\0" + bytes(6))
     assert solver.checkpoint_info(short) is None
     assert solver.checkpoint_info(tmp_path / "missing.ckpt") is None
+
+
+def test_reference_run_directory(ref, tmp_path):
+    """The reference's runCase output that nb_run_case reproduces: a meta line,
+    one record per step with these keys in this order, checkpoint files."""
+    import json
+    grid, cfg = cases.channel(16, 8, 100.0)
+    s = ref.run_case(grid, cfg, tmp_path, 3, checkpoint_every=2)
+    assert s["steps"] == 3
+    lines = [json.loads(x) for x in (tmp_path / "diagnostics.jsonl").read_text().splitlines()]
+    assert list(lines[0]) == ["event", "solver", "solver_version", "git_sha"]
+    assert [r["step"] for r in lines[1:]] == [1, 2, 3]
+    assert list(lines[1]) == ["step", "t", "dt", "cfl", "momentum_residual", "continuity_residual",
+                              "divergence_max", "mass_error", "cd", "cl", "poisson_iters", "poisson_residual",
+                              "cells", "accepted"]
+    assert solver.checkpoint_info(tmp_path / "checkpoint_2.ckpt")["step"] == 2
+    assert solver.checkpoint_info(tmp_path / "final.ckpt")["step"] == 3
