@@ -157,6 +157,15 @@ nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, in
  * concurrently. One step in flight per case; not available while profiling. */
 nb_status nb_step_async(nb_case* c, double dt);
 nb_status nb_step_wait(nb_case* c, nb_step_report* rep);
+/* Replaces SolverBackend::sample (core/include/nabla/adaptive/run.hpp:17), as
+ * BaselineBackend implements it (core/src/adaptive/run.cpp:49-62), for n points
+ * at once: out[q] = component `component` (0 = u, 1 = v, 2 = w: the average of
+ * the two faces of the containing cell along that axis, NSSolver::cellU/V/W,
+ * ns_solver.cpp:677-688; 3 = the cell's pressure) at point (xyz[3q], xyz[3q+1],
+ * xyz[3q+2]). On octree cases the containing cell is the leaf cell. Cell
+ * indices are truncated toward zero and clamped into the domain. xyz and out
+ * are host arrays; one kernel launch for all points. */
+nb_status nb_case_sample(nb_case* c, int component, int64_t n, const double* xyz, double* out);
 /* Device bytes held by the case (admission control uses this). */
 uint64_t nb_case_device_bytes(const nb_case* c);
 /* Leaf cells of the case (Mcell-steps/s numerator). */

@@ -625,6 +625,43 @@ __global__ void __launch_bounds__(NT) k_amr_max_inv(AmrFlowView F, const double*
   });
 }
 
+// Cell-centred values at points on an octree: the leaf cell containing the
+// point (finest level first; indices truncated toward zero and clamped into
+// the domain), then the average of its two a-faces (NSSolver::cellU/V/W,
+// ns_solver.cpp:677-688, on that cell) or its pressure.
+__global__ void k_amr_sample(AmrFlowView F, int comp, long long n, const double* __restrict__ xyz,
+                             const double* __restrict__ u, const double* __restrict__ v,
+                             const double* __restrict__ w, const double* __restrict__ p, double* __restrict__ out) {
+  const LevelView& L = F.L;
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    int brick = -1, loc[3] = {0, 0, 0};
+    for (int lev = L.nlev - 1; lev >= 0 && brick < 0; --lev) {
+      int c[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int N = L.lcells[lev][a];
+        const double d = fmin(fmax((xyz[3 * q + a] - F.origin[a]) / F.h[lev][a], -1.0), static_cast<double>(N));
+        c[a] = min(max(static_cast<int>(d), 0), N - 1);
+      }
+      brick = lut_at(L, lev, c[0] >> 3, c[1] >> 3, c[2] >> 3);
+      for (int a = 0; a < 3; ++a) loc[a] = c[a] & 7;
+    }
+    double val = 0.0;
+    if (brick >= 0) {
+      const int l = (loc[2] << 6) | (loc[1] << 3) | loc[0];
+      const long long cell = brick * static_cast<long long>(BR3) + l;
+      if (comp < 3) {
+        const double* f = comp == 0 ? u : (comp == 1 ? v : w);
+        val = 0.5 * (f[cell] + hi_face(F, comp, f, brick, l, loc));
+      } else {
+        val = p[cell];
+      }
+    }
+    out[q] = val;
+  }
+}
+
 }  // namespace
 
 void amr_flow_setup() {
@@ -669,6 +706,14 @@ void launch_amr_diag(cudaStream_t s, const AmrFlowView& F, const double* u, cons
                      const double* w, const double* u0, const double* v0, const double* w0, RedBuf rb,
                      AmrStepScalars* out) {
   k_amr_diag<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, u0, v0, w0, rb, out);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_sample(cudaStream_t s, const AmrFlowView& F, int comp, long long n, const double* xyz,
+                       const double* u, const double* v, const double* w, const double* p, double* out) {
+  if (n <= 0) return;
+  const int grid = static_cast<int>(std::min<long long>((n + 255) / 256, 148 * 8));
+  k_amr_sample<<<grid, 256, 0, s>>>(F, comp, n, xyz, u, v, w, p, out);
   NB_CUDA(cudaGetLastError());
 }
 

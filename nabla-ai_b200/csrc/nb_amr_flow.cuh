@@ -41,6 +41,9 @@ void launch_amr_correct(cudaStream_t s, const AmrFlowView& F, const double* phi,
 void launch_amr_diag(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
                      const double* w, const double* u0, const double* v0, const double* w0, RedBuf rb,
                      AmrStepScalars* out);
+// out[q] = cell-centred component `comp` (3: pressure) of the leaf cell containing xyz[3q..3q+2].
+void launch_amr_sample(cudaStream_t s, const AmrFlowView& F, int comp, long long n, const double* xyz,
+                       const double* u, const double* v, const double* w, const double* p, double* out);
 void launch_amr_max_inv(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
                         const double* w, double cfl, double* dt_out, RedBuf rb, AmrStepScalars* out);
 

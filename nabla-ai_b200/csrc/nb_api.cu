@@ -1020,6 +1020,29 @@ nb_status nb_case_initialize(nb_case* c) {
   });
 }
 
+// Cell-centred values at host points (SolverBackend::sample): points and
+// results pass through the context's staging buffers.
+nb_status nb_case_sample(nb_case* c, int component, int64_t n, const double* xyz, double* out) {
+  if (!c || component < 0 || component > 3 || n < 0 || (n > 0 && (!xyz || !out))) return NB_ERR_BAD_ARG;
+  if (c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "nb_case_sample: the case has a step in flight");
+  if (n == 0) return NB_OK;
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    ensure_staging(c->ctx, static_cast<size_t>(n) * 3);
+    double* dxyz = c->ctx->stage_a;
+    double* dout = c->ctx->stage_b;
+    NB_CUDA(cudaMemcpyAsync(dxyz, xyz, static_cast<size_t>(n) * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    double** f = c->uvw[c->cur];
+    if (c->amr) launch_amr_sample(c->stream, c->AF, component, n, dxyz, f[0], f[1], f[2], c->p, dout);
+    else launch_sample(c->stream, c->F, component, n, dxyz, f[0], f[1], f[2], c->p, dout);
+    ++c->ctx->launches;
+    NB_CUDA(cudaMemcpyAsync(out, dout, static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NB_OK;
+  });
+}
+
 nb_status nb_case_compute_dt(nb_case* c, double* dt) {
   if (!c || !dt) return NB_ERR_BAD_ARG;
   return guarded(c->ctx, [&] {

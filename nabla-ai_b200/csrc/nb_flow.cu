@@ -494,6 +494,32 @@ __global__ void k_convert(FlowView F, int comp, int dir, const double* __restric
   }
 }
 
+// Cell-centred values at points (BaselineBackend::sample,
+// core/src/adaptive/run.cpp:49-62): the containing cell, indices truncated
+// toward zero and clamped into the grid, then NSSolver::cellU/V/W
+// (ns_solver.cpp:677-688) or the cell's pressure.
+__global__ void k_sample(FlowView F, int comp, long long n, const double* __restrict__ xyz,
+                         const double* __restrict__ u, const double* __restrict__ v,
+                         const double* __restrict__ w, const double* __restrict__ p, double* __restrict__ out) {
+  const LevelView& L = F.L;
+  const int dims[3] = {L.nx, L.ny, L.nz};
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double d = fmin(fmax((xyz[3 * q + a] - F.origin[a]) / L.dxyz[a], -1.0), static_cast<double>(dims[a]));
+      c[a] = min(max(static_cast<int>(d), 0), dims[a] - 1);
+    }
+    double val;
+    if (comp == 0) val = 0.5 * (u[uidx(F, c[0], c[1], c[2])] + u[uidx(F, c[0] + 1, c[1], c[2])]);
+    else if (comp == 1) val = 0.5 * (v[vidx(F, c[0], c[1], c[2])] + v[vidx(F, c[0], c[1] + 1, c[2])]);
+    else if (comp == 2) val = 0.5 * (w[widx(F, c[0], c[1], c[2])] + w[widx(F, c[0], c[1], c[2] + 1)]);
+    else val = p[cell_index(L, c[0], c[1], c[2])];
+    out[q] = val;
+  }
+}
+
 }  // namespace
 
 long long lex_size(const FlowView& F, int comp) {
@@ -559,6 +585,14 @@ void launch_diag(cudaStream_t s, const FlowView& F, const double* u, const doubl
                  const double* w, const double* u0, const double* v0, const double* w0,
                  const double* p, RedBuf rb, StepScalars* out) {
   k_diag<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, u0, v0, w0, p, rb, out);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_sample(cudaStream_t s, const FlowView& F, int comp, long long n, const double* xyz, const double* u,
+                   const double* v, const double* w, const double* p, double* out) {
+  if (n <= 0) return;
+  const int grid = static_cast<int>(std::min<long long>((n + 255) / 256, 148 * 8));
+  k_sample<<<grid, 256, 0, s>>>(F, comp, n, xyz, u, v, w, p, out);
   NB_CUDA(cudaGetLastError());
 }
 

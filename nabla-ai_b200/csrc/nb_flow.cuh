@@ -46,6 +46,9 @@ void launch_correct(cudaStream_t s, const FlowView& F, const double* phi, const 
 void launch_diag(cudaStream_t s, const FlowView& F, const double* u, const double* v,
                  const double* w, const double* u0, const double* v0, const double* w0,
                  const double* p, RedBuf rb, StepScalars* out);
+// out[q] = cell-centred component `comp` (3: pressure) at point xyz[3q..3q+2].
+void launch_sample(cudaStream_t s, const FlowView& F, int comp, long long n, const double* xyz, const double* u,
+                   const double* v, const double* w, const double* p, double* out);
 void launch_max_inv(cudaStream_t s, const FlowView& F, const double* u, const double* v,
                     const double* w, double visc, double cfl, double* dt_out, RedBuf rb,
                     StepScalars* out);

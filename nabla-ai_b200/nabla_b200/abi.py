@@ -194,6 +194,7 @@ PROTOTYPES = [
     ("nb_case_cell_count", C.c_uint64, [VP]),
     ("nb_case_stream", VP, [VP]),
     ("nb_ctx_profile", C.c_int, [VP, C.c_char_p]),
+    ("nb_case_sample", C.c_int, [VP, C.c_int, C.c_int64, DP, DP]),
     ("nb_run_case", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(FlowConfig), C.POINTER(RunOptions),
                               C.POINTER(RunSummary)]),
     ("nb_case_write_checkpoint", C.c_int, [VP, C.c_char_p]),

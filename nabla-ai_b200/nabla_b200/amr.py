@@ -156,6 +156,15 @@ class AmrCase:
             self.ctx.lib.nb_case_destroy(self.h)
             self.h = None
 
+    def sample(self, component: int, points) -> np.ndarray:
+        """SolverBackend::sample for many points: component 0-2 = cell-centred
+        velocity of the containing cell, 3 = its pressure (nb_case_sample)."""
+        pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros(pts.shape[0])
+        self.ctx.check(self.ctx.lib.nb_case_sample(self.h, component, pts.shape[0], abi.dptr(pts), abi.dptr(out)),
+                       "nb_case_sample")
+        return out
+
     def write_checkpoint(self, path):
         """Octree checkpoint (NBFAMR1): leaf list, step clock, u, v, w, p."""
         self.ctx.check(self.ctx.lib.nb_case_write_checkpoint(self.h, str(path).encode()), "write_checkpoint")

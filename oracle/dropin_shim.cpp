@@ -6,7 +6,11 @@
 //   mode 0  NSSolver + the reference's MgPoisson (CPU)
 //   mode 1  NSSolver + CudaMgPoisson (PoissonSolver seam, poisson.hpp:20-33)
 //   mode 2  CudaNSSolver (the whole step on the GPU, NSSolver's surface)
+// and the adaptive seam (SolverBackend, core/include/nabla/adaptive/run.hpp)
+// with CudaSolverBackend from nabla-ai_b200/integration/nabla_adaptive_cuda.hpp.
 // Built into oracle/_ref/libnabla_dropin.so; loaded only by tests/.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -16,6 +20,8 @@
 #include "nabla/flow/grid.hpp"
 #include "nabla/flow/ns_solver.hpp"
 #include "nabla/flow/poisson.hpp"
+#include "nabla/mesh/octree.hpp"
+#include "nabla_adaptive_cuda.hpp"
 #include "nabla_flow_cuda.hpp"
 
 using namespace nabla;
@@ -134,6 +140,72 @@ int dropin_poisson(const nb_grid_desc* grid, const double* b, double* x, double 
     *iters = r.iterations;
     *residual = r.residual;
     *converged = r.converged ? 1 : 0;
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// CudaSolverBackend after nsteps steps against the reference's NSSolver
+// stepped alike and read the way BaselineBackend::sample reads it
+// (core/src/adaptive/run.cpp:49-62). For each component c = 0..3 and point q:
+// one[c*n+q] = sample(), many[c*n+q] = sampleMany(), ref[c*n+q] = reference.
+// tele = backend t, dt, cfl, momentum residual, divergence max, poisson iters,
+// then the reference StepReport's same fields. tree_err = max |sampleFlowCuda -
+// per-cell sample()| over a uniformly refined reference Octree (3 levels).
+int dropin_backend(const nb_grid_desc* grid, const nb_flow_config* cfg, int nsteps, int64_t n, const double* xyz,
+                   double* one, double* many, double* ref, double* tele, double* tree_err) {
+  try {
+    const flow::UniformGrid g = grid_of(grid);
+    const flow::FlowConfig c = config_of(cfg);
+    adaptive::CudaSolverBackend be(context(), g, c);
+    flow::NSSolver ns(g, c, std::make_shared<flow::MgPoisson>(c.poissonTol, c.poissonMaxIters));
+    ns.initialize();
+    flow::StepReport last;
+    for (int s = 0; s < nsteps; ++s) {
+      be.step();
+      last = ns.step();
+    }
+    std::vector<adaptive::Vec3> pts(static_cast<size_t>(n));
+    for (int64_t q = 0; q < n; ++q) pts[q] = {xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]};
+    const std::vector<double> pc = ns.cellPressure();
+    for (int comp = 0; comp < 4; ++comp) {
+      std::vector<double> m;
+      be.sampleMany(comp, pts, m);
+      for (int64_t q = 0; q < n; ++q) {
+        one[comp * n + q] = be.sample(comp, pts[q]);
+        many[comp * n + q] = m[q];
+        int i = static_cast<int>((pts[q].x - g.origin.x) / g.dx);
+        int j = static_cast<int>((pts[q].y - g.origin.y) / g.dy);
+        int k = static_cast<int>((pts[q].z - g.origin.z) / g.dz);
+        i = std::clamp(i, 0, g.nx - 1);
+        j = std::clamp(j, 0, g.ny - 1);
+        k = std::clamp(k, 0, g.nz - 1);
+        ref[comp * n + q] = comp == 0   ? ns.cellU(i, j, k)
+                            : comp == 1 ? ns.cellV(i, j, k)
+                            : comp == 2 ? ns.cellW(i, j, k)
+                                        : pc[g.cidx(i, j, k)];
+      }
+    }
+    const double mine[6] = {be.t(), be.dt(), be.cfl(), be.momentumResidual(), be.divergenceMax(),
+                            static_cast<double>(be.poissonIters())};
+    const double theirs[6] = {last.t, last.dt, last.cfl, last.momentumResidual, last.divergenceMax,
+                              static_cast<double>(last.poissonIters)};
+    for (int q = 0; q < 6; ++q) {
+      tele[q] = mine[q];
+      tele[6 + q] = theirs[q];
+    }
+    mesh::Octree tree({g.origin.x, g.origin.y, g.origin.z}, {g.nx * g.dx, g.ny * g.dy, g.nz * g.dz}, 6);
+    tree.refineUniform(3);
+    adaptive::sampleFlowCuda(tree, be);
+    double err = 0.0;
+    for (std::size_t i = 0; i < tree.cellCount(); ++i) {
+      const adaptive::Vec3 ctr = tree.cellCenter(i);
+      const double got[4] = {tree.u()[i], tree.v()[i], tree.w()[i], tree.p()[i]};
+      for (int comp = 0; comp < 4; ++comp) err = std::max(err, std::abs(got[comp] - be.sample(comp, ctr)));
+    }
+    *tree_err = err;
     return 0;
   } catch (const std::exception& e) {
     g_err = e.what();

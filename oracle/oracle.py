@@ -376,6 +376,22 @@ class Dropin:
             raise RuntimeError(self.lib.dropin_last_error().decode())
         return out, list(iters), dts
 
+    def backend(self, grid, cfg, nsteps, points):
+        """CudaSolverBackend (the SolverBackend seam) against the reference's NSSolver read as
+        BaselineBackend reads it: (sample(), sampleMany(), reference) as [4, n] arrays, the
+        telemetry (t, dt, cfl, momentum residual, divergence max, poisson iters) of both, and the
+        largest difference of sampleFlowCuda from per-cell sample() on a refined reference Octree."""
+        pts = np.ascontiguousarray(np.asarray(points, dtype=np.float64).reshape(-1, 3))
+        n = pts.shape[0]
+        one, many, ref, tele, err = np.zeros(4 * n), np.zeros(4 * n), np.zeros(4 * n), np.zeros(12), C.c_double()
+        L = self.lib
+        L.dropin_backend.argtypes = [GP, FP, C.c_int, C.c_int64, DP, DP, DP, DP, DP, C.POINTER(C.c_double)]
+        st = L.dropin_backend(C.byref(grid.desc()), C.byref(cfg), nsteps, n, abi.dptr(pts), abi.dptr(one),
+                              abi.dptr(many), abi.dptr(ref), abi.dptr(tele), C.byref(err))
+        if st != 0:
+            raise RuntimeError(L.dropin_last_error().decode())
+        return one.reshape(4, n), many.reshape(4, n), ref.reshape(4, n), tele[:6], tele[6:], err.value
+
     def poisson(self, grid, b, tol, max_cycles, mode):
         gd = grid.desc()
         b = np.ascontiguousarray(b, dtype=np.float64)
