@@ -304,6 +304,28 @@ nb_status nb_amr_poisson_solve(nb_ctx* ctx, nb_amr_mesh* m, const double* b, dou
  * (overwritten on every update). Pressure: nbrick*512 cell values. */
 nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* m, const nb_flow_config* cfg, int precision,
                              nb_case** out);
+/* Merges each complete octet of sibling leaves whose eight members are all
+ * flagged into its parent (Octree::coarsen, core/src/mesh/octree.cpp:393-473,
+ * at brick granularity: all eight children must be leaves, and the merge is
+ * refused where the parent would sit next to a leaf two levels finer, here over
+ * all 26 neighbours with periodic wrap since these meshes are balanced across
+ * edges and corners too). Same output convention as nb_amr_refine. */
+nb_status nb_amr_coarsen(const nb_amr_geom* g, const int32_t* leaves, int64_t n, const uint8_t* flags,
+                         int32_t* out, int64_t cap, int64_t* n_out);
+/* Per-leaf refinement sensors of an octree case, the velocity-gradient
+ * sensors of PhysicalSensorEvaluator::evaluate (core/src/adaptive/
+ * adaptive_core.cpp:96-113) on brick cells: out[4 r + 0..3] = the maximum over
+ * leaf r's fluid cells of |vorticity|, sqrt(2 S:S), Q and |grad p| (cell-centred
+ * values, central differences inside the brick, one-sided on its faces). */
+nb_status nb_amr_case_sensors(nb_case* c, double* out);
+/* Regrid transfer: dst (a fresh case on a mesh from nb_amr_refine or
+ * nb_amr_coarsen of src's mesh: same geometry, at most one level apart at every
+ * leaf) takes src's state and step clock. Every face dst stores takes src's
+ * value at that face: the same face, the average of four finer sub-faces, or
+ * the coarse face (or, mid-cell, the mean of the coarse cell's two normal
+ * faces), so a divergence-free field stays divergence-free; pressure is copied,
+ * injected from the coarser cell or averaged over the eight finer cells. */
+nb_status nb_amr_case_transfer(nb_case* dst, nb_case* src);
 /* sizes[0..2] = face storage lengths of u, v, w; sizes[3] = cells. */
 nb_status nb_amr_case_sizes(const nb_case* c, int64_t sizes[4]);
 /* Leaf rank of every a-slab, in slab order ((sizes[a] - cells) / 64 values). */

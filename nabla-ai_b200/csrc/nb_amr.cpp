@@ -1,9 +1,12 @@
 // nb_amr.cpp — octree brick trees: refinement, 26-neighbour 2:1 balance,
-// Morton ranking, per-level lookup tables, composite coarsening.
+// Morton ranking, per-level lookup tables, composite coarsening, and the
+// merging of flagged sibling octets for regridding.
 #include "nb_amr.h"
 
 #include <algorithm>
 #include <array>
+#include <map>
+#include <set>
 #include <string>
 
 #include "nb_morton.h"
@@ -218,6 +221,58 @@ std::vector<AmrLeaf> refine_leaves(const AmrGeom& g, const std::vector<AmrLeaf>&
   }
   S.balance();
   return finish(g, S).leaves;
+}
+
+std::vector<AmrLeaf> coarsen_leaves(const AmrGeom& g, const std::vector<AmrLeaf>& leaves,
+                                    const std::vector<uint8_t>& flags, std::string& err) {
+  AmrTree t = tree_from_leaves(g, leaves, err);
+  if (!err.empty()) return {};
+  // parents whose eight children are all flagged leaves
+  std::map<std::array<int, 4>, int> flagged;  // (level, bx, by, bz) of the parent -> flagged children
+  for (size_t q = 0; q < leaves.size(); ++q) {
+    const AmrLeaf& f = leaves[q];
+    if (!flags[q] || f.level == 0) continue;
+    ++flagged[{f.level - 1, f.b[0] >> 1, f.b[1] >> 1, f.b[2] >> 1}];
+  }
+  std::set<std::array<int, 4>> merge;
+  for (const auto& [P, n] : flagged) {
+    if (n != 8) continue;
+    const int Lp = P[0];
+    // a leaf two levels finer than the parent inside any neighbour region blocks the merge
+    bool ok = true;
+    for (int d = 0; d < 27 && ok; ++d) {
+      if (d == 13) continue;
+      int c[3] = {P[1] + d % 3 - 1, P[2] + (d / 3) % 3 - 1, P[3] + d / 9 - 1};
+      bool inside = true;
+      for (int a = 0; a < 3; ++a) {
+        const int nb = t.lnb(Lp, a);
+        if (c[a] < 0 || c[a] >= nb) {
+          if (g.bc[2 * a] == NB_BC_PERIODIC) c[a] = (c[a] + nb) % nb;
+          else inside = false;
+        }
+      }
+      if (!inside || Lp + 2 >= t.nlev) continue;
+      for (int z = 0; z < 4 && ok; ++z)
+        for (int y = 0; y < 4 && ok; ++y)
+          for (int x = 0; x < 4 && ok; ++x)
+            if (t.find(Lp + 2, 4 * c[0] + x, 4 * c[1] + y, 4 * c[2] + z) >= 0) ok = false;
+    }
+    if (ok) merge.insert(P);
+  }
+  std::vector<AmrLeaf> out;
+  out.reserve(leaves.size());
+  for (const AmrLeaf& f : t.leaves) {
+    if (f.level > 0 && merge.count({f.level - 1, f.b[0] >> 1, f.b[1] >> 1, f.b[2] >> 1})) continue;
+    out.push_back(f);
+  }
+  for (const auto& P : merge) out.push_back(AmrLeaf{P[0], {P[1], P[2], P[3]}});
+  AmrTree check = tree_from_leaves(g, out, err);
+  if (!err.empty()) return {};
+  if (!tree_balanced(check)) {
+    err = "coarsening broke the 2:1 balance";
+    return {};
+  }
+  return check.leaves;
 }
 
 bool tree_balanced(const AmrTree& t) {

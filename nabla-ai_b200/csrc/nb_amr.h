@@ -60,6 +60,12 @@ AmrTree tree_from_leaves(const AmrGeom& g, const std::vector<AmrLeaf>& leaves, s
 AmrTree coarsen_tree(const AmrTree& t, std::vector<int>& xf_brick, std::vector<int>& xf_oct);
 bool tree_balanced(const AmrTree& t);
 // Splits leaves[q] where flags[q] != 0 (below lmax), then restores balance.
+// Merges every complete octet of sibling leaves whose eight members are all
+// flagged into their parent, except where the parent would touch (26
+// neighbours, periodic wrap) a leaf two levels finer than itself. The result
+// is balanced whenever the input is.
+std::vector<AmrLeaf> coarsen_leaves(const AmrGeom& g, const std::vector<AmrLeaf>& leaves,
+                                    const std::vector<uint8_t>& flags, std::string& err);
 std::vector<AmrLeaf> refine_leaves(const AmrGeom& g, const std::vector<AmrLeaf>& leaves,
                                    const std::vector<uint8_t>& flags, std::string& err);
 

@@ -84,6 +84,27 @@ nb_status nb_amr_refine(const nb_amr_geom* g, const int32_t* leaves, int64_t n, 
   }
 }
 
+nb_status nb_amr_coarsen(const nb_amr_geom* g, const int32_t* leaves, int64_t n, const uint8_t* flags,
+                         int32_t* out, int64_t cap, int64_t* n_out) {
+  std::string why;
+  if (!geom_ok(g, why) || !leaves || n <= 0 || !flags || !n_out) return NB_ERR_BAD_ARG;
+  try {
+    std::string err;
+    const std::vector<uint8_t> fl(flags, flags + n);
+    const std::vector<AmrLeaf> res = coarsen_leaves(to_geom(*g), to_leaves(leaves, n), fl, err);
+    if (!err.empty()) return NB_ERR_BAD_ARG;
+    *n_out = static_cast<int64_t>(res.size());
+    if (!out || cap < static_cast<int64_t>(res.size())) return NB_ERR_BAD_ARG;
+    for (size_t q = 0; q < res.size(); ++q) {
+      out[4 * q] = res[q].level;
+      for (int a = 0; a < 3; ++a) out[4 * q + 1 + a] = res[q].b[a];
+    }
+    return NB_OK;
+  } catch (const std::exception&) {
+    return NB_ERR_BAD_ARG;
+  }
+}
+
 nb_status nb_amr_mesh_create(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* leaves, int64_t n,
                              const uint8_t* solid, nb_amr_mesh** out) {
   if (!ctx || !out || !leaves || n <= 0) return NB_ERR_BAD_ARG;

@@ -662,6 +662,126 @@ __global__ void k_amr_sample(AmrFlowView F, int comp, long long n, const double*
   }
 }
 
+// Per-brick refinement sensors, the velocity-gradient sensors of
+// PhysicalSensorEvaluator::evaluate (core/src/adaptive/adaptive_core.cpp:
+// 96-113) on brick cells: cell-centred u, v, w, p; gradients by central
+// differences inside the brick (one-sided on its faces); per brick the
+// maximum over fluid cells of |omega|, sqrt(2 S:S), Q = (O:O - S:S)/2 and
+// |grad p| (0 for a brick without fluid cells).
+__global__ void __launch_bounds__(NT) k_amr_sensors(AmrFlowView F, const double* __restrict__ u,
+                                                    const double* __restrict__ v, const double* __restrict__ w,
+                                                    const double* __restrict__ p, double* __restrict__ out) {
+  __shared__ double cv[4][BR3];
+  __shared__ double sh[4 * 32];
+  const LevelView& L = F.L;
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int lev = L.blevel[brick];
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      const long long c = brick * static_cast<long long>(BR3) + l;
+      cv[0][l] = 0.5 * (u[c] + hi_face(F, 0, u, brick, l, loc));
+      cv[1][l] = 0.5 * (v[c] + hi_face(F, 1, v, brick, l, loc));
+      cv[2][l] = 0.5 * (w[c] + hi_face(F, 2, w, brick, l, loc));
+      cv[3][l] = p[c];
+    }
+    __syncthreads();
+    double best[4] = {-1.0e308, -1.0e308, -1.0e308, -1.0e308};
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      if (L.type[brick * static_cast<long long>(BR3) + l] != CELL_FLUID) continue;
+      const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
+      double g[4][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const int st = d == 0 ? 1 : (d == 1 ? 8 : 64);
+        const double h = F.h[lev][d];
+        const int lo = loc[d] == 0 ? l : l - st, hi = loc[d] == 7 ? l : l + st;
+        const double span = (loc[d] == 0 || loc[d] == 7) ? h : 2.0 * h;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) g[f][d] = (cv[f][hi] - cv[f][lo]) / span;
+      }
+      const double* du = g[0];
+      const double* dv = g[1];
+      const double* dw = g[2];
+      const double ox = dw[1] - dv[2], oy = du[2] - dw[0], oz = dv[0] - du[1];
+      const double vort = sqrt(ox * ox + oy * oy + oz * oz);
+      const double sxy = 0.5 * (du[1] + dv[0]), sxz = 0.5 * (du[2] + dw[0]), syz = 0.5 * (dv[2] + dw[1]);
+      const double ss = du[0] * du[0] + dv[1] * dv[1] + dw[2] * dw[2] + 2 * (sxy * sxy + sxz * sxz + syz * syz);
+      const double axy = 0.5 * (du[1] - dv[0]), axz = 0.5 * (du[2] - dw[0]), ayz = 0.5 * (dv[2] - dw[1]);
+      const double oo = 2 * (axy * axy + axz * axz + ayz * ayz);
+      const double gp = sqrt(g[3][0] * g[3][0] + g[3][1] * g[3][1] + g[3][2] * g[3][2]);
+      const double val[4] = {vort, sqrt(2.0 * ss), 0.5 * (oo - ss), gp};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) best[k] = fmax(best[k], val[k]);
+    }
+    block_reduce<4, 0xFu>(best, sh);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 4; ++k) out[4LL * brick + k] = best[k] < -1.0e300 ? 0.0 : best[k];
+    __syncthreads();
+  }
+}
+
+// State transfer between two meshes of one geometry whose levels differ by
+// at most one everywhere (one regrid pass). Every face the destination stores
+// takes the source's value at that face through the level-aware face rule
+// (same level: the face; finer source: the average of its four sub-faces;
+// coarser source: the coarse face, or the midpoint of the coarse cell's two
+// normal faces), which keeps a discretely divergence-free field free of
+// divergence; cells take the same-level value, the coarser cell's value, or
+// the mean of their eight finer cells.
+__global__ void k_amr_transfer_faces(AmrFlowView D, AmrFlowView S, int a, const int* __restrict__ dslab_brick,
+                                     long long nslot, const double* __restrict__ fsrc, double* __restrict__ fdst) {
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < nslot;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    int brick, loc[3];
+    if (q < D.nb) {
+      brick = static_cast<int>(q >> 9);
+      const int l = static_cast<int>(q & 511);
+      loc[0] = l & 7;
+      loc[1] = (l >> 3) & 7;
+      loc[2] = l >> 6;
+    } else {  // high slab face: the inverse of slab_local
+      const long long r = q - D.nb;
+      const int m = static_cast<int>(r & 63);
+      brick = dslab_brick[r >> 6];
+      loc[a] = 8;
+      loc[a == 0 ? 1 : 0] = m & 7;
+      loc[a == 2 ? 1 : 2] = m >> 3;
+    }
+    const int lev = D.L.blevel[brick];
+    const int pos[3] = {D.L.bcoord[3 * brick] * BR + loc[0], D.L.bcoord[3 * brick + 1] * BR + loc[1],
+                        D.L.bcoord[3 * brick + 2] * BR + loc[2]};
+    fdst[q] = face_read(S, a, fsrc, lev, pos);
+  }
+}
+
+__global__ void k_amr_transfer_cells(AmrFlowView D, AmrFlowView S, const double* __restrict__ psrc,
+                                     double* __restrict__ pdst) {
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < D.nb;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int brick = static_cast<int>(q >> 9), l = static_cast<int>(q & 511);
+    const int lev = D.L.blevel[brick];
+    const int pos[3] = {D.L.bcoord[3 * brick] * BR + (l & 7), D.L.bcoord[3 * brick + 1] * BR + ((l >> 3) & 7),
+                        D.L.bcoord[3 * brick + 2] * BR + (l >> 6)};
+    int ls = -1;
+    const int r = leaf_of(S.L, lev, pos, ls);
+    double val = 0.0;
+    if (r >= 0 && ls == lev) {
+      val = psrc[r * static_cast<long long>(BR3) + local_of(pos)];
+    } else if (r >= 0 && ls == lev - 1) {
+      const int cp[3] = {pos[0] >> 1, pos[1] >> 1, pos[2] >> 1};
+      val = psrc[r * static_cast<long long>(BR3) + local_of(cp)];
+    } else if (r >= 0 && ls == lev + 1) {
+      double sum = 0.0;
+      for (int d = 0; d < 8; ++d) {
+        const int ch[3] = {2 * pos[0] + (d & 1), 2 * pos[1] + ((d >> 1) & 1), 2 * pos[2] + (d >> 2)};
+        sum += psrc[r * static_cast<long long>(BR3) + local_of(ch)];
+      }
+      val = 0.125 * sum;
+    }
+    pdst[q] = val;
+  }
+}
+
 }  // namespace
 
 void amr_flow_setup() {
@@ -714,6 +834,25 @@ void launch_amr_sample(cudaStream_t s, const AmrFlowView& F, int comp, long long
   if (n <= 0) return;
   const int grid = static_cast<int>(std::min<long long>((n + 255) / 256, 148 * 8));
   k_amr_sample<<<grid, 256, 0, s>>>(F, comp, n, xyz, u, v, w, p, out);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_sensors(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v, const double* w,
+                        const double* p, double* out) {
+  k_amr_sensors<<<grid_for(F.L.nbrick), NT, 0, s>>>(F, u, v, w, p, out);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_amr_transfer(cudaStream_t s, const AmrFlowView& D, const AmrFlowView& S, const int* const dslab[3],
+                         const long long nstore[3], const double* const fsrc[3], double* const fdst[3],
+                         const double* psrc, double* pdst) {
+  for (int a = 0; a < 3; ++a) {
+    const int grid = static_cast<int>(std::min<long long>((nstore[a] + 255) / 256, 148 * 8));
+    k_amr_transfer_faces<<<grid, 256, 0, s>>>(D, S, a, dslab[a], nstore[a], fsrc[a], fdst[a]);
+    NB_CUDA(cudaGetLastError());
+  }
+  const int grid = static_cast<int>(std::min<long long>((D.nb + 255) / 256, 148 * 8));
+  k_amr_transfer_cells<<<grid, 256, 0, s>>>(D, S, psrc, pdst);
   NB_CUDA(cudaGetLastError());
 }
 

@@ -44,6 +44,13 @@ void launch_amr_diag(cudaStream_t s, const AmrFlowView& F, const double* u, cons
 // out[q] = cell-centred component `comp` (3: pressure) of the leaf cell containing xyz[3q..3q+2].
 void launch_amr_sample(cudaStream_t s, const AmrFlowView& F, int comp, long long n, const double* xyz,
                        const double* u, const double* v, const double* w, const double* p, double* out);
+// out[4 b .. 4 b + 3] = max |omega|, sqrt(2 S:S), Q, |grad p| over brick b's fluid cells.
+void launch_amr_sensors(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v, const double* w,
+                        const double* p, double* out);
+// Conservative state transfer from the mesh of view S to the mesh of view D.
+void launch_amr_transfer(cudaStream_t s, const AmrFlowView& D, const AmrFlowView& S, const int* const dslab[3],
+                         const long long nstore[3], const double* const fsrc[3], double* const fdst[3],
+                         const double* psrc, double* pdst);
 void launch_amr_max_inv(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v,
                         const double* w, double cfl, double* dt_out, RedBuf rb, AmrStepScalars* out);
 

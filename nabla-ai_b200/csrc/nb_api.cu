@@ -1020,6 +1020,85 @@ nb_status nb_case_initialize(nb_case* c) {
   });
 }
 
+// Per-brick refinement sensors of an octree case (host array nleaf x 4).
+nb_status nb_amr_case_sensors(nb_case* c, double* out) {
+  if (!c || !c->amr || !out) return NB_ERR_BAD_ARG;
+  if (c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "nb_amr_case_sensors: the case has a step in flight");
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    const size_t n = static_cast<size_t>(c->fm.nbrick) * 4;
+    ensure_staging(c->ctx, n);
+    double** f = c->uvw[c->cur];
+    launch_amr_sensors(c->stream, c->AF, f[0], f[1], f[2], c->p, c->ctx->stage_a);
+    ++c->ctx->launches;
+    NB_CUDA(cudaMemcpyAsync(out, c->ctx->stage_a, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NB_OK;
+  });
+}
+
+namespace {
+bool same_geometry(const nb_amr_geom& a, const nb_amr_geom& b) {
+  for (int q = 0; q < 3; ++q)
+    if (a.nb0[q] != b.nb0[q] || a.h0[q] != b.h0[q] || a.origin[q] != b.origin[q]) return false;
+  for (int f = 0; f < 6; ++f)
+    if (a.face[f].type != b.face[f].type) return false;
+  return a.lmax == b.lmax;
+}
+}  // namespace
+
+// Conservative state transfer onto dst's mesh from src (meshes of one
+// geometry, at most one level apart at every destination leaf).
+nb_status nb_amr_case_transfer(nb_case* dst, nb_case* src) {
+  if (!dst || !src || !dst->amr || !src->amr || dst->ctx != src->ctx) return NB_ERR_BAD_ARG;
+  nb_ctx* ctx = dst->ctx;
+  if (dst->pending || src->pending) return fail(ctx, NB_ERR_BAD_ARG, "nb_amr_case_transfer: a step is in flight");
+  if (!same_geometry(dst->mesh->geom, src->mesh->geom))
+    return fail(ctx, NB_ERR_BAD_ARG, "nb_amr_case_transfer: the meshes have different geometries");
+  const AmrTree& ts = src->mesh->lvl.tree;
+  // leaf of the source at (level, brick), with the level bounded to the source's levels
+  auto has = [&](int L, int x, int y, int z) { return L >= 0 && L < ts.nlev && ts.find(L, x, y, z) >= 0; };
+  for (const AmrLeaf& f : dst->mesh->lvl.tree.leaves) {
+    bool ok = has(f.level, f.b[0], f.b[1], f.b[2]) || has(f.level - 1, f.b[0] >> 1, f.b[1] >> 1, f.b[2] >> 1);
+    if (!ok) {
+      ok = true;
+      for (int d = 0; d < 8 && ok; ++d)
+        ok = has(f.level + 1, 2 * f.b[0] + (d & 1), 2 * f.b[1] + ((d >> 1) & 1), 2 * f.b[2] + (d >> 2));
+    }
+    if (!ok) return fail(ctx, NB_ERR_BAD_ARG, "nb_amr_case_transfer: the meshes differ by more than one level");
+  }
+  std::vector<void*> tmp;
+  const nb_status st = guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    NB_CUDA(cudaStreamSynchronize(src->stream));
+    const int* dslab[3];
+    long long nstore[3];
+    const double* fsrc[3];
+    double* fdst[3];
+    for (int a = 0; a < 3; ++a) {
+      const std::vector<int>& sb = dst->fm.slab_brick[a];
+      void* d = nullptr;
+      NB_CUDA(cudaMalloc(&d, std::max<size_t>(1, sb.size()) * sizeof(int)));
+      tmp.push_back(d);
+      if (!sb.empty()) NB_CUDA(cudaMemcpy(d, sb.data(), sb.size() * sizeof(int), cudaMemcpyHostToDevice));
+      dslab[a] = static_cast<const int*>(d);
+      nstore[a] = dst->fm.store[a];
+      fsrc[a] = src->uvw[src->cur][a];
+      fdst[a] = dst->uvw[dst->cur][a];
+    }
+    launch_amr_transfer(dst->stream, dst->AF, src->AF, dslab, nstore, fsrc, fdst, src->p, dst->p);
+    ctx->launches += 4;
+    amr_sync(*dst, dst->uvw[dst->cur]);
+    NB_CUDA(cudaStreamSynchronize(dst->stream));
+    dst->step = src->step;
+    dst->t = src->t;
+    dst->dt_last = src->dt_last;
+    return NB_OK;
+  });
+  for (void* d : tmp) cudaFree(d);
+  return st;
+}
+
 // Cell-centred values at host points (SolverBackend::sample): points and
 // results pass through the context's staging buffers.
 nb_status nb_case_sample(nb_case* c, int component, int64_t n, const double* xyz, double* out) {
@@ -1217,8 +1296,12 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     V.nx = t.cells(0, 0);
     V.ny = t.cells(0, 1);
     V.nz = t.cells(0, 2);
-    for (int L = 0; L < t.nlev && L < AMR_MAXLEV; ++L) {
-      V.lut_off[L] = t.lut_off[L];
+    // Level sizes up to the geometry's finest level (a state transfer reads
+    // this view at the levels of a mesh one level finer); LUTs only for the
+    // levels present.
+    const int ltab = std::min(g.lmax + 1, AMR_MAXLEV);
+    for (int L = 0; L < ltab; ++L) {
+      if (L < t.nlev) V.lut_off[L] = t.lut_off[L];
       for (int a = 0; a < 3; ++a) {
         V.lnb[L][a] = t.lnb(L, a);
         V.lcells[L][a] = t.cells(L, a);
@@ -1231,7 +1314,7 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     V.type = static_cast<const uint8_t*>(up(lv.type.data(), lv.type.size()));
     V.blevel = static_cast<const int8_t*>(up(lv.blevel.data(), lv.blevel.size()));
     for (int a = 0; a < 3; ++a) F.origin[a] = g.origin[a];
-    for (int L = 0; L < t.nlev && L < AMR_MAXLEV; ++L)
+    for (int L = 0; L < ltab; ++L)
       for (int a = 0; a < 3; ++a) F.h[L][a] = t.h(L, a);
     for (int f = 0; f < 6; ++f) {
       for (int a = 0; a < 3; ++a) F.wallv[f][a] = g.face[f].wall_velocity[a];

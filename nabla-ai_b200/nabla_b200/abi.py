@@ -195,6 +195,10 @@ PROTOTYPES = [
     ("nb_case_stream", VP, [VP]),
     ("nb_ctx_profile", C.c_int, [VP, C.c_char_p]),
     ("nb_case_sample", C.c_int, [VP, C.c_int, C.c_int64, DP, DP]),
+    ("nb_amr_case_sensors", C.c_int, [VP, DP]),
+    ("nb_amr_case_transfer", C.c_int, [VP, VP]),
+    ("nb_amr_coarsen", C.c_int, [C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_uint8),
+                                 C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
     ("nb_run_case", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(FlowConfig), C.POINTER(RunOptions),
                               C.POINTER(RunSummary)]),
     ("nb_case_write_checkpoint", C.c_int, [VP, C.c_char_p]),

@@ -58,6 +58,23 @@ def refine(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray) -> np.ndarr
         raise NablaError(st, "nb_amr_refine failed")
 
 
+def coarsen(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray) -> np.ndarray:
+    """Merge complete flagged sibling octets into their parents where the 2:1
+    balance allows (nb_amr_coarsen)."""
+    lib = abi.load()
+    leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+    flags = np.ascontiguousarray(flags, dtype=np.uint8)
+    n = leaves.shape[0]
+    need = C.c_int64()
+    out = np.zeros((n, 4), dtype=np.int32)
+    st = lib.nb_amr_coarsen(C.byref(geom), leaves.ctypes.data_as(C.POINTER(C.c_int32)), n,
+                            flags.ctypes.data_as(C.POINTER(C.c_uint8)), out.ctypes.data_as(C.POINTER(C.c_int32)),
+                            n, C.byref(need))
+    if st != abi.NB_OK:
+        raise ValueError("nb_amr_coarsen rejected the leaf list")
+    return out[:need.value].copy()
+
+
 def cell_coords(leaves: np.ndarray):
     """(level, i, j, k) of every cell, leaves x 512, in array order."""
     l = np.arange(512)
@@ -134,7 +151,7 @@ class AmrCase:
     ``face_positions``)."""
 
     def __init__(self, mesh: AmrMesh, config: abi.FlowConfig, precision: int = abi.PRECISION_FP64):
-        self.mesh, self.ctx, self.config = mesh, mesh.ctx, config
+        self.mesh, self.ctx, self.config, self.precision = mesh, mesh.ctx, config, precision
         h = C.c_void_p()
         self.ctx.check(self.ctx.lib.nb_amr_case_create(self.ctx.h, mesh.h, C.byref(config), precision,
                                                        C.byref(h)), "nb_amr_case_create")
@@ -164,6 +181,16 @@ class AmrCase:
         self.ctx.check(self.ctx.lib.nb_case_sample(self.h, component, pts.shape[0], abi.dptr(pts), abi.dptr(out)),
                        "nb_case_sample")
         return out
+
+    def sensors(self) -> np.ndarray:
+        """Per-leaf max |vorticity|, strain magnitude, Q, |grad p| (nb_amr_case_sensors), shape (nleaf, 4)."""
+        out = np.zeros((self.mesh.leaves.shape[0], 4))
+        self.ctx.check(self.ctx.lib.nb_amr_case_sensors(self.h, abi.dptr(out)), "nb_amr_case_sensors")
+        return out
+
+    def transfer_from(self, src: "AmrCase"):
+        """Take src's state and clock across a regrid (nb_amr_case_transfer)."""
+        self.ctx.check(self.ctx.lib.nb_amr_case_transfer(self.h, src.h), "nb_amr_case_transfer")
 
     def write_checkpoint(self, path):
         """Octree checkpoint (NBFAMR1): leaf list, step clock, u, v, w, p."""
@@ -237,3 +264,26 @@ class AmrCase:
     @property
     def cell_count(self) -> int:
         return self.ctx.lib.nb_case_cell_count(self.h)
+
+
+def regrid(case: AmrCase, refine_above: float, coarsen_below: float, sensor: int = 0, solid_fn=None) -> AmrCase:
+    """One regrid pass on the device sensors: leaves whose sensor `sensor`
+    (0 |vorticity|, 1 strain, 2 Q, 3 |grad p|) exceeds refine_above are split
+    (2:1 balance restored), then complete octets of untouched leaves below
+    coarsen_below are merged; a new case on the new mesh takes the state
+    conservatively. solid_fn(leaves) -> per-cell solid flags (leaves x 512, in
+    leaf order) or None. Returns the new case (the old one is left as it was)."""
+    mesh = case.mesh
+    geom, leaves = mesh.geom, mesh.leaves
+    s = case.sensors()[:, sensor]
+    refined = refine(geom, leaves, (s > refine_above) & (leaves[:, 0] < geom.lmax))
+    # leaves the refinement left alone keep their sensor value; new ones are not coarsened
+    old = {tuple(l): v for l, v in zip(map(tuple, leaves), s)}
+    flags = np.array([old.get(tuple(l), np.inf) < coarsen_below for l in refined], dtype=np.uint8)
+    new_leaves = coarsen(geom, refined, flags)
+    solid = solid_fn(new_leaves) if solid_fn else None
+    new_mesh = AmrMesh(geom, new_leaves, solid=solid, ctx=case.ctx)
+    new = AmrCase(new_mesh, case.config, precision=case.precision)
+    new.transfer_from(case)
+    new._mesh_keepalive = new_mesh
+    return new

@@ -1,10 +1,11 @@
 """Host-side octree brick maps (integer work, CPU): refinement, 26-neighbour
 2:1 balance (the balance rule of Octree::refineByMorton,
-core/src/mesh/octree.cpp:325-356, at brick granularity), coverage and
-deterministic Morton ranking."""
+core/src/mesh/octree.cpp:325-356, at brick granularity), coverage,
+deterministic Morton ranking, and the merging of sibling octets
+(Octree::coarsen, core/src/mesh/octree.cpp:393-473)."""
 import numpy as np
 
-from amr_helpers import check_balanced, closed_box_geom, three_level_leaves, two_level_leaves
+from amr_helpers import check_balanced, closed_box_geom, refine_where, three_level_leaves, two_level_leaves
 from nabla_b200 import abi, amr
 
 
@@ -63,3 +64,45 @@ def test_refine_rejects_bad_leaf_sets():
     from nabla_b200.solver import NablaError
     with pytest.raises(NablaError):
         amr.refine(g, lv, np.zeros(len(lv), dtype=np.uint8))
+
+
+def _as_set(leaves):
+    return {tuple(int(v) for v in lf) for lf in leaves}
+
+
+def test_coarsen_undoes_a_uniform_refinement():
+    geom = closed_box_geom()
+    base = amr.base_leaves(list(geom.nb0))
+    fine = amr.refine(geom, base, np.ones(len(base), dtype=np.uint8))
+    assert len(fine) == 64
+    back = amr.coarsen(geom, fine, np.ones(len(fine), dtype=np.uint8))
+    assert _as_set(back) == _as_set(base)
+
+
+def test_coarsen_keeps_balance():
+    geom = closed_box_geom()
+    lv = three_level_leaves(geom)  # level-2 leaves inside refined brick (0,0,0)
+    # flag every level-1 leaf: the octet under base brick (0,0,0) holds a
+    # refined member, so it cannot merge; nothing else is complete
+    flags = (lv[:, 0] == 1).astype(np.uint8)
+    out = amr.coarsen(geom, lv, flags)
+    check_balanced(out, geom.nb0)
+    assert _as_set(out) == _as_set(lv)
+    # flag the level-2 octet: it merges back, then the level-1 octet can too
+    once = amr.coarsen(geom, lv, (lv[:, 0] == 2).astype(np.uint8))
+    check_balanced(once, geom.nb0)
+    assert int(once[:, 0].max()) == 1
+    twice = amr.coarsen(geom, once, np.ones(len(once), dtype=np.uint8))
+    assert _as_set(twice) == _as_set(amr.base_leaves(list(geom.nb0)))
+
+
+def test_coarsen_refuses_a_merge_next_to_two_levels_finer():
+    geom = closed_box_geom(nb0=(4, 2, 2))
+    lv = amr.base_leaves(list(geom.nb0))
+    lv = refine_where(geom, lv, lambda L, x, y, z: L == 0 and x in (1, 2))
+    lv = refine_where(geom, lv, lambda L, x, y, z: L == 1 and x == 4 and y == 0 and z == 0)
+    check_balanced(lv, geom.nb0)
+    # the level-1 octet of base brick 1 touches the level-2 leaves inside brick 2
+    out = amr.coarsen(geom, lv, ((lv[:, 0] == 1) & (lv[:, 1] < 4)).astype(np.uint8))
+    check_balanced(out, geom.nb0)
+    assert (1, 2, 0, 0) in _as_set(out)  # still refined
