@@ -353,15 +353,26 @@ nb_status nb_case_read_checkpoint(nb_case* c, const char* path);
 int nb_checkpoint_info(const char* path, int32_t* kind, int32_t dims[3], int64_t* nleaf, int32_t* step,
                        double* t, double* dt);
 
+/* ---- field output -------------------------------------------------------------
+ * Replaces writeGridVtu (core/src/flow/case.cpp:175-241): a VTK XML
+ * unstructured grid, one hexahedron per cell (8 corners in VTK order), ASCII
+ * values at 8 significant digits, cell data u, v, w (cell-centred, NSSolver::
+ * cellVelocity), p, speed and solid. Uniform cases list cells in the
+ * reference's lexicographic order; octree cases list every leaf cell (leaves in
+ * rank order, cells x-fastest) and add an Int32 `level` array, as the octree
+ * writer does (core/src/io/vtu_writer.cpp:8-80). */
+nb_status nb_case_write_vtu(nb_case* c, const char* path);
+
 /* ---- case run loop ------------------------------------------------------------
  * Replaces runCase (core/src/flow/case.cpp:349-401), the loop behind
  * `nabla_solve run`: create and initialize the case, optionally restart from
  * a checkpoint, then step (dt from computeDt) up to max_steps times, appending
  * one diagnostics.jsonl record per step in the reference's schema and number
  * formatting (a provenance line first in a fresh file), writing
- * checkpoint_<step>.ckpt every checkpoint_every steps and final.ckpt at the
- * end, stopping at stop_time or when the momentum residual falls below
- * steady_tol after step 20. No .vtu snapshots are written. */
+ * checkpoint_<step>.ckpt every checkpoint_every steps, snapshot_<step>.vtu
+ * every snapshot_every steps, final.vtu and final.ckpt at the end (files as
+ * nb_case_write_vtu / nb_case_write_checkpoint write them), stopping at
+ * stop_time or when the momentum residual falls below steady_tol after step 20. */
 typedef struct nb_run_options {
   const char* run_dir;        /* RunOptions::runDir (created if missing) */
   int32_t max_steps;          /* RunOptions::maxSteps */
@@ -370,7 +381,7 @@ typedef struct nb_run_options {
   double steady_tol;          /* RunOptions::steadyTol (0: ignore) */
   const char* restart_from;   /* RunOptions::restartFrom (NULL or "": fresh run) */
   int32_t precision;          /* NB_PRECISION_* */
-  int32_t reserved;
+  int32_t snapshot_every;     /* RunOptions::snapshotEvery: snapshot_<step>.vtu (0: final.vtu only) */
 } nb_run_options;
 
 typedef struct nb_run_summary {  /* mirrors RunSummary (case.hpp:29-40) */

@@ -676,6 +676,16 @@ void nb::case_set_clock(nb_case* c, int step, double t, double dt_last) {
   c->dt_last = dt_last;
 }
 
+std::vector<uint8_t> nb::case_solid(const nb_case* c) {
+  if (!c->amr) return c->solid;
+  const std::vector<uint8_t>& ty = c->mesh->lvl.type;
+  std::vector<uint8_t> out(ty.size());
+  for (size_t q = 0; q < ty.size(); ++q) out[q] = ty[q] == CELL_SOLID ? 1 : 0;
+  return out;
+}
+
+const nb_grid_desc& nb::case_grid(const nb_case* c) { return c->grid; }
+
 nb_status nb::clone_case(nb_case* src, nb_case** out) {
   nb_ctx* ctx = src->ctx;
   nb_case* c = nullptr;

@@ -4,6 +4,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "nb_internal.h"
 #include "nb_mg.cuh"
@@ -76,6 +77,11 @@ nb_ctx* case_ctx(const nb_case* c);
 void case_dims(const nb_case* c, int dims[3]);
 nb_amr_mesh* case_mesh(const nb_case* c);
 void case_set_clock(nb_case* c, int step, double t, double dt_last);
+// Per-cell solid flags for output: uniform cases nx*ny*nz lexicographic (or
+// empty when the grid has none), octree cases leaves*512 in storage order.
+std::vector<uint8_t> case_solid(const nb_case* c);
+// The grid description a uniform case was created with.
+const nb_grid_desc& case_grid(const nb_case* c);
 
 // Grows the context's two staging buffers to at least `elems` doubles each.
 void ensure_staging(nb_ctx* ctx, size_t elems);

@@ -5,8 +5,7 @@
 // (one JSON object per step, keys in the reference's order, numbers written by
 // a default-formatted std::ostream as the reference writes them) are the
 // reference's, so the consumers of a run directory read either. The first line
-// of a fresh file is a provenance record naming this library. Snapshots
-// (.vtu) are not written: this library has no VTU writer.
+// of a fresh file is a provenance record naming this library.
 #include <filesystem>
 #include <fstream>
 #include <string>
@@ -61,6 +60,10 @@ nb_status nb_run_case(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_confi
     if ((st = nb_step(h.c, 0.0, &last)) != NB_OK) return st;  // dt from computeDt, as NSSolver::step()
     append_step(diag, last);
     diag.flush();
+    if (opt->snapshot_every > 0 && last.step % opt->snapshot_every == 0) {
+      const std::string p = dir + "/snapshot_" + std::to_string(last.step) + ".vtu";
+      if ((st = nb_case_write_vtu(h.c, p.c_str())) != NB_OK) return st;
+    }
     if (opt->checkpoint_every > 0 && last.step % opt->checkpoint_every == 0) {
       const std::string p = dir + "/checkpoint_" + std::to_string(last.step) + ".ckpt";
       if ((st = nb_case_write_checkpoint(h.c, p.c_str())) != NB_OK) return st;
@@ -71,6 +74,7 @@ nb_status nb_run_case(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_confi
       break;
     }
   }
+  if ((st = nb_case_write_vtu(h.c, (dir + "/final.vtu").c_str())) != NB_OK) return st;
   if ((st = nb_case_write_checkpoint(h.c, (dir + "/final.ckpt").c_str())) != NB_OK) return st;
   sum.steps = last.step;
   sum.time = last.t;

@@ -155,7 +155,7 @@ class TuneReport(C.Structure):
 class RunOptions(C.Structure):
     _fields_ = [("run_dir", C.c_char_p), ("max_steps", C.c_int32), ("checkpoint_every", C.c_int32),
                 ("stop_time", C.c_double), ("steady_tol", C.c_double), ("restart_from", C.c_char_p),
-                ("precision", C.c_int32), ("reserved", C.c_int32)]
+                ("precision", C.c_int32), ("snapshot_every", C.c_int32)]
 
 
 class RunSummary(C.Structure):
@@ -199,6 +199,7 @@ PROTOTYPES = [
     ("nb_amr_case_transfer", C.c_int, [VP, VP]),
     ("nb_amr_coarsen", C.c_int, [C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_uint8),
                                  C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
+    ("nb_case_write_vtu", C.c_int, [VP, C.c_char_p]),
     ("nb_run_case", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(FlowConfig), C.POINTER(RunOptions),
                               C.POINTER(RunSummary)]),
     ("nb_case_write_checkpoint", C.c_int, [VP, C.c_char_p]),

@@ -192,6 +192,10 @@ class AmrCase:
         """Take src's state and clock across a regrid (nb_amr_case_transfer)."""
         self.ctx.check(self.ctx.lib.nb_amr_case_transfer(self.h, src.h), "nb_amr_case_transfer")
 
+    def write_vtu(self, path):
+        """VTK XML unstructured grid of the cell-centred state (nb_case_write_vtu)."""
+        self.ctx.check(self.ctx.lib.nb_case_write_vtu(self.h, str(path).encode()), "write_vtu")
+
     def write_checkpoint(self, path):
         """Octree checkpoint (NBFAMR1): leaf list, step clock, u, v, w, p."""
         self.ctx.check(self.ctx.lib.nb_case_write_checkpoint(self.h, str(path).encode()), "write_checkpoint")

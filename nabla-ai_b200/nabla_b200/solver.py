@@ -156,6 +156,10 @@ class NSSolver:
                        "nb_case_sample")
         return out
 
+    def write_vtu(self, path):
+        """VTK XML unstructured grid of the cell-centred state (nb_case_write_vtu)."""
+        self.ctx.check(self.ctx.lib.nb_case_write_vtu(self.h, str(path).encode()), "write_vtu")
+
     def write_checkpoint(self, path):
         """writeCheckpoint (core/src/flow/case.cpp:274-294): the reference's NBFCK01 file."""
         self.ctx.check(self.ctx.lib.nb_case_write_checkpoint(self.h, str(path).encode()), "write_checkpoint")
@@ -291,13 +295,13 @@ def checkpoint_info(path) -> dict | None:
 
 
 def run_case(grid: Grid, config: abi.FlowConfig, run_dir, max_steps: int, *, checkpoint_every: int = 0,
-             stop_time: float = 0.0, steady_tol: float = 0.0, restart_from=None,
+             snapshot_every: int = 0, stop_time: float = 0.0, steady_tol: float = 0.0, restart_from=None,
              precision: int = abi.PRECISION_FP64, ctx: Context | None = None) -> dict:
     """nb_run_case: runCase (core/src/flow/case.cpp:349-401) on the GPU, writing
     diagnostics.jsonl and checkpoints into run_dir. Returns the RunSummary."""
     ctx = ctx or default_context()
     opt = abi.RunOptions(str(run_dir).encode(), max_steps, checkpoint_every, stop_time, steady_tol,
-                         str(restart_from).encode() if restart_from else None, precision, 0)
+                         str(restart_from).encode() if restart_from else None, precision, snapshot_every)
     out = abi.RunSummary()
     ctx.check(ctx.lib.nb_run_case(ctx.h, C.byref(grid.desc()), C.byref(config), C.byref(opt), C.byref(out)),
               "nb_run_case")

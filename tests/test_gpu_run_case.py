@@ -1,8 +1,10 @@
 """The case run loop (nb_run_case) against the reference's runCase
 (core/src/flow/case.cpp:349-401) on the same channel: diagnostics.jsonl
 records with the same keys in the same order and matching values, the same
-checkpoint files with states within 1e-10 relative, and a restart from an
-intermediate checkpoint that ends bit for bit on the uninterrupted run."""
+checkpoint files with states within 1e-10 relative, the same final.vtu
+(writeGridVtu, case.cpp:175-241) to its 8 printed digits, and a restart from
+an intermediate checkpoint that ends bit for bit on the uninterrupted run.
+Octree cases write every leaf cell with its level."""
 import json
 import struct
 
@@ -32,6 +34,17 @@ def _ckpt(path):
     return struct.unpack_from("<i", raw, 20)[0], arrs
 
 
+def _vtu(path):
+    """Points, the three cell arrays and every CellData array of a VTU file."""
+    import xml.etree.ElementTree as ET
+    root = ET.parse(path).getroot()
+    piece = root.find("UnstructuredGrid/Piece")
+    arrays = {}
+    for da in piece.iter("DataArray"):
+        arrays[da.get("Name") or "points"] = np.array(da.text.split(), dtype=np.float64)
+    return int(piece.get("NumberOfCells")), arrays
+
+
 def _channel():
     grid, cfg = cases.channel(32, 16, 100.0, 1.0)
     cfg.poisson_tol = 1e-9
@@ -57,6 +70,13 @@ def test_run_case_matches_reference(ctx, ref, tmp_path):
             assert g[k] == pytest.approx(r[k], rel=2e-5, abs=1e-12), k
         for k in RESIDUAL:  # solver-tolerance quantities: same order of magnitude
             assert abs(g[k]) <= max(10 * abs(r[k]), 1e-9), k
+    nr, ra = _vtu(rd / "final.vtu")
+    ng, ga = _vtu(gd / "final.vtu")
+    assert ng == nr == grid.nx * grid.ny * grid.nz and set(ga) == set(ra)
+    for k in ("points", "connectivity", "offsets", "types", "solid"):
+        assert np.array_equal(ga[k], ra[k]), k
+    for k in ("u", "v", "w", "p", "speed"):  # 8 significant digits in the file
+        assert np.allclose(ga[k], ra[k], rtol=1e-6, atol=1e-9 * np.abs(ra[k]).max()), k
     for name in ("checkpoint_5.ckpt", "checkpoint_10.ckpt", "final.ckpt"):
         rstep, ra = _ckpt(rd / name)
         gstep, ga = _ckpt(gd / name)
@@ -79,3 +99,24 @@ def test_run_case_restart_is_bit_exact(ctx, tmp_path):
         assert np.array_equal(x, y)
     with pytest.raises(solver.NablaError, match="cannot open"):
         solver.run_case(grid, cfg, tmp_path / "bad", 1, restart_from=tmp_path / "missing.ckpt", ctx=ctx)
+
+
+def test_octree_vtu(ctx, tmp_path):
+    from amr_helpers import closed_box_geom, two_level_leaves
+    from nabla_b200 import abi, amr
+    geom = closed_box_geom()
+    mesh = amr.AmrMesh(geom, two_level_leaves(geom), ctx=ctx)
+    ac = amr.AmrCase(mesh, cases.flow_config(reynolds=100.0, convection=abi.CONV_WENO5))
+    rng = np.random.default_rng(7)
+    ac.set_state(*[rng.uniform(-1, 1, n) for n in ac.sizes])
+    ac.write_vtu(tmp_path / "o.vtu")
+    n, arr = _vtu(tmp_path / "o.vtu")
+    assert n == mesh.ncell and arr["points"].size == 24 * n
+    assert np.array_equal(arr["level"], np.repeat(mesh.leaves[:, 0], 512))
+    x, y, z = mesh.cell_centers()
+    pts = np.stack([x, y, z], axis=1)
+    for c, k in enumerate("uvwp"):
+        want = ac.sample(c, pts)
+        assert np.allclose(arr[k], want, rtol=1e-7, atol=1e-12), k
+    corners = arr["points"].reshape(n, 8, 3)
+    assert np.allclose(corners.mean(axis=1), pts, rtol=0, atol=1e-12)
