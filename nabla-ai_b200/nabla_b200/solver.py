@@ -306,3 +306,56 @@ def run_case(grid: Grid, config: abi.FlowConfig, run_dir, max_steps: int, *, che
     ctx.check(ctx.lib.nb_run_case(ctx.h, C.byref(grid.desc()), C.byref(config), C.byref(opt), C.byref(out)),
               "nb_run_case")
     return out.as_dict()
+
+
+def load_case(path) -> dict:
+    """loadCase (core/src/flow/case.cpp:136-170) for a case JSON file: the same
+    keys, case types, builder defaults and run options, plus this library's keys
+    "precision" ("fp64" default, or "mixed") and "backend" ("cuda"; "cpu" names the
+    reference's own solver and is refused here). Returns name, grid, config, run
+    (run_case keyword arguments), precision and backend."""
+    import json
+
+    from . import cases
+    j = json.loads(open(path).read())
+    kind = j.get("type", "lid-cavity")
+    re_, res = float(j.get("reynolds", 100.0)), int(j.get("resolution", 64))
+    run = dict(max_steps=20000, snapshot_every=0, checkpoint_every=0, stop_time=0.0, steady_tol=0.0)
+    if kind == "lid-cavity":
+        grid, cfg = cases.lid_cavity(res, re_, float(j.get("lid_velocity", 1.0)))
+        run.update(max_steps=60000, steady_tol=1e-6)
+    elif kind in ("channel", "poiseuille"):
+        grid, cfg = cases.channel(int(j.get("nx", 6 * res)), res, re_, float(j.get("bulk_velocity", 1.0)))
+        run.update(max_steps=40000, steady_tol=1e-6)
+    elif kind == "wall-mounted-cube":
+        grid, cfg = cases.wall_mounted_cube(res, re_)
+        run.update(max_steps=200, snapshot_every=50, checkpoint_every=50)
+    else:
+        raise ValueError(f"loadCase: unknown case type '{kind}'")
+    cfg.cfl = float(j.get("cfl", cfg.cfl))
+    if j.get("convection") == "weno5":
+        cfg.convection = abi.CONV_WENO5
+    elif j.get("convection") == "central":
+        cfg.convection = abi.CONV_CENTRAL
+    run["run_dir"] = j.get("run_dir", "run_" + kind)
+    for key, cast in (("max_steps", int), ("snapshot_every", int), ("checkpoint_every", int),
+                      ("stop_time", float), ("steady_tol", float)):
+        if key in j:
+            run[key] = cast(j[key])
+    run["restart_from"] = j.get("restart_from") or None
+    backend = j.get("backend", "cuda")
+    if backend != "cuda":
+        raise ValueError(f"load_case: backend '{backend}' is not this library's (use \"cuda\")")
+    precision = {"fp64": abi.PRECISION_FP64, "mixed": abi.PRECISION_MIXED}.get(j.get("precision", "fp64"))
+    if precision is None:
+        raise ValueError(f"load_case: unknown precision '{j.get('precision')}'")
+    return dict(name=j.get("name", kind), grid=grid, config=cfg, run=run, precision=precision, backend=backend)
+
+
+def run_case_file(path, ctx: Context | None = None) -> dict:
+    """`nabla_solve run <case.json>` on the GPU: load_case + run_case."""
+    spec = load_case(path)
+    run = dict(spec["run"])
+    run_dir = run.pop("run_dir")
+    max_steps = run.pop("max_steps")
+    return run_case(spec["grid"], spec["config"], run_dir, max_steps, precision=spec["precision"], ctx=ctx, **run)

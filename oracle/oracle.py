@@ -162,6 +162,8 @@ class Reference(_Common):
         L.ref_ns_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_run_case.argtypes = [GP, FP, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_char_p,
                                    DP, C.POINTER(C.c_int)]
+        L.ref_load_case.argtypes = [C.c_char_p, GP, C.POINTER(C.c_uint8), C.c_uint64, FP, C.c_char_p, C.c_int,
+                                    C.POINTER(C.c_int), DP]
         L.ref_morton_encode.restype = C.c_uint64
         L.ref_morton_encode.argtypes = [C.c_uint32] * 3
         L.ref_morton_decode.argtypes = [C.c_uint64] + [C.POINTER(C.c_uint32)] * 3
@@ -203,6 +205,23 @@ class Reference(_Common):
 
     def ns(self, grid, cfg):
         return _NS(self.lib, "ref", grid, cfg)
+
+    def load_case(self, path, max_cells=1 << 24):
+        """The reference's loadCase (core/src/flow/case.cpp:136-170): grid descriptor, solid
+        mask, flow config, run directory and run options (max_steps, snapshot_every,
+        checkpoint_every, stop_time, steady_tol)."""
+        g, cfg = abi.GridDesc(), abi.FlowConfig()
+        solid = np.zeros(max_cells, dtype=np.uint8)
+        run_dir = C.create_string_buffer(4096)
+        run, runf = (C.c_int * 3)(), np.zeros(2)
+        rc = self.lib.ref_load_case(str(path).encode(), C.byref(g), solid.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                    max_cells, C.byref(cfg), run_dir, 4096, run, abi.dptr(runf))
+        if rc:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        n = g.nx * g.ny * g.nz
+        opts = dict(run_dir=run_dir.value.decode(), max_steps=run[0], snapshot_every=run[1],
+                    checkpoint_every=run[2], stop_time=float(runf[0]), steady_tol=float(runf[1]))
+        return g, solid[:n].copy(), cfg, opts
 
     def run_case(self, grid, cfg, run_dir, max_steps, stop_time=0.0, steady_tol=0.0, checkpoint_every=0,
                  restart_from=None):

@@ -15,6 +15,7 @@
 //   nabla::flow::makeChannel etc.    core/src/flow/case.cpp:25-134
 //   writeCheckpoint / readCheckpoint core/src/flow/case.cpp:274-323
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -287,6 +288,28 @@ int ref_run_case(const nb_grid_desc* grid, const nb_flow_config* cfg, const char
                        s.massError, s.cd, s.cl};
   for (int q = 0; q < 7; ++q) summary[q] = v[q];
   *steady = s.steady ? 1 : 0;
+  return 0;
+  SHIM_CATCH
+}
+
+// loadCase (core/src/flow/case.cpp:136-170): the spec's grid (solid mask into
+// `solid`, cap bytes), flow config and run options; run = max_steps,
+// snapshot_every, checkpoint_every; runf = stop_time, steady_tol.
+int ref_load_case(const char* path, nb_grid_desc* grid, uint8_t* solid, uint64_t cap, nb_flow_config* cfg,
+                  char* run_dir, int run_dir_cap, int* run, double* runf) {
+  SHIM_TRY
+  const flow::CaseSpec s = flow::loadCase(path);
+  fromGrid(s.grid, grid);
+  const size_t n = s.grid.cellCount();
+  if (s.grid.solid.size() == n && n <= cap) std::memcpy(solid, s.grid.solid.data(), n);
+  grid->solid = nullptr;
+  fromCfg(s.flow, cfg);
+  std::snprintf(run_dir, static_cast<size_t>(run_dir_cap), "%s", s.run.runDir.c_str());
+  run[0] = s.run.maxSteps;
+  run[1] = s.run.snapshotEvery;
+  run[2] = s.run.checkpointEvery;
+  runf[0] = s.run.stopTime;
+  runf[1] = s.run.steadyTol;
   return 0;
   SHIM_CATCH
 }

@@ -67,3 +67,45 @@ def test_reference_run_directory(ref, tmp_path):
                               "cells", "accepted"]
     assert solver.checkpoint_info(tmp_path / "checkpoint_2.ckpt")["step"] == 2
     assert solver.checkpoint_info(tmp_path / "final.ckpt")["step"] == 3
+
+
+def _case_files(tmp_path):
+    import json
+    specs = {
+        "cavity.json": {"type": "lid-cavity", "name": "c", "reynolds": 100, "resolution": 24, "cfl": 0.8,
+                        "convection": "central", "max_steps": 80, "steady_tol": 1e-5, "run_dir": "rc"},
+        "channel.json": {"type": "channel", "reynolds": 50, "resolution": 8, "nx": 40, "bulk_velocity": 1.5,
+                         "checkpoint_every": 7},
+        "cube.json": {"type": "wall-mounted-cube", "reynolds": 300, "resolution": 4, "convection": "weno5",
+                      "stop_time": 2.5, "precision": "mixed"},
+    }
+    out = []
+    for name, spec in specs.items():
+        p = tmp_path / name
+        p.write_text(json.dumps(spec))
+        out.append(p)
+    return out
+
+
+def test_load_case_matches_the_reference(ref, tmp_path):
+    """solver.load_case against the reference's own loadCase on the same files."""
+    for path in _case_files(tmp_path):
+        g, solid, cfg, run = ref.load_case(path)
+        spec = solver.load_case(path)
+        d = spec["grid"].desc()
+        for f in ("nx", "ny", "nz", "dx", "dy", "dz"):
+            assert getattr(d, f) == getattr(g, f), (path.name, f)
+        assert tuple(d.origin) == tuple(g.origin)
+        for q in range(6):
+            for f in ("type", "profile", "inlet_axis", "inlet_speed"):
+                assert getattr(d.face[q], f) == getattr(g.face[q], f), (path.name, q, f)
+            assert tuple(d.face[q].wall_velocity) == tuple(g.face[q].wall_velocity)
+        assert np.array_equal(np.asarray(spec["grid"].solid, dtype=np.uint8), solid)
+        c = spec["config"]
+        for f, _ in cfg._fields_:
+            a, b = getattr(c, f), getattr(cfg, f)
+            assert (tuple(a) == tuple(b)) if f == "body_force" else a == b, (path.name, f)
+        r = dict(spec["run"])
+        r.pop("restart_from")
+        assert r == run, path.name
+    assert solver.load_case(_case_files(tmp_path)[2])["precision"] == 1

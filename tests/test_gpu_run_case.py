@@ -120,3 +120,28 @@ def test_octree_vtu(ctx, tmp_path):
         assert np.allclose(arr[k], want, rtol=1e-7, atol=1e-12), k
     corners = arr["points"].reshape(n, 8, 3)
     assert np.allclose(corners.mean(axis=1), pts, rtol=0, atol=1e-12)
+
+
+def test_case_file_run_matches_reference(ctx, ref, tmp_path):
+    """`nabla_solve run <case.json>` on the GPU (solver.run_case_file) against the
+    reference's runCase on the same file's spec."""
+    path = tmp_path / "cavity.json"
+    gd = tmp_path / "gpu"
+    path.write_text(json.dumps({"type": "lid-cavity", "reynolds": 100, "resolution": 24, "cfl": 0.8,
+                                "convection": "central", "max_steps": 6, "run_dir": str(gd),
+                                "checkpoint_every": 3, "backend": "cuda", "precision": "fp64"}))
+    spec = solver.load_case(path)
+    rd = tmp_path / "ref"
+    ref.run_case(spec["grid"], spec["config"], rd, 6, checkpoint_every=3)
+    s = solver.run_case_file(path, ctx=ctx)
+    assert s["steps"] == 6
+    R, G = _records(rd / "diagnostics.jsonl"), _records(gd / "diagnostics.jsonl")
+    assert [r["poisson_iters"] for r in R[1:]] == [g["poisson_iters"] for g in G[1:]]
+    for r, g in zip(R[1:], G[1:]):
+        for k in PHYSICAL:
+            assert g[k] == pytest.approx(r[k], rel=2e-5, abs=1e-12), k
+    for name in ("checkpoint_3.ckpt", "checkpoint_6.ckpt", "final.ckpt", "final.vtu"):
+        assert (gd / name).exists() and (rd / name).exists()
+    with pytest.raises(ValueError, match="backend"):
+        path.write_text(json.dumps({"type": "lid-cavity", "backend": "cpu"}))
+        solver.load_case(path)
