@@ -770,7 +770,7 @@ void nb_ctx_destroy(nb_ctx* ctx) {
 
 const char* nb_last_error(const nb_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
-uint64_t nb_ctx_launch_count(const nb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+uint64_t nb_ctx_launch_count(const nb_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
 
 void* nb_ctx_stream(const nb_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
@@ -864,7 +864,9 @@ nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_co
     NB_CUDA(cudaMemset(c->d_blk, 0, sizeof(StepBlock)));
     NB_CUDA(cudaMallocHost(&c->h_blk, sizeof(StepBlock)));
     NB_CUDA(cudaMallocHost(&c->h_dt, sizeof(double)));
-    NB_CUDA(cudaDeviceSynchronize());
+    // the uploads and memsets above ran on the legacy stream; the case's own
+    // stream is non-blocking, so steps of other cases keep running meanwhile
+    NB_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
     return NB_OK;
   });
   if (s != NB_OK) return s;
@@ -1384,7 +1386,9 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     NB_CUDA(cudaMemset(c->d_blk, 0, sizeof(StepBlock)));
     NB_CUDA(cudaMallocHost(&c->h_blk, sizeof(StepBlock)));
     NB_CUDA(cudaMallocHost(&c->h_dt, sizeof(double)));
-    NB_CUDA(cudaDeviceSynchronize());
+    // the uploads and memsets above ran on the legacy stream; the case's own
+    // stream is non-blocking, so steps of other cases keep running meanwhile
+    NB_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
     return NB_OK;
   });
   if (s != NB_OK) return s;

@@ -28,7 +28,7 @@ struct nb_ctx {
   // whatever order the caller (or a garbage collector) destroys them
   std::atomic<int> refs{1};
   std::string err;
-  uint64_t launches = 0;
+  std::atomic<uint64_t> launches{0};  // atomic: cases may be built on one thread while others step
   nb::Profiler prof;
   cudaStream_t stream = nullptr;
   int nsm = 148;     // SMs of the device

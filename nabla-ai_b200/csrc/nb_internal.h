@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -234,10 +235,10 @@ struct Profiler {
 
 // Launch accounting shared by every launch site of a context.
 struct LaunchCounter {
-  uint64_t* count = nullptr;
+  std::atomic<uint64_t>* count = nullptr;
   Profiler* prof = nullptr;
   void add(uint64_t n = 1) {
-    if (count) *count += n;
+    if (count) count->fetch_add(n, std::memory_order_relaxed);
   }
 };
 

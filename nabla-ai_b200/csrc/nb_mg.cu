@@ -1732,8 +1732,8 @@ void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int ma
   NB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
   cudaGraph_t body = p.conditional.phGraph_out[0];
   if (!side_) NB_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-  uint64_t* saved = lc_.count;
-  uint64_t nbody = 0;
+  std::atomic<uint64_t>* saved = lc_.count;
+  std::atomic<uint64_t> nbody{0};
   lc_.count = &nbody;
   NB_CUDA(cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   iterate(side_, tol, maxit, 2);
@@ -1741,7 +1741,7 @@ void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int ma
   cudaGraph_t body_out = nullptr;
   NB_CUDA(cudaStreamEndCapture(side_, &body_out));
   lc_.count = saved;
-  if (body_kernels) *body_kernels = nbody;
+  if (body_kernels) *body_kernels = nbody.load();
   NB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
   finish(s, report);
 }

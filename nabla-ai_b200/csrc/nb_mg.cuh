@@ -68,8 +68,8 @@ class MgSolver {
   static nb_poisson_report report_from(const double* r, double tol);
   // Number of loop-body executions so far (device counter).
   unsigned long long* body_execs() const { return body_execs_; }
-  void set_counter(uint64_t* c) { lc_.count = c; }
-  uint64_t* counter() const { return lc_.count; }
+  void set_counter(std::atomic<uint64_t>* c) { lc_.count = c; }
+  std::atomic<uint64_t>* counter() const { return lc_.count; }
 
   // out = A x (CgPoisson::applyA on level 0), brick layout.
   void apply_a(cudaStream_t s, const double* x, double* out);

@@ -75,72 +75,97 @@ def poisson_arrivals(rate: float, duration: float, seed: int) -> np.ndarray:
 class Server:
     """`slots` caps the cases in flight (continuous batching admits a waiting
     request only when a slot and its footprint are free, so requests finish
-    at the rate the device serves them instead of all slowing down together)."""
+    at the rate the device serves them instead of all slowing down together).
+    Admitted cases are built on `builders` host threads (ctypes releases the
+    GIL; case creation synchronises only its own uploads), so the loop keeps
+    launching steps of the active cases while new ones are set up."""
 
     def __init__(self, ctx: solver.Context, hbm_budget: float, precision: int = abi.PRECISION_MIXED,
-                 keep_results: bool = False, slots: int = 32):
+                 keep_results: bool = False, slots: int = 32, builders: int = 2):
         self.ctx, self.budget, self.precision, self.keep = ctx, hbm_budget, precision, keep_results
-        self.slots = slots
+        self.slots, self.builders = slots, builders
+
+    def _build(self, r: Request):
+        b0 = time.perf_counter()
+        case = r.build(self.ctx, self.precision)
+        return case, time.perf_counter() - b0
 
     def run(self, requests: list[Request], time_limit: float | None = None) -> ServeStats:
+        from concurrent.futures import ThreadPoolExecutor, wait, FIRST_COMPLETED
         st = ServeStats(offered=len(requests))
         pending = sorted(requests, key=lambda r: r.arrival)
         queue: list[Request] = []
         active: list[tuple[Request, object, int]] = []  # (request, case, steps left)
-        used = 0
+        building: list[tuple[Request, object, float]] = []  # (request, future, reserved bytes)
+        used = 0.0
         t0 = time.perf_counter()
         nxt = 0
-        while nxt < len(pending) or queue or active:
-            now = time.perf_counter() - t0
-            if time_limit is not None and now > time_limit:
-                break
-            while nxt < len(pending) and pending[nxt].arrival <= now:
-                queue.append(pending[nxt])
-                nxt += 1
-            st.max_queue = max(st.max_queue, len(queue))
-            # launch one step of every active case, then admit (build on the
-            # host while those steps run), then collect
-            for _, case, _ in active:
-                solver.step_async(case, 0.0)
-            joined = []
-            while queue and len(active) + len(joined) < self.slots:
-                r = queue[0]
-                need = r.cells_hint * BYTES_PER_CELL[self.precision]
-                if (active or joined) and used + need > self.budget:
+        pool = ThreadPoolExecutor(max_workers=max(1, self.builders))
+        try:
+            while nxt < len(pending) or queue or active or building:
+                now = time.perf_counter() - t0
+                if time_limit is not None and now > time_limit:
                     break
-                queue.pop(0)
-                r.admitted = time.perf_counter() - t0
-                b0 = time.perf_counter()
-                case = r.build(self.ctx, self.precision)
-                st.build_s += time.perf_counter() - b0
-                r.cells = case.cell_count
-                used += self.ctx.lib.nb_case_device_bytes(case.h)
-                joined.append((r, case, r.steps))
-            st.max_active = max(st.max_active, len(active) + len(joined))
-            st.peak_bytes = max(st.peak_bytes, used)
-            if not active:
-                active = joined
-                if not active and nxt < len(pending):
-                    time.sleep(max(0.0, pending[nxt].arrival - (time.perf_counter() - t0)))
-                continue
-            still = []
-            for r, case, left in active:
-                rep = solver.step_wait(case)
-                st.cell_steps += r.cells
-                left -= 1
-                if left > 0:
-                    still.append((r, case, left))
+                while nxt < len(pending) and pending[nxt].arrival <= now:
+                    queue.append(pending[nxt])
+                    nxt += 1
+                st.max_queue = max(st.max_queue, len(queue))
+                # launch one step of every active case; admit and build while they run
+                for _, case, _ in active:
+                    solver.step_async(case, 0.0)
+                while queue and len(active) + len(building) < self.slots:
+                    r = queue[0]
+                    need = r.cells_hint * BYTES_PER_CELL[self.precision]
+                    if (active or building) and used + need > self.budget:
+                        break
+                    queue.pop(0)
+                    r.admitted = time.perf_counter() - t0
+                    used += need
+                    building.append((r, pool.submit(self._build, r), need))
+                joined, still_building = [], []
+                for r, fut, need in building:
+                    if not fut.done():
+                        still_building.append((r, fut, need))
+                        continue
+                    case, dt = fut.result()
+                    st.build_s += dt
+                    r.cells = case.cell_count
+                    used += self.ctx.lib.nb_case_device_bytes(case.h) - need
+                    joined.append((r, case, r.steps))
+                building = still_building
+                st.max_active = max(st.max_active, len(active) + len(joined) + len(building))
+                st.peak_bytes = max(st.peak_bytes, used)
+                if not active:
+                    active = joined
+                    if not active:
+                        if building:
+                            wait([f for _, f, _ in building], timeout=0.05, return_when=FIRST_COMPLETED)
+                        elif nxt < len(pending):
+                            time.sleep(max(0.0, pending[nxt].arrival - (time.perf_counter() - t0)))
                     continue
-                r.done = time.perf_counter() - t0
-                r.report = rep
-                if self.keep:
-                    r.result = case.get_state()
-                st.served += 1
-                st.latencies.append(r.done - r.arrival)
-                used -= self.ctx.lib.nb_case_device_bytes(case.h)
+                still = []
+                for r, case, left in active:
+                    rep = solver.step_wait(case)
+                    st.cell_steps += r.cells
+                    left -= 1
+                    if left > 0:
+                        still.append((r, case, left))
+                        continue
+                    r.done = time.perf_counter() - t0
+                    r.report = rep
+                    if self.keep:
+                        r.result = case.get_state()
+                    st.served += 1
+                    st.latencies.append(r.done - r.arrival)
+                    used -= self.ctx.lib.nb_case_device_bytes(case.h)
+                    case.close()
+                active = still + joined
+            st.wall_s = time.perf_counter() - t0
+        finally:
+            for _, case, _ in active:
                 case.close()
-            active = still + joined
-        st.wall_s = time.perf_counter() - t0
-        for _, case, _ in active:
-            case.close()
+            for _, fut, _ in building:
+                case, _ = fut.result()
+                case.close()
+            pool.shutdown(wait=True)
         return st
