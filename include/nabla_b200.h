@@ -200,6 +200,10 @@ typedef struct nb_tuning {
   int32_t threads_per_brick; /* CTA size of the smoother, residual-restriction and
                                 matvec kernels: 512, 256 or 128 (1, 2 or 4 cells
                                 per thread; smaller CTAs keep more bricks in flight) */
+  int32_t smoother;          /* mixed form: 1 (default) Chebyshev polynomial on
+                                [lmax/6, lmax] of D^-1 A (same cost per sweep,
+                                stronger smoothing), 0 damped Jacobi (omega 0.8);
+                                the FP64 form always uses the reference's Jacobi */
 } nb_tuning;
 
 typedef struct nb_tune_report {

@@ -299,15 +299,22 @@ __device__ __forceinline__ void full_row(const LevelView& L, uint32_t code, cons
 
 // ---------------------------------------------------------------------------
 // Damped-Jacobi sweep (multigrid.cpp:102-114), one sweep per launch.
-//   xout = fluid ? x' + omega (b' - A x') / D : 0
-// where x' / b' include pending mean / prolongation. Optionally reduces the
-// fluid sum of xout into `mean_out` (= sum / nfluid) for the next removeMean.
+//   xout = fluid ? x' + c2 (b' - A x') / D + c1 (x' - x_prev) : 0
+// where x' / b' include pending mean / prolongation. c2 = omega, c1 = 0 is the
+// reference's Jacobi (prev_mode 0); the mixed form may run a Chebyshev
+// polynomial instead, whose later sweeps add c1 times the last step: x_prev
+// is 0 (prev_mode 2, the first step of a phase from x = 0) or the previous
+// iterate as P fetches it at the cell (prev_mode 1: its buffer is xout's,
+// read before it is overwritten, with its pending mean and prolongation).
+// Optionally reduces the fluid sum of xout into `mean_out` (= sum / nfluid)
+// for the next removeMean.
 // ---------------------------------------------------------------------------
 template <typename T, int NTH>
 __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b,
-                                                const double* bmean, XFetch<T> X, T* __restrict__ xout,
+                                                const double* bmean, XFetch<T> X, T* xout,
                                                 RedBuf rb, double* mean_out, double inv_nfluid,
-                                                const SolveFlags* flags, int maxit) {
+                                                const SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
+                                                XFetch<T> P) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   pdl_wait();
   if (stopped(flags, maxit)) return;
@@ -354,7 +361,16 @@ __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict
         if (bmean) bc = bc - static_cast<T>(*bmean);
         const T Ax = diag * xc - off;
         const T dM = diag > T(0) ? diag : T(1);
-        out = xc + static_cast<T>(kOmega) * (bc - Ax) / dM;
+        out = xc + c2 * (bc - Ax) / dM;
+        if (prev_mode) {
+          T xp = T(0);
+          if (prev_mode == 1) {
+            int gi, gj, gk;
+            cell_coords(L, c, gi, gj, gk);
+            xp = P(c, gi, gj, gk);
+          }
+          out = out + c1 * (xc - xp);
+        }
         part[0] += wgt * static_cast<double>(out);
       }
       xout[c] = out;
@@ -1453,6 +1469,29 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
   sweeps_ = precision_ == NB_PRECISION_MIXED ? std::min(std::max(t.sweeps, 1), 3) : 2;  // FP64: V(2,2) as the reference
   halo_mode_ = t.halo_mode == 1 ? 1 : 0;
   direct_max_ = std::min(std::max(t.coarse_direct_max, 0), 512);
+  // Smoother coefficients per sweep of a phase: damped Jacobi (the reference's,
+  // c2 = omega) or, mixed form only, Chebyshev on [lmax / 6, lmax] of D^-1 A
+  // with lmax = 2.05 above the Gershgorin bound 2 (three-term recurrence:
+  // theta = (lmax + lmin) / 2, delta = (lmax - lmin) / 2, sigma = theta / delta,
+  // rho_0 = 1 / sigma, rho_k = 1 / (2 sigma - rho_(k-1)); sweep 0 steps by
+  // r / theta, sweep k by 2 rho_k / delta r + rho_k rho_(k-1) times the last step).
+  cheb_ = precision_ == NB_PRECISION_MIXED && t.smoother == 1;
+  for (int k = 0; k < 4; ++k) {
+    cheb_c2_[k] = kOmega;
+    cheb_c1_[k] = 0.0;
+  }
+  if (cheb_) {
+    const double lmax = 2.05, lmin = lmax / 6.0;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    cheb_c2_[0] = 1.0 / theta;
+    for (int k = 1; k < 4; ++k) {
+      const double r = 1.0 / (2.0 * sigma - rho);
+      cheb_c1_[k] = r * rho;
+      cheb_c2_[k] = 2.0 * r / delta;
+      rho = r;
+    }
+  }
 }
 
 MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc, const nb_tuning* tune)
@@ -1601,16 +1640,17 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   T* buf[2] = {xa, xb};
   double* mean[2] = {mA, mB};
   int cur = 0;
+  const XFetch<T> none{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1};
+  auto plain = [&](int i) { return XFetch<T>{buf[i], mean[i], nullptr, nullptr, dummy, 1, 1, 1}; };
   // pre-smoothing (sweeps_ sweeps; 2 as the reference), the first from x = 0
   NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
-            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
-                        XFetch<T>{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1}, buf[cur], rb_, mean[cur],
-                        inv_nf, flags_, maxit_)));
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, none, buf[cur], rb_, mean[cur],
+                        inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
     NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
-                          XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, buf[cur ^ 1], rb_,
-                          mean[cur ^ 1], inv_nf, flags_, maxit_)));
+              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
+                          mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
+                          static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1))));
   // residual + restriction
   const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
@@ -1624,17 +1664,17 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec);
   const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
   // post-smoothing: the first sweep folds in the prolongation x += P e
+  const XFetch<T> prolonged{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
+                            Cd.h.fz, D.d_xfb, D.d_xfo};
   NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
-            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
-                        XFetch<T>{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
-                                  Cd.h.fz, D.d_xfb, D.d_xfo},
-                        buf[cur ^ 1], rb_, mean[cur ^ 1], inv_nf, flags_, maxit_)));
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
+                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
   cur ^= 1;
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
     NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
-              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
-                          XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, buf[cur ^ 1], rb_,
-                          mean[cur ^ 1], inv_nf, flags_, maxit_)));
+              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
+                          mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
+                          static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1))));
   *out_x = buf[cur];
   *out_mean_slot = sing ? lvl_slot(lvl, cur) : -1;
 }

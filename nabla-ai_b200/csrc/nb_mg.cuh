@@ -107,6 +107,9 @@ class MgSolver {
   int sweeps_ = 2;     // smoothing sweeps per side of the coarse correction
   int halo_mode_ = 0;  // 0 per-brick neighbour maps, 1 per-cell walk
   int direct_max_ = 256;  // exact coarsest solve up to this many cells
+  bool cheb_ = false;     // mixed form: Chebyshev smoothing instead of damped Jacobi
+  double cheb_c2_[4] = {0.8, 0.8, 0.8, 0.8};  // residual weight per sweep of a phase
+  double cheb_c1_[4] = {0.0, 0.0, 0.0, 0.0};  // weight of the last step per sweep
   // Exact coarsest-level solve (composite hierarchies only): the inverse of the
   // fluid block of the coarsest operator (regularised on the constant mode when
   // singular), host-factored once.

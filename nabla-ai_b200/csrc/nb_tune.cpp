@@ -2,7 +2,7 @@
 // counterpart).
 //
 // The tuned choices change launch shapes (threads per brick and CTAs per SM),
-// the multigrid halo staging, the mixed form's smoothing sweeps, the exact
+// the multigrid halo staging, the mixed form's smoother and sweeps, the exact
 // coarse-solve threshold and PDL.
 // None of them changes the discretisation: FP64 results move only by the
 // summation order of the grid reductions (grid size), mixed results by the
@@ -36,6 +36,7 @@ bool tuning_ok(const nb_tuning& t, std::string& why) {
   else if (t.pdl != 0 && t.pdl != 1) why = "pdl must be 0 or 1";
   else if (t.threads_per_brick != 128 && t.threads_per_brick != 256 && t.threads_per_brick != 512)
     why = "threads_per_brick must be 128, 256 or 512";
+  else if (t.smoother != 0 && t.smoother != 1) why = "smoother must be 0 or 1";
   else return true;
   return false;
 }
@@ -58,11 +59,11 @@ std::string tune_key(nb_ctx* ctx, const nb_case* c) {
   return s;
 }
 
-// One cache line: key and the seven fields, then ms per step.
+// One cache line: key and the eight fields, then ms per step.
 bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double& ms) {
   std::istringstream in(line);
   if (!(in >> key >> t.mg_ctas_per_sm >> t.rhs_ctas_per_sm >> t.halo_mode >> t.sweeps >> t.coarse_direct_max >>
-        t.pdl >> t.threads_per_brick >> ms))
+        t.pdl >> t.threads_per_brick >> t.smoother >> ms))
     return false;
   std::string why;
   return tuning_ok(t, why);
@@ -70,8 +71,9 @@ bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double&
 
 std::string format_line(const std::string& key, const nb_tuning& t, double ms) {
   char buf[320];
-  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm, t.rhs_ctas_per_sm,
-                t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, ms);
+  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
+                t.rhs_ctas_per_sm, t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, t.smoother,
+                ms);
   return buf;
 }
 
@@ -94,6 +96,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->coarse_direct_max = 256;
   t->pdl = 1;
   t->threads_per_brick = 512;
+  t->smoother = 1;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {
@@ -270,7 +273,10 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
   std::vector<Knob> knobs = {{&nb_tuning::rhs_ctas_per_sm, {1, 2, 3, 4}},
                              {&nb_tuning::halo_mode, {0, 1}},
                              {&nb_tuning::pdl, {0, 1}}};
-  if (prec == NB_PRECISION_MIXED) knobs.push_back({&nb_tuning::sweeps, {1, 2, 3}});
+  if (prec == NB_PRECISION_MIXED) {
+    knobs.push_back({&nb_tuning::smoother, {0, 1}});
+    knobs.push_back({&nb_tuning::sweeps, {1, 2, 3}});
+  }
   if (amr && lev > 1) knobs.push_back({&nb_tuning::coarse_direct_max, {0, 256, 512}});
   for (const Knob& k : knobs)
     for (int32_t v : k.values) {

@@ -134,6 +134,7 @@ class Tuning(C.Structure):
         ("coarse_direct_max", C.c_int32),
         ("pdl", C.c_int32),
         ("threads_per_brick", C.c_int32),
+        ("smoother", C.c_int32),
     ]
 
     def as_dict(self):

@@ -57,10 +57,10 @@ def test_fp64_tuning_keeps_the_solution(ctx, tuning):
         assert np.abs(got[a] - ref[a]).max() <= 1e-8 * np.abs(ref[0]).max()
 
 
-@pytest.mark.parametrize("sweeps", [1, 3])
-def test_mixed_sweeps_stay_within_tolerance(ctx, sweeps):
+@pytest.mark.parametrize("sweeps,smoother", [(1, 0), (3, 0), (1, 1), (2, 1), (3, 1)])
+def test_mixed_sweeps_stay_within_tolerance(ctx, sweeps, smoother):
     ref = _run(ctx, abi.PRECISION_FP64, {})
-    got = _run(ctx, abi.PRECISION_MIXED, dict(sweeps=sweeps))
+    got = _run(ctx, abi.PRECISION_MIXED, dict(sweeps=sweeps, smoother=smoother))
     for a in range(3):
         assert np.abs(got[a] - ref[a]).max() <= 1e-6 * np.abs(ref[0]).max()
 
@@ -111,3 +111,26 @@ def test_uniform_threads_per_brick(ctx, tpb):
     u1, p1 = run(dict(threads_per_brick=tpb, mg_ctas_per_sm=2048 // tpb))
     assert np.abs(u1 - u0).max() <= 1e-10 * np.abs(u0).max()
     assert np.abs(p1 - p0).max() <= 1e-10 * max(np.abs(p0).max(), 1e-30)
+
+
+@pytest.mark.parametrize("sweeps", [2, 3])
+def test_chebyshev_on_a_singular_uniform_box(ctx, sweeps):
+    """Periodic TGV 32^3 (singular: pending means on every level) in the mixed
+    form with the Chebyshev smoother against the FP64 form: converged, within
+    1e-6, and with no more MG-PCG cycles than Jacobi needs."""
+    def run(precision, tuning):
+        ctx.set_tuning(**tuning)
+        try:
+            g, cfg = cases.taylor_green(32)
+            ns = solver.NSSolver(g, cfg, precision=precision, ctx=ctx)
+            ns.set_state(*cases.taylor_green_state(g))
+            reps = [ns.step(0.05) for _ in range(2)]
+            assert all(r.converged for r in reps)
+            return ns.u_face(), sum(r.poisson_iters for r in reps)
+        finally:
+            ctx.set_tuning(**solver.default_tuning())
+    u64, _ = run(abi.PRECISION_FP64, {})
+    uj, it_j = run(abi.PRECISION_MIXED, dict(sweeps=sweeps, smoother=0))
+    uc, it_c = run(abi.PRECISION_MIXED, dict(sweeps=sweeps, smoother=1))
+    assert np.abs(uc - u64).max() <= 1e-6 * np.abs(u64).max()
+    assert it_c <= it_j
