@@ -1646,8 +1646,8 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, none, buf[cur], rb_, mean[cur],
                         inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
-  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
-    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
+  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)  // a Chebyshev step from sweep 2 on also reads x_prev
+    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + (cheb_ && sw >= 2 ? ncell * tsz : 0.0),
               (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
                           mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
                           static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1))));
@@ -1670,8 +1670,9 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
                         mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
   cur ^= 1;
-  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)
-    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1),
+  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)  // Chebyshev: x_prev, after the prolongation with its coarse value
+    NB_LAUNCH(lc_, "smooth", s,
+              ncell * (3 * tsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0),
               (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
                           mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
                           static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1))));
