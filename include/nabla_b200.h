@@ -204,6 +204,11 @@ typedef struct nb_tuning {
                                 [lmax/6, lmax] of D^-1 A (same cost per sweep,
                                 stronger smoothing), 0 damped Jacobi (omega 0.8);
                                 the FP64 form always uses the reference's Jacobi */
+  int32_t tail_bricks;       /* 0: one launch per multigrid sweep on every level;
+                                n > 0 (default 8): the V-cycle from the first level
+                                below the finest with at most n bricks down to the
+                                coarsest solve runs as one thread-block-cluster
+                                launch with those levels in shared memory (0..4096) */
 } nb_tuning;
 
 typedef struct nb_tune_report {

@@ -16,10 +16,14 @@
 #include <cmath>
 #include <cstring>
 
+#include <cooperative_groups.h>
+
 #include "nb_mg.cuh"
 #include "nb_reduce.cuh"
 
 namespace nb {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -41,16 +45,58 @@ __device__ __forceinline__ bool stopped(const SolveFlags* f, int maxit) {
 // Value of a level vector at an (in-grid, fluid) cell after the operations
 // still pending on it: the lazy removeMean (x - mean) and the lazy
 // prolongAdd (+ e[parent], itself with the coarse level's pending mean).
-template <typename T>
-struct XFetch {
+//
+// CV is how the coarse level is held (by value in kernel parameters, or as a
+// pointer into shared memory in the cluster tail); ACC is how level vectors
+// are addressed (global memory, or distributed over a cluster's shared memory).
+__device__ __forceinline__ const LevelView& lv_of(const LevelView& v) { return v; }
+__device__ __forceinline__ const LevelView& lv_of(const LevelView* v) { return *v; }
+template <bool CG, typename T>
+__device__ __forceinline__ T ldv(const T* p) {
+  if constexpr (CG) return __ldcg(p);
+  else return *p;
+}
+// Level vectors in global memory.
+struct GAcc {
+  static constexpr bool kCG = false;  // pending means: plain loads
+  template <typename T>
+  __device__ __forceinline__ T ld(const T* p, int n) const { return p[n]; }
+  template <typename T>
+  __device__ __forceinline__ void st(T* p, int n, T v) const { p[n] = v; }
+};
+// Level vectors distributed over the shared memory of a thread-block
+// cluster: brick g of a vector lives in CTA g mod cs at slot g / cs of the
+// vector's array, and a vector "pointer" is that array's byte offset in every
+// CTA's arena plus kArenaBias (so that no vector encodes as null).
+constexpr uintptr_t kArenaBias = 128;
+struct DAcc {
+  static constexpr bool kCG = true;  // pending means (global) are written inside the launch
+  char* arena;                       // this CTA's arena
+  int lcs;                           // log2 of the cluster size
+  template <typename T>
+  __device__ __forceinline__ T* at(const T* p, int n) const {
+    const int g = n >> 9;
+    T* local = reinterpret_cast<T*>(arena + (reinterpret_cast<uintptr_t>(p) - kArenaBias)) + ((g >> lcs) << 9) +
+               (n & 511);
+    return cg::this_cluster().map_shared_rank(local, static_cast<unsigned>(g & ((1 << lcs) - 1)));
+  }
+  template <typename T>
+  __device__ __forceinline__ T ld(const T* p, int n) const { return *at(p, n); }
+  template <typename T>
+  __device__ __forceinline__ void st(T* p, int n, T v) const { *at(p, n) = v; }
+};
+
+template <typename T, class CV = LevelView, class ACC = GAcc>
+struct XFetchT {
   const T* x;            // nullptr => the vector is identically zero
   const double* xmean;   // pending mean (nullptr => none)
   const T* ec;           // pending prolongation source (nullptr => none)
   const double* ecmean;  // pending mean of ec
-  LevelView C;           // coarse level (for parent lookup)
+  CV C;                  // coarse level (for parent lookup)
   int fx, fy, fz;
   const int* xfb = nullptr;  // composite fine level: parent brick per brick
   const int* xfo = nullptr;  // composite fine level: octant in the parent (-1 kept)
+  ACC acc{};
   __device__ __forceinline__ int parent(int n, int gi, int gj, int gk) const {
     if (xfb) {
       const int b = n >> 9, l = n & 511, oct = xfo[b];
@@ -59,14 +105,14 @@ struct XFetch {
                 ck = (oct >> 2) * 4 + ((l >> 6) >> 1);
       return xfb[b] * BR3 + ((ck << 6) | (cj << 3) | ci);
     }
-    return cell_index(C, gi / fx, gj / fy, gk / fz);
+    return cell_index(lv_of(C), gi / fx, gj / fy, gk / fz);
   }
   __device__ __forceinline__ T operator()(int n, int gi, int gj, int gk) const {
-    T v = x ? x[n] : T(0);
-    if (xmean) v = v - static_cast<T>(*xmean);
+    T v = x ? acc.ld(x, n) : T(0);
+    if (xmean) v = v - static_cast<T>(ldv<ACC::kCG>(xmean));
     if (ec) {
-      T e = ec[parent(n, gi, gj, gk)];
-      if (ecmean) e = e - static_cast<T>(*ecmean);
+      T e = acc.ld(ec, parent(n, gi, gj, gk));
+      if (ecmean) e = e - static_cast<T>(ldv<ACC::kCG>(ecmean));
       v = v + e;
     }
     return v;
@@ -76,8 +122,8 @@ struct XFetch {
   // brick pb of the coarser level at octant po (-1: cell for cell); composite
   // levels merge by 2 on every axis, uniform levels by fx, fy, fz.
   __device__ __forceinline__ T at(int n, int pb, int po, int amr) const {
-    T v = x ? x[n] : T(0);
-    if (xmean) v = v - static_cast<T>(*xmean);
+    T v = x ? acc.ld(x, n) : T(0);
+    if (xmean) v = v - static_cast<T>(ldv<ACC::kCG>(xmean));
     if (ec) {
       const int l = n & 511;
       int pl = l;
@@ -88,13 +134,15 @@ struct XFetch {
         const int ck = (amr || fz == 2) ? (((po >> 2) & 1) << 2) + (lk >> 1) : lk;
         pl = (ck << 6) | (cj << 3) | ci;
       }
-      T e = ec[pb * BR3 + pl];
-      if (ecmean) e = e - static_cast<T>(*ecmean);
+      T e = acc.ld(ec, pb * BR3 + pl);
+      if (ecmean) e = e - static_cast<T>(ldv<ACC::kCG>(ecmean));
       v = v + e;
     }
     return v;
   }
 };
+template <typename T>
+using XFetch = XFetchT<T>;
 
 __device__ __forceinline__ double cell_weight(const LevelView& L, int brick) {
   return L.amr ? L.bweight[brick] : 1.0;
@@ -309,26 +357,23 @@ __device__ __forceinline__ void full_row(const LevelView& L, uint32_t code, cons
 // Optionally reduces the fluid sum of xout into `mean_out` (= sum / nfluid)
 // for the next removeMean.
 // ---------------------------------------------------------------------------
-template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b,
-                                                const double* bmean, XFetch<T> X, T* xout,
-                                                RedBuf rb, double* mean_out, double inv_nfluid,
-                                                const SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
-                                                XFetch<T> P) {
+// Bricks first, first + stride, ... of one sweep; returns this thread's part
+// of the weighted fluid sum of xout. `acc` addresses b and xout.
+template <typename T, int NTH, class ACC, class FX, class FP>
+__device__ __forceinline__ double smooth_bricks(const LevelView& L, const T* b, const double* bmean, const FX& X,
+                                               T* xout, T c2, T c1, int prev_mode, const FP& P, int first,
+                                               int stride, T* tile, const ACC& acc) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
-  pdl_wait();
-  if (stopped(flags, maxit)) return;
-  __shared__ T tile[TSN];
-  double part[1] = {0.0};
+  double part = 0.0;
   const bool staged = X.x || X.ec;
-  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+  for (int brick = first; brick < L.nbrick; brick += stride) {
     uint32_t code[CPT];
     T bv[CPT];
 #pragma unroll
     for (int q = 0; q < CPT; ++q) {
       const int c = brick * BR3 + threadIdx.x + q * NTH;
       code[q] = L.code[c];
-      bv[q] = b[c];
+      bv[q] = acc.ld(b, c);
     }
     if (staged) fill_halo<T, NTH>(L, brick, tile, X);
     __syncthreads();
@@ -358,7 +403,7 @@ __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict
           xc = T(0);
         }
         T bc = bv[q];
-        if (bmean) bc = bc - static_cast<T>(*bmean);
+        if (bmean) bc = bc - static_cast<T>(ldv<ACC::kCG>(bmean));
         const T Ax = diag * xc - off;
         const T dM = diag > T(0) ? diag : T(1);
         out = xc + c2 * (bc - Ax) / dM;
@@ -371,12 +416,26 @@ __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict
           }
           out = out + c1 * (xc - xp);
         }
-        part[0] += wgt * static_cast<double>(out);
+        part += wgt * static_cast<double>(out);
       }
-      xout[c] = out;
+      acc.st(xout, c, out);
     }
     __syncthreads();
   }
+  return part;
+}
+
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b,
+                                                const double* bmean, XFetch<T> X, T* xout,
+                                                RedBuf rb, double* mean_out, double inv_nfluid,
+                                                const SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
+                                                XFetch<T> P) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;
+  __shared__ T tile[TSN];
+  double part[1] = {smooth_bricks<T, NTH>(L, b, bmean, X, xout, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile,
+                                          GAcc{})};
   if (mean_out) {
     grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
   }
@@ -388,28 +447,22 @@ __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict
 // coarse cell covered by the brick averages its fluid children, summed in the
 // reference's lexicographic child order (k, then j, then i).
 // ---------------------------------------------------------------------------
-template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __restrict__ b,
-                                                        const double* bmean, XFetch<T> X, LevelView C,
-                                                        int fx, int fy, int fz, T* __restrict__ rc,
-                                                        RedBuf rb, double* mean_out, double inv_nfluid_c,
-                                                        const SolveFlags* flags, int maxit) {
+template <typename T, int NTH, class ACC, class FX>
+__device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, const T* b, const double* bmean,
+                                                       const FX& X, const LevelView& C, int fx, int fy, int fz,
+                                                       T* rc, int first, int stride, T* tile, T* rs, uint8_t* fl,
+                                                       const ACC& acc) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
-  pdl_wait();
-  if (stopped(flags, maxit)) return;
-  __shared__ T tile[TSN];
-  __shared__ T rs[BR3];
-  __shared__ uint8_t fl[BR3];
-  double part[1] = {0.0};
+  double part = 0.0;
   const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
-  for (int brick = blockIdx.x; brick < F.nbrick; brick += gridDim.x) {
+  for (int brick = first; brick < F.nbrick; brick += stride) {
     uint32_t code[CPT];
     T bv[CPT];
 #pragma unroll
     for (int q = 0; q < CPT; ++q) {
       const int c = brick * BR3 + threadIdx.x + q * NTH;
       code[q] = F.code[c];
-      bv[q] = b[c];
+      bv[q] = acc.ld(b, c);
     }
     fill_halo<T, NTH>(F, brick, tile, X);
     __syncthreads();
@@ -423,7 +476,7 @@ __global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __
         T diag, off;
         full_row<T>(F, code[q], tile, brick, c, X, diag, off);
         T bc = bv[q];
-        if (bmean) bc = bc - static_cast<T>(*bmean);
+        if (bmean) bc = bc - static_cast<T>(ldv<ACC::kCG>(bmean));
         r = bc - (diag * tile[tpos_local(l)] - off);
       }
       rs[l] = r;
@@ -438,8 +491,8 @@ __global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __
       if (oct < 0) {
         for (int t = threadIdx.x; t < BR3; t += NTH) {
           const T val = fl[t] ? rs[t] : T(0);
-          rc[cb * BR3 + t] = val;
-          part[0] += wc * static_cast<double>(val);
+          acc.st(rc, cb * BR3 + t, val);
+          part += wc * static_cast<double>(val);
         }
       } else {
         for (int t = threadIdx.x; t < 64; t += NTH) {
@@ -457,8 +510,8 @@ __global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __
               }
           const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
           const int ci = (oct & 1) * 4 + lci, cj = ((oct >> 1) & 1) * 4 + lcj, ck = (oct >> 2) * 4 + lck;
-          rc[cb * BR3 + ((ck << 6) | (cj << 3) | ci)] = val;
-          part[0] += wc * static_cast<double>(val);
+          acc.st(rc, cb * BR3 + ((ck << 6) | (cj << 3) | ci), val);
+          part += wc * static_cast<double>(val);
         }
       }
     } else {
@@ -480,13 +533,29 @@ __global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __
                 }
               }
           const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
-          rc[cell_index(C, gci, gcj, gck)] = val;
-          part[0] += static_cast<double>(val);
+          acc.st(rc, cell_index(C, gci, gcj, gck), val);
+          part += static_cast<double>(val);
         }
       }
     }
     __syncthreads();
   }
+  return part;
+}
+
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __restrict__ b,
+                                                        const double* bmean, XFetch<T> X, LevelView C,
+                                                        int fx, int fy, int fz, T* __restrict__ rc,
+                                                        RedBuf rb, double* mean_out, double inv_nfluid_c,
+                                                        const SolveFlags* flags, int maxit) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;
+  __shared__ T tile[TSN];
+  __shared__ T rs[BR3];
+  __shared__ uint8_t fl[BR3];
+  double part[1] = {resid_restrict_bricks<T, NTH>(F, b, bmean, X, C, fx, fy, fz, rc, blockIdx.x, gridDim.x, tile,
+                                                  rs, fl, GAcc{})};
   if (mean_out) {
     grid_reduce<1>(part, rb, [=] __device__(const double* tt) { *mean_out = tt[0] * inv_nfluid_c; });
   }
@@ -516,14 +585,10 @@ __device__ __forceinline__ void bsum2_bcast(double& v0, double& v1, double* sh) 
   v1 = sh[65];
 }
 
-template <typename T>
-__global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restrict__ b,
-                                                  const double* bmean, T* __restrict__ xout,
-                                                  int singular, double tol, int maxit_cg,
-                                                  const SolveFlags* flags, int maxit) {
-  pdl_wait();
-  if (stopped(flags, maxit)) return;
-  extern __shared__ double sm[];
+// One CTA; `sm` holds coarse_smem(cells) bytes; `acc` addresses b and xout.
+template <typename T, class ACC>
+__device__ __forceinline__ void coarse_cg_body(const LevelView& C, const T* b, const double* bmean, T* xout,
+                                               int singular, double tol, int maxit_cg, double* sm, const ACC& acc) {
   const int n = C.nx * C.ny * C.nz;
   const bool pre = n <= COARSE_PRE_CELLS;
   double* xs = sm;
@@ -581,7 +646,7 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
     }
   };
   // load
-  double bm = bmean ? *bmean : 0.0;
+  double bm = bmean ? ldv<ACC::kCG>(bmean) : 0.0;
   int nf_local = 0;
   for (int m = tid; m < n; m += blockDim.x) {
     int i, j, k;
@@ -590,7 +655,7 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
     const bool f = C.type[gidx] == CELL_FLUID;
     fl[m] = f;
     nf_local += f;
-    rh[m] = f ? static_cast<double>(b[gidx]) - (bmean ? bm : 0.0) : 0.0;
+    rh[m] = f ? static_cast<double>(acc.ld(b, gidx)) - (bmean ? bm : 0.0) : 0.0;
     xs[m] = 0.0;
   }
   __syncthreads();
@@ -719,8 +784,19 @@ __global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restri
     int i, j, k;
     lex_coords(m, i, j, k);
     const double v = (singular && fl[m]) ? xs[m] - mean : xs[m];
-    xout[cell_index(C, i, j, k)] = static_cast<T>(v);
+    acc.st(xout, cell_index(C, i, j, k), static_cast<T>(v));
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_coarse_cg(LevelView C, const T* __restrict__ b,
+                                                  const double* bmean, T* __restrict__ xout,
+                                                  int singular, double tol, int maxit_cg,
+                                                  const SolveFlags* flags, int maxit) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;
+  extern __shared__ double sm[];
+  coarse_cg_body<T>(C, b, bmean, xout, singular, tol, maxit_cg, sm, GAcc{});
 }
 
 // ---------------------------------------------------------------------------
@@ -774,6 +850,150 @@ __global__ void __launch_bounds__(NT) k_coarse_direct(LevelView C, const T* __re
     const int q = lexpos[m];
     xout[lexcell[m]] = static_cast<T>(q >= 0 ? (singular ? xs[q] - mean : xs[q]) : 0.0);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster-resident V-cycle tail. The coarse end of every V-cycle (the levels
+// from the first one of at most `tail_bricks` bricks down to the coarsest
+// solve) costs one launch and a chain of dependent global loads per sweep
+// when each sweep is its own kernel, whatever the level's size. Here one
+// thread-block cluster of up to 16 CTAs runs all of it with every vector of
+// those levels resident in the cluster's distributed shared memory (brick g in
+// CTA g mod cs): each phase (sweep, residual + restriction, coarsest solve) is
+// the launch path's own per-brick code over bricks rank, rank + cs, ...,
+// reading neighbours and parents from the owning CTA's shared memory, and the
+// phases are separated by the cluster's hardware barrier (barrier.cluster
+// arrive.release / wait.acquire). The tail level's rhs is loaded from global
+// memory at the start and its result stored back at the end. Pending means
+// stay in global memory, summed over the CTAs' partials in rank order. Every
+// CTA executes the same barriers: no CTA waits on a flag.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ XFetchT<T, const LevelView*, DAcc> tail_fetch(const TailFetch& f, const LevelView* lv,
+                                                                         const DAcc& acc) {
+  return XFetchT<T, const LevelView*, DAcc>{static_cast<const T*>(f.x), f.xmean, static_cast<const T*>(f.ec),
+                                            f.ecmean, f.clvl >= 0 ? lv + f.clvl : lv, f.fx, f.fy, f.fz, f.xfb,
+                                            f.xfo, acc};
+}
+
+// Exact coarsest solve spread over the cluster: every CTA stages the rhs, CTA
+// r forms the rows of warps r * nwarp + w, ... into the (global) scratch
+// vector, and after a cluster barrier every CTA scatters its share of the level.
+template <typename T>
+__device__ __forceinline__ void tail_direct(const TailProg* prog, const LevelView& C, const TailPhase& ph, int rank,
+                                           int cs, cg::cluster_group& cl, double* rh, double* red, const DAcc& acc) {
+  const int nf = prog->nf, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const T* b = static_cast<const T*>(ph.b);
+  const double bm = ph.bmean ? ldv<true>(ph.bmean) : 0.0;
+  double s = 0.0;
+  for (int q = tid; q < nf; q += blockDim.x) {
+    const double v = static_cast<double>(acc.ld(b, prog->fmap[q])) - bm;
+    rh[q] = v;
+    s += v;
+  }
+  if (prog->singular && nf > 0) {  // poisson.cpp:160-178 (rhs projected to zero mean)
+    const double mean = bsum_bcast(s, red) / nf;
+    for (int q = tid; q < nf; q += blockDim.x) rh[q] -= mean;
+  }
+  __syncthreads();
+  double* xs = prog->xs;
+  for (int q = rank * nwarp + warp; q < nf; q += cs * nwarp) {
+    const double* row = prog->inv + static_cast<size_t>(q) * nf;
+    double acc_r = 0.0;
+    for (int c = lane; c < nf; c += 32) acc_r += row[c] * rh[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc_r += __shfl_down_sync(0xffffffffu, acc_r, off);
+    if (lane == 0) xs[q] = acc_r;
+  }
+  cl.sync();
+  double mean = 0.0;
+  if (prog->singular && nf > 0) {
+    double t = 0.0;
+    for (int q = tid; q < nf; q += blockDim.x) t += __ldcg(xs + q);
+    mean = bsum_bcast(t, red) / nf;
+  }
+  const int n = C.nx * C.ny * C.nz;
+  T* xout = static_cast<T*>(ph.out);
+  for (int m = rank * static_cast<int>(blockDim.x) + tid; m < n; m += cs * static_cast<int>(blockDim.x)) {
+    const int q = prog->lexpos[m];
+    const double v = q >= 0 ? __ldcg(xs + q) : 0.0;
+    acc.st(xout, prog->lexcell[m], static_cast<T>(q >= 0 && prog->singular ? v - mean : v));
+  }
+}
+
+// Copies this CTA's bricks (rank, rank + cs, ... of nbrick) between a global
+// vector and its arena array at byte offset `off`.
+template <typename T, bool TO_ARENA>
+__device__ __forceinline__ void tail_copy(T* global, char* arena, uintptr_t off, int nbrick, int rank, int lcs) {
+  T* local = reinterpret_cast<T*>(arena + (off - kArenaBias));
+  for (int g = rank; g < nbrick; g += 1 << lcs)
+    for (int l = threadIdx.x; l < BR3; l += blockDim.x) {
+      if constexpr (TO_ARENA) local[((g >> lcs) << 9) + l] = global[g * BR3 + l];
+      else global[g * BR3 + l] = local[((g >> lcs) << 9) + l];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_vtail(const TailProg* __restrict__ prog, const SolveFlags* flags, int maxit) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;  // the same answer in every CTA: nothing writes the flags meanwhile
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = static_cast<int>(cl.block_rank()), cs = static_cast<int>(cl.num_blocks());
+  __shared__ LevelView slv[MAX_TAIL_LEV];
+  __shared__ TailPhase sph[MAX_TAIL_PH];
+  __shared__ T tile[TSN];
+  __shared__ T rs[BR3];
+  __shared__ uint8_t fl[BR3];
+  __shared__ double red[128];
+  __shared__ double cpart;
+  extern __shared__ __align__(128) char dsm[];  // [arena | coarsest-solve scratch]
+  const int nlev = prog->nlev, nph = prog->nphase, lcs = prog->lcs;
+  const DAcc acc{dsm, lcs};
+  double* scratch = reinterpret_cast<double*>(dsm + prog->arena_bytes);
+  {
+    const int* src = reinterpret_cast<const int*>(prog->lv);
+    int* dst = reinterpret_cast<int*>(slv);
+    for (int i = threadIdx.x; i < nlev * static_cast<int>(sizeof(LevelView) / 4); i += blockDim.x) dst[i] = src[i];
+    src = reinterpret_cast<const int*>(prog->ph);
+    dst = reinterpret_cast<int*>(sph);
+    for (int i = threadIdx.x; i < nph * static_cast<int>(sizeof(TailPhase) / 4); i += blockDim.x) dst[i] = src[i];
+  }
+  tail_copy<T, true>(static_cast<T*>(prog->b_in), dsm, prog->b_enc, prog->nbrick, rank, lcs);
+  cl.sync();
+  for (int p = 0; p < nph; ++p) {
+    const TailPhase& ph = sph[p];
+    const LevelView& L = slv[ph.lvl];
+    double part = 0.0;
+    if (ph.op == TAIL_SMOOTH) {
+      part = smooth_bricks<T, NT>(L, static_cast<const T*>(ph.b), ph.bmean, tail_fetch<T>(ph.X, slv, acc),
+                                  static_cast<T*>(ph.out), static_cast<T>(ph.c2), static_cast<T>(ph.c1), ph.prev_mode,
+                                  tail_fetch<T>(ph.P, slv, acc), rank, cs, tile, acc);
+    } else if (ph.op == TAIL_RESID) {
+      part = resid_restrict_bricks<T, NT>(L, static_cast<const T*>(ph.b), ph.bmean, tail_fetch<T>(ph.X, slv, acc),
+                                          slv[ph.clvl], ph.fx, ph.fy, ph.fz, static_cast<T*>(ph.out), rank, cs, tile,
+                                          rs, fl, acc);
+    } else if (ph.op == TAIL_DIRECT) {
+      tail_direct<T>(prog, L, ph, rank, cs, cl, scratch, red, acc);
+    } else if (rank == 0) {  // TAIL_CG: CgPoisson(1e-6, 500) on one CTA
+      coarse_cg_body<T>(L, static_cast<const T*>(ph.b), ph.bmean, static_cast<T*>(ph.out), prog->singular, 1e-6, 500,
+                        scratch, acc);
+    }
+    if (ph.mean_out) {
+      double a[1] = {part};
+      block_reduce<1>(a, red);
+      if (threadIdx.x == 0) cpart = a[0];
+    }
+    cl.sync();
+    if (ph.mean_out) {
+      if (rank == 0 && threadIdx.x == 0) {
+        double t = 0.0;
+        for (int r = 0; r < cs; ++r) t += *cl.map_shared_rank(&cpart, r);
+        *ph.mean_out = t * ph.inv_nf;
+      }
+      cl.sync();
+    }
+  }
+  tail_copy<T, false>(static_cast<T*>(prog->x_out), dsm, prog->x_enc, prog->nbrick, rank, lcs);
 }
 
 // ---------------------------------------------------------------------------
@@ -1469,6 +1689,7 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
   sweeps_ = precision_ == NB_PRECISION_MIXED ? std::min(std::max(t.sweeps, 1), 3) : 2;  // FP64: V(2,2) as the reference
   halo_mode_ = t.halo_mode == 1 ? 1 : 0;
   direct_max_ = std::min(std::max(t.coarse_direct_max, 0), 512);
+  tail_bricks_ = std::min(std::max(t.tail_bricks, 0), 4096);
   // Smoother coefficients per sweep of a phase: damped Jacobi (the reference's,
   // c2 = omega) or, mixed form only, Chebyshev on [lmax / 6, lmax] of D^-1 A
   // with lmax = 2.05 above the Gershgorin bound 2 (three-term recurrence:
@@ -1509,6 +1730,7 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc, const
     upload_uniform(lv_[l], bcs);
   }
   common_alloc();
+  build_tail();
 }
 
 // Composite hierarchy: MG level m+1 merges the finest octree level of level m
@@ -1577,6 +1799,7 @@ MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc, co
   // Below a multi-level mesh (no reference hierarchy to reproduce) the
   // coarsest level is solved exactly instead of by CgPoisson(1e-6, 500).
   if (fine.tree.nlev > 1) build_dense_coarse();
+  build_tail();
 }
 
 MgSolver::~MgSolver() {
@@ -1595,9 +1818,17 @@ void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
 
 // One V-cycle at level `lvl` on rhs b (pending mean slot bmean_slot or -1).
 // Returns the level's x buffer and the slot of its pending mean (-1 if none).
+// With `prog`, every launch below is appended to prog as a cluster-tail phase
+// (same arguments) instead of being issued.
 template <typename T>
 void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, void* /*unused*/,
-                      int* out_mean_slot, void** out_x) {
+                      int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog) {
+  if (!prog && lvl == tail_lvl_) {
+    launch_tail(s);
+    *out_x = tail_x_;
+    *out_mean_slot = tail_slot_;
+    return;
+  }
   DevLevel& D = lv_[lvl];
   const LevelView& L = D.v;
   const T* b = static_cast<const T*>(bv);
@@ -1605,18 +1836,40 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const int grid = grid_of(L.nbrick);
   const double tsz = sizeof(T);
   const double ncell = D.ncell;
+  const int rl = lvl - tail_lvl_;  // tail-relative level (prog only)
+  // Records a phase (prog) or runs the launch.
+#define MG_EMIT(fam, nbytes, phase, launch)           \
+  do {                                                \
+    if (prog) {                                       \
+      prog->push_back(phase);                         \
+      tail_bytes_ += static_cast<double>(nbytes);     \
+    } else {                                          \
+      NB_LAUNCH(lc_, fam, s, nbytes, launch);         \
+    }                                                 \
+  } while (0)
+  const auto fetch = [&](const XFetch<T>& f, int clvl) {
+    return TailFetch{f.x, f.xmean, f.ec, f.ecmean, f.ec ? clvl : -1, f.fx, f.fy, f.fz, f.xfb, f.xfo};
+  };
   if (lvl + 1 == static_cast<int>(lv_.size())) {
     const size_t nco = static_cast<size_t>(L.nx) * L.ny * L.nz;
+    TailPhase ph{};
+    ph.op = dense_ ? TAIL_DIRECT : TAIL_CG;
+    ph.lvl = rl;
+    ph.clvl = -1;
+    ph.b = b;
+    ph.bmean = bmean;
+    ph.X.clvl = ph.P.clvl = -1;
+    ph.out = D.x0;
     if (dense_) {
-      NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1) + 8.0 * dense_nf_ * dense_nf_,
-                launch_pdl(pdl_, k_coarse_direct<T>, dim3(1), dim3(NT), 2 * sizeof(double) * dense_nf_, s, L, b, bmean,
-                           static_cast<T*>(D.x0), dense_inv_, dense_fmap_, dense_lexpos_, dense_lexcell_,
-                           dense_nf_, singular_ ? 1 : 0, flags_, maxit_));
+      MG_EMIT("coarse_cg", ncell * (2 * tsz + 1) + 8.0 * dense_nf_ * dense_nf_, ph,
+              launch_pdl(pdl_, k_coarse_direct<T>, dim3(1), dim3(NT), 2 * sizeof(double) * dense_nf_, s, L, b, bmean,
+                         static_cast<T*>(D.x0), dense_inv_, dense_fmap_, dense_lexpos_, dense_lexcell_, dense_nf_,
+                         singular_ ? 1 : 0, flags_, maxit_));
     } else {
       const size_t smem = coarse_smem(nco);
-      NB_LAUNCH(lc_, "coarse_cg", s, ncell * (2 * tsz + 1),
-                (launch_pdl(pdl_, k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0),
-                            singular_ ? 1 : 0, 1e-6, 500, flags_, maxit_)));
+      MG_EMIT("coarse_cg", ncell * (2 * tsz + 1), ph,
+              (launch_pdl(pdl_, k_coarse_cg<T>, dim3(1), dim3(NT), smem, s, L, b, bmean, static_cast<T*>(D.x0),
+                          singular_ ? 1 : 0, 1e-6, 500, flags_, maxit_)));
     }
     *out_x = D.x0;
     *out_mean_slot = -1;
@@ -1642,42 +1895,231 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   int cur = 0;
   const XFetch<T> none{nullptr, nullptr, nullptr, nullptr, dummy, 1, 1, 1};
   auto plain = [&](int i) { return XFetch<T>{buf[i], mean[i], nullptr, nullptr, dummy, 1, 1, 1}; };
+  const auto smooth_phase = [&](const XFetch<T>& X, T* out, double* mout, double c2, double c1, int pm,
+                                const XFetch<T>& P) {
+    TailPhase ph{};
+    ph.op = TAIL_SMOOTH;
+    ph.lvl = rl;
+    ph.clvl = rl + 1;
+    ph.prev_mode = pm;
+    ph.b = b;
+    ph.bmean = bmean;
+    ph.X = fetch(X, rl + 1);
+    ph.P = fetch(P, rl + 1);
+    ph.out = out;
+    ph.mean_out = mout;
+    ph.inv_nf = inv_nf;
+    ph.c2 = c2;
+    ph.c1 = c1;
+    return ph;
+  };
   // pre-smoothing (sweeps_ sweeps; 2 as the reference), the first from x = 0
-  NB_LAUNCH(lc_, "smooth", s, ncell * (2 * tsz + 1),
-            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, none, buf[cur], rb_, mean[cur],
-                        inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+  MG_EMIT("smooth", ncell * (2 * tsz + 1), smooth_phase(none, buf[cur], mean[cur], cheb_c2_[0], 0.0, 0, none),
+          (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, none, buf[cur], rb_, mean[cur], inv_nf,
+                      flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)  // a Chebyshev step from sweep 2 on also reads x_prev
-    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + (cheb_ && sw >= 2 ? ncell * tsz : 0.0),
-              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
-                          mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
-                          static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1))));
+    MG_EMIT("smooth", ncell * (3 * tsz + 1) + (cheb_ && sw >= 2 ? ncell * tsz : 0.0),
+            smooth_phase(plain(cur), buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[sw], cheb_c1_[sw],
+                         cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1)),
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
+                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
+                        static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1))));
   // residual + restriction
   const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
   double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
-  NB_LAUNCH(lc_, "resid_restrict", s, ncell * (2 * tsz + 1) + ncoarse * tsz,
+  {
+    TailPhase ph{};
+    ph.op = TAIL_RESID;
+    ph.lvl = rl;
+    ph.clvl = rl + 1;
+    ph.b = b;
+    ph.bmean = bmean;
+    ph.X = fetch(plain(cur), -1);
+    ph.P = fetch(none, -1);
+    ph.out = Cd.b;
+    ph.mean_out = cmean;
+    ph.inv_nf = inv_nfc;
+    ph.fx = Cd.h.fx;
+    ph.fy = Cd.h.fy;
+    ph.fz = Cd.h.fz;
+    MG_EMIT("resid_restrict", ncell * (2 * tsz + 1) + ncoarse * tsz, ph,
             (launch_pdl(pdl_, kr, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                         XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, C, Cd.h.fx, Cd.h.fy,
                         Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_)));
+  }
   void* ec = nullptr;
   int ec_slot = -1;
-  vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec);
+  vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec, prog);
   const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
   // post-smoothing: the first sweep folds in the prolongation x += P e
   const XFetch<T> prolonged{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
                             Cd.h.fz, D.d_xfb, D.d_xfo};
-  NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz,
-            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
-                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+  MG_EMIT("smooth", ncell * (3 * tsz + 1) + ncoarse * tsz,
+          smooth_phase(prolonged, buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[0], 0.0, 0, none),
+          (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
+                      mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
   cur ^= 1;
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)  // Chebyshev: x_prev, after the prolongation with its coarse value
-    NB_LAUNCH(lc_, "smooth", s,
-              ncell * (3 * tsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0),
-              (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
-                          mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
-                          static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1))));
+    MG_EMIT("smooth", ncell * (3 * tsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0),
+            smooth_phase(plain(cur), buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[sw], cheb_c1_[sw], cheb_ ? 1 : 0,
+                         sw == 1 ? prolonged : plain(cur ^ 1)),
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
+                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
+                        static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1))));
+#undef MG_EMIT
   *out_x = buf[cur];
   *out_mean_slot = sing ? lvl_slot(lvl, cur) : -1;
+}
+
+// Records the V-cycle from the first level (>= 1, above the coarsest) of at
+// most tail_bricks_ bricks as one cluster program, with the levels' vectors
+// placed in the CTAs' shared-memory arenas, when the device can hold the
+// cluster; otherwise leaves the per-sweep launches in place.
+void MgSolver::build_tail() {
+  tail_lvl_ = -1;
+  const int last = static_cast<int>(lv_.size()) - 1;
+  if (tail_bricks_ <= 0) return;
+  int t = -1;
+  for (int l = 1; l < last; ++l)
+    if (lv_[l].h.nbrick <= tail_bricks_) {
+      t = l;
+      break;
+    }
+  if (t < 0 || last - t + 1 > MAX_TAIL_LEV) return;
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  const size_t tsz = mixed ? sizeof(float) : sizeof(double);
+  const size_t nco = static_cast<size_t>(lv_[last].v.nx) * lv_[last].v.ny * lv_[last].v.nz;
+  const size_t scratch = dense_ ? sizeof(double) * dense_nf_ : coarse_smem(nco);
+  const void* fn = mixed ? reinterpret_cast<const void*>(k_vtail<float>) : reinterpret_cast<const void*>(k_vtail<double>);
+  int dev = 0, optin = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  NB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  NB_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  // Arena of cluster size cs: b, x0, x1 of every tail level, ceil(nbrick / cs)
+  // bricks each, 128-byte aligned.
+  const auto arena_of = [&](int cs, std::vector<size_t>* offs) {
+    size_t off = 0;
+    for (int l = t; l <= last; ++l) {
+      const size_t slots = static_cast<size_t>((lv_[l].h.nbrick + cs - 1) / cs);
+      for (int v = 0; v < 3; ++v) {
+        if (offs) offs->push_back(off);
+        off += (slots * BR3 * tsz + 127) / 128 * 128;
+      }
+    }
+    return off;
+  };
+  int lcs = 4;
+  while (lcs > 1 && (1 << lcs) > lv_[t].h.nbrick) --lcs;
+  size_t smem = 0;
+  for (; lcs >= 1; --lcs) {  // largest power-of-two cluster the device schedules
+    const int cs = 1 << lcs;
+    smem = arena_of(cs, nullptr) + scratch;
+    if (fa.sharedSizeBytes + smem > static_cast<size_t>(optin)) continue;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) == cudaSuccess && nclusters > 0) break;
+    (void)cudaGetLastError();
+  }
+  if (lcs < 1) return;
+  const int cs = 1 << lcs;
+  std::vector<size_t> offs;
+  const size_t arena = arena_of(cs, &offs);
+  std::vector<TailPhase> ph;
+  tail_lvl_ = t;
+  tail_bytes_ = 0.0;
+  const int bslot = (singular_ && lv_[t].h.nfluid > 0) ? lvl_slot(t, 2) : -1;
+  if (mixed) vcycle<float>(nullptr, t, lv_[t].b, bslot, nullptr, &tail_slot_, &tail_x_, &ph);
+  else vcycle<double>(nullptr, t, lv_[t].b, bslot, nullptr, &tail_slot_, &tail_x_, &ph);
+  tail_lvl_ = -1;
+  if (ph.size() > static_cast<size_t>(MAX_TAIL_PH)) return;
+  // global vector -> arena encoding
+  bool ok = true;
+  const auto enc = [&](const void* g) -> uintptr_t {
+    if (!g) return 0;
+    for (int l = t; l <= last; ++l) {
+      const void* v[3] = {lv_[l].b, lv_[l].x0, lv_[l].x1};
+      for (int k = 0; k < 3; ++k)
+        if (v[k] == g) return offs[3 * (l - t) + k] + kArenaBias;
+    }
+    ok = false;
+    return 0;
+  };
+  const auto encp = [&](const void* g) { return reinterpret_cast<void*>(enc(g)); };
+  for (TailPhase& q : ph) {
+    q.b = encp(q.b);
+    q.out = encp(q.out);
+    for (TailFetch* f : {&q.X, &q.P}) {
+      f->x = encp(f->x);
+      f->ec = encp(f->ec);
+    }
+  }
+  TailProg h{};
+  h.nlev = last - t + 1;
+  h.nphase = static_cast<int>(ph.size());
+  h.singular = singular_ ? 1 : 0;
+  h.nf = dense_ ? dense_nf_ : 0;
+  h.lcs = lcs;
+  h.nbrick = lv_[t].h.nbrick;
+  h.arena_bytes = arena;
+  h.b_in = lv_[t].b;
+  h.b_enc = enc(lv_[t].b);
+  h.x_out = tail_x_;
+  h.x_enc = enc(tail_x_);
+  if (!ok) return;
+  h.inv = dense_inv_;
+  h.fmap = dense_fmap_;
+  h.lexpos = dense_lexpos_;
+  h.lexcell = dense_lexcell_;
+  h.xs = dense_ ? static_cast<double*>(alloc(sizeof(double) * std::max(dense_nf_, 1))) : nullptr;
+  for (int l = 0; l < h.nlev; ++l) h.lv[l] = lv_[t + l].v;
+  for (size_t i = 0; i < ph.size(); ++i) h.ph[i] = ph[i];
+  tail_prog_ = static_cast<TailProg*>(alloc(sizeof(TailProg)));
+  NB_CUDA(cudaMemcpy(tail_prog_, &h, sizeof(TailProg), cudaMemcpyHostToDevice));
+  tail_lvl_ = t;
+  tail_cs_ = cs;
+  tail_smem_ = smem;
+}
+
+void MgSolver::launch_tail(cudaStream_t s) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(tail_cs_);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = tail_smem_;
+  cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = tail_cs_;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_ ? 2 : 1;
+  const TailProg* prog = tail_prog_;
+  if (precision_ == NB_PRECISION_MIXED)
+    NB_LAUNCH(lc_, "vtail", s, tail_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vtail<float>, prog, flags_, maxit_)));
+  else
+    NB_LAUNCH(lc_, "vtail", s, tail_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vtail<double>, prog, flags_, maxit_)));
 }
 
 // Minv: z = V-cycle(r) (+ Minv's removeMean), then either p = z, rz = r.z
@@ -1877,7 +2319,9 @@ void MgSolver::solve(cudaStream_t s, const double* b, double tol, int maxit) {
   solve_async(s, b, tol, maxit);
 }
 
-template void MgSolver::vcycle<double>(cudaStream_t, int, const void*, int, void*, int*, void**);
-template void MgSolver::vcycle<float>(cudaStream_t, int, const void*, int, void*, int*, void**);
+template void MgSolver::vcycle<double>(cudaStream_t, int, const void*, int, void*, int*, void**,
+                                       std::vector<TailPhase>*);
+template void MgSolver::vcycle<float>(cudaStream_t, int, const void*, int, void*, int*, void**,
+                                      std::vector<TailPhase>*);
 
 }  // namespace nb

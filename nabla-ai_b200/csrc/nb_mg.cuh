@@ -37,6 +37,54 @@ struct DevLevel {
   void* x1 = nullptr;
 };
 
+// Cluster-resident V-cycle tail: one launch runs the V-cycle from level
+// `tail_lvl` down (sweeps, residual + restriction, coarsest solve), phase by
+// phase, on one thread-block cluster.
+constexpr int MAX_TAIL_LEV = 8;
+constexpr int MAX_TAIL_PH = 64;
+enum TailOp : int { TAIL_SMOOTH = 0, TAIL_RESID = 1, TAIL_DIRECT = 2, TAIL_CG = 3 };
+// A level vector as the launch path's fetch reads it (pending mean and
+// prolongation); clvl is the tail-relative coarse level, -1 none.
+struct TailFetch {
+  const void* x;
+  const double* xmean;
+  const void* ec;
+  const double* ecmean;
+  int clvl, fx, fy, fz;
+  const int* xfb;
+  const int* xfo;
+};
+struct TailPhase {
+  int op, lvl, clvl, prev_mode;  // lvl / clvl: tail-relative level and its coarser level
+  const void* b;
+  const double* bmean;
+  TailFetch X, P;
+  void* out;          // smoothed x, restricted residual, or coarsest x
+  double* mean_out;   // pending mean of `out` (nullptr: none)
+  double inv_nf;
+  double c2, c1;
+  int fx, fy, fz, pad;
+};
+// Vector pointers in the phases are arena encodings (byte offset in every
+// CTA's shared-memory arena + 128), not device addresses.
+struct TailProg {
+  int nlev, nphase, singular, nf;
+  int lcs;            // log2 of the cluster size
+  int nbrick;         // bricks of the tail level
+  size_t arena_bytes;  // per CTA
+  void* b_in;         // tail level's rhs (global), loaded into arena array b_enc
+  uintptr_t b_enc;
+  void* x_out;        // tail level's result (global), stored from arena array x_enc
+  uintptr_t x_enc;
+  const double* inv;  // exact coarsest solve (TAIL_DIRECT)
+  const int* fmap;
+  const int* lexpos;
+  const int* lexcell;
+  double* xs;  // [nf] scratch
+  LevelView lv[MAX_TAIL_LEV];
+  TailPhase ph[MAX_TAIL_PH];
+};
+
 class MgSolver {
  public:
   // `tune` sets launch shapes, halo staging, mixed-form sweeps, the exact
@@ -87,9 +135,12 @@ class MgSolver {
   RedBuf red() const { return rb_; }
 
  private:
+  // With `prog` the launches are recorded as tail phases instead (no stream).
   template <typename T>
   void vcycle(cudaStream_t s, int lvl, const void* b, int bmean_slot, void* xout_final,
-              int* out_mean_slot, void** out_x);
+              int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog = nullptr);
+  void build_tail();
+  void launch_tail(cudaStream_t s);
   void iterate(cudaStream_t s, double tol, int maxit, int count);
   void setup(cudaStream_t s, const double* b, double tol, int maxit);
   void finish(cudaStream_t s, double* report);
@@ -107,6 +158,14 @@ class MgSolver {
   int sweeps_ = 2;     // smoothing sweeps per side of the coarse correction
   int halo_mode_ = 0;  // 0 per-brick neighbour maps, 1 per-cell walk
   int direct_max_ = 256;  // exact coarsest solve up to this many cells
+  int tail_bricks_ = 0;   // cluster tail from the first level (>= 1) of at most this many bricks; 0 off
+  int tail_lvl_ = -1;     // first level of the tail (-1: no tail)
+  int tail_cs_ = 0;       // CTAs of the tail's cluster
+  size_t tail_smem_ = 0;  // dynamic shared memory of the tail (coarsest solve)
+  TailProg* tail_prog_ = nullptr;  // device
+  void* tail_x_ = nullptr;         // tail level's result and its pending-mean slot
+  int tail_slot_ = -1;
+  double tail_bytes_ = 0.0;        // algorithmic bytes of one tail launch
   bool cheb_ = false;     // mixed form: Chebyshev smoothing instead of damped Jacobi
   double cheb_c2_[4] = {0.8, 0.8, 0.8, 0.8};  // residual weight per sweep of a phase
   double cheb_c1_[4] = {0.0, 0.0, 0.0, 0.0};  // weight of the last step per sweep

@@ -3,9 +3,9 @@
 //
 // The tuned choices change launch shapes (threads per brick and CTAs per SM),
 // the multigrid halo staging, the mixed form's smoother and sweeps, the exact
-// coarse-solve threshold and PDL.
+// coarse-solve threshold, the cluster-resident V-cycle tail and PDL.
 // None of them changes the discretisation: FP64 results move only by the
-// summation order of the grid reductions (grid size), mixed results by the
+// summation order of the grid reductions (grid size, cluster tail), mixed results by the
 // preconditioner (sweeps, coarse solve) within the solve tolerance.
 //
 // The autotuner times candidates on scratch copies of a sample case with
@@ -37,6 +37,7 @@ bool tuning_ok(const nb_tuning& t, std::string& why) {
   else if (t.threads_per_brick != 128 && t.threads_per_brick != 256 && t.threads_per_brick != 512)
     why = "threads_per_brick must be 128, 256 or 512";
   else if (t.smoother != 0 && t.smoother != 1) why = "smoother must be 0 or 1";
+  else if (t.tail_bricks < 0 || t.tail_bricks > 4096) why = "tail_bricks must be in 0..4096";
   else return true;
   return false;
 }
@@ -59,11 +60,11 @@ std::string tune_key(nb_ctx* ctx, const nb_case* c) {
   return s;
 }
 
-// One cache line: key and the eight fields, then ms per step.
+// One cache line: key and the nine fields, then ms per step.
 bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double& ms) {
   std::istringstream in(line);
   if (!(in >> key >> t.mg_ctas_per_sm >> t.rhs_ctas_per_sm >> t.halo_mode >> t.sweeps >> t.coarse_direct_max >>
-        t.pdl >> t.threads_per_brick >> t.smoother >> ms))
+        t.pdl >> t.threads_per_brick >> t.smoother >> t.tail_bricks >> ms))
     return false;
   std::string why;
   return tuning_ok(t, why);
@@ -71,9 +72,9 @@ bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double&
 
 std::string format_line(const std::string& key, const nb_tuning& t, double ms) {
   char buf[320];
-  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
+  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
                 t.rhs_ctas_per_sm, t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, t.smoother,
-                ms);
+                t.tail_bricks, ms);
   return buf;
 }
 
@@ -97,6 +98,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->pdl = 1;
   t->threads_per_brick = 512;
   t->smoother = 1;
+  t->tail_bricks = 8;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {
@@ -270,7 +272,8 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
     int32_t nb_tuning::*field;
     std::vector<int32_t> values;
   };
-  std::vector<Knob> knobs = {{&nb_tuning::rhs_ctas_per_sm, {1, 2, 3, 4}},
+  std::vector<Knob> knobs = {{&nb_tuning::tail_bricks, {0, 8, 32, 128}},
+                             {&nb_tuning::rhs_ctas_per_sm, {1, 2, 3, 4}},
                              {&nb_tuning::halo_mode, {0, 1}},
                              {&nb_tuning::pdl, {0, 1}}};
   if (prec == NB_PRECISION_MIXED) {

@@ -135,6 +135,7 @@ class Tuning(C.Structure):
         ("pdl", C.c_int32),
         ("threads_per_brick", C.c_int32),
         ("smoother", C.c_int32),
+        ("tail_bricks", C.c_int32),
     ]
 
     def as_dict(self):
