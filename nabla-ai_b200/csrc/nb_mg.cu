@@ -1997,7 +1997,11 @@ void MgSolver::build_tail() {
   NB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   cudaFuncAttributes fa{};
   NB_CUDA(cudaFuncGetAttributes(&fa, fn));
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+  // The dynamic shared-memory limit is a property of the kernel, shared by all
+  // solvers: set it to the device maximum once rather than to this solver's need.
+  const int dyn_max = optin - static_cast<int>(fa.sharedSizeBytes);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) != cudaSuccess) {
     (void)cudaGetLastError();
     return;
   }
@@ -2020,11 +2024,7 @@ void MgSolver::build_tail() {
   for (; lcs >= 1; --lcs) {  // largest power-of-two cluster the device schedules
     const int cs = 1 << lcs;
     smem = arena_of(cs, nullptr) + scratch;
-    if (fa.sharedSizeBytes + smem > static_cast<size_t>(optin)) continue;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
-      (void)cudaGetLastError();
-      continue;
-    }
+    if (smem > static_cast<size_t>(dyn_max)) continue;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(cs);
     cfg.blockDim = dim3(NT);

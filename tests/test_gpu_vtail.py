@@ -107,3 +107,15 @@ def test_singular_three_level_box_whole_hierarchy_in_the_tail(ctx, precision, to
     scale = max(np.abs(ref[a]).max() for a in range(3))
     for a in range(3):
         assert np.abs(got[a] - ref[a]).max() <= tol * scale
+
+
+def test_cases_with_different_tail_sizes_coexist(ctx):
+    """The tail kernel's shared-memory limit is shared by every solver: a case
+    whose tail needs more shared memory must still step after a case with a
+    smaller tail was built."""
+    g, cfg = cases.taylor_green(32)
+    big = solver.NSSolver(g, cfg, ctx=ctx)  # tail: 8 + 1 bricks and the CG scratch
+    big.set_state(*cases.taylor_green_state(g))
+    assert big.step(0.05).converged
+    _channel_run(ctx, abi.PRECISION_FP64, nsteps=1)  # tail: 2 + 1 bricks, exact solve
+    assert big.step(0.05).converged
