@@ -45,7 +45,7 @@ UNIT = "Mcell-steps/s"
 # (profiles/channel3_launches_and_captures.md: 40 consecutive k_smooth launches).
 NCU_TRAFFIC = {("channel3", "smooth"): 1.463e6}
 FAMILIES = ["rhs_rk", "smooth", "resid_restrict", "coarse_cg", "vtail", "pcg_matvec", "pcg_update",
-            "pcg_center", "pcg_mean", "pcg_dots", "pcg_dir", "div", "correct", "diag", "sync"]
+            "pcg_center", "pcg_mean", "pcg_dots", "div", "correct", "diag", "sync"]
 
 
 # ---------------------------------------------------------------------------

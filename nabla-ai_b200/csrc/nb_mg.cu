@@ -357,14 +357,26 @@ __device__ __forceinline__ void full_row(const LevelView& L, uint32_t code, cons
 // Optionally reduces the fluid sum of xout into `mean_out` (= sum / nfluid)
 // for the next removeMean.
 // ---------------------------------------------------------------------------
-// Bricks first, first + stride, ... of one sweep; returns this thread's part
-// of the weighted fluid sum of xout. `acc` addresses b and xout.
-template <typename T, int NTH, class ACC, class FX, class FP>
-__device__ __forceinline__ double smooth_bricks(const LevelView& L, const T* b, const double* bmean, const FX& X,
-                                               T* xout, T c2, T c1, int prev_mode, const FP& P, int first,
-                                               int stride, T* tile, const ACC& acc) {
-  constexpr int CPT = BR3 / NTH;  // cells per thread
+// Where a sweep's result goes: xout (addressed by acc) and this thread's part
+// of the weighted fluid sum for the next removeMean.
+template <typename T, class ACC>
+struct SweepOut {
+  T* xout;
+  const ACC& acc;
   double part = 0.0;
+  __device__ __forceinline__ void operator()(int c, double wgt, T out, bool fluid) {
+    if (fluid) part += wgt * static_cast<double>(out);
+    acc.st(xout, c, out);
+  }
+};
+
+// Bricks first, first + stride, ... of one sweep; every cell's result goes
+// to out(c, weight, value, fluid). `acc` addresses b.
+template <typename T, int NTH, class ACC, class FX, class FP, class OUT>
+__device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, const double* bmean, const FX& X,
+                                             OUT& sink, T c2, T c1, int prev_mode, const FP& P, int first,
+                                             int stride, T* tile, const ACC& acc) {
+  constexpr int CPT = BR3 / NTH;  // cells per thread
   const bool staged = X.x || X.ec;
   for (int brick = first; brick < L.nbrick; brick += stride) {
     uint32_t code[CPT];
@@ -383,7 +395,8 @@ __device__ __forceinline__ double smooth_bricks(const LevelView& L, const T* b, 
       const int l = threadIdx.x + q * NTH;
       const int c = brick * BR3 + l;
       T out = T(0);
-      if (code_type(code[q]) == CELL_FLUID) {
+      const bool fluid = code_type(code[q]) == CELL_FLUID;
+      if (fluid) {
         T diag, off, xc;
         if (staged) {
           full_row<T>(L, code[q], tile, brick, c, X, diag, off);
@@ -416,13 +429,20 @@ __device__ __forceinline__ double smooth_bricks(const LevelView& L, const T* b, 
           }
           out = out + c1 * (xc - xp);
         }
-        part += wgt * static_cast<double>(out);
       }
-      acc.st(xout, c, out);
+      sink(c, wgt, out, fluid);
     }
     __syncthreads();
   }
-  return part;
+}
+
+// Flexible beta of the PCG (multigrid.cpp:330-338) from t = {z'.rnew, z'.r}.
+__device__ __forceinline__ void flex_beta(const double* t, double* S, SolveFlags* flags) {
+  S[S_RNEWZ] = t[0];
+  S[S_RZCROSS] = t[1];
+  S[S_BETA] = (t[0] - t[1]) / S[S_RZ];
+  S[S_RZ] = t[0];
+  flags->iters += 1;
 }
 
 template <typename T, int NTH>
@@ -434,11 +454,45 @@ __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
-  double part[1] = {smooth_bricks<T, NTH>(L, b, bmean, X, xout, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile,
-                                          GAcc{})};
+  const GAcc acc{};
+  SweepOut<T, GAcc> sink{xout, acc};
+  smooth_bricks<T, NTH>(L, b, bmean, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, acc);
   if (mean_out) {
+    double part[1] = {sink.part};
     grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
   }
+}
+
+// The last post-smoothing sweep of level 0 on a non-singular system, fused
+// with the PCG dots that follow it (k_pcg_dots, first = 0): z' = fluid ? z :
+// 0 goes to zo (FP64) and z'.rnew, z'.r are reduced in the same pass, cell for
+// cell in k_pcg_dots' order, into the flexible beta.
+template <typename T>
+struct DotsOut {
+  double* zo;
+  const double* rnew;
+  const double* r;
+  double part[2] = {0.0, 0.0};
+  __device__ __forceinline__ void operator()(int c, double wgt, T out, bool fluid) {
+    const double v = fluid ? static_cast<double>(out) : 0.0;
+    zo[c] = v;
+    part[0] += wgt * (v * rnew[c]);
+    part[1] += wgt * (v * r[c]);
+  }
+};
+
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) k_smooth_dots(LevelView L, const T* __restrict__ b, XFetch<T> X,
+                                                     double* __restrict__ zo, const double* __restrict__ rnew,
+                                                     const double* __restrict__ r, RedBuf rb, double* S,
+                                                     SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
+                                                     XFetch<T> P) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;
+  __shared__ T tile[TSN];
+  DotsOut<T> sink{zo, rnew, r};
+  smooth_bricks<T, NTH>(L, b, nullptr, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, GAcc{});
+  grid_reduce<2>(sink.part, rb, [=] __device__(const double* t) { flex_beta(t, S, flags); });
 }
 
 // ---------------------------------------------------------------------------
@@ -965,9 +1019,11 @@ __global__ void __launch_bounds__(NT) k_vtail(const TailProg* __restrict__ prog,
     const LevelView& L = slv[ph.lvl];
     double part = 0.0;
     if (ph.op == TAIL_SMOOTH) {
-      part = smooth_bricks<T, NT>(L, static_cast<const T*>(ph.b), ph.bmean, tail_fetch<T>(ph.X, slv, acc),
-                                  static_cast<T*>(ph.out), static_cast<T>(ph.c2), static_cast<T>(ph.c1), ph.prev_mode,
-                                  tail_fetch<T>(ph.P, slv, acc), rank, cs, tile, acc);
+      SweepOut<T, DAcc> sink{static_cast<T*>(ph.out), acc};
+      smooth_bricks<T, NT>(L, static_cast<const T*>(ph.b), ph.bmean, tail_fetch<T>(ph.X, slv, acc), sink,
+                           static_cast<T>(ph.c2), static_cast<T>(ph.c1), ph.prev_mode, tail_fetch<T>(ph.P, slv, acc),
+                           rank, cs, tile, acc);
+      part = sink.part;
     } else if (ph.op == TAIL_RESID) {
       part = resid_restrict_bricks<T, NT>(L, static_cast<const T*>(ph.b), ph.bmean, tail_fetch<T>(ph.X, slv, acc),
                                           slv[ph.clvl], ph.fx, ph.fy, ph.fz, static_cast<T*>(ph.out), rank, cs, tile,
@@ -1136,38 +1192,37 @@ __global__ void __launch_bounds__(NT) k_pcg_dots(LevelView L, const TZ* __restri
   grid_reduce<2>(part, rb, [=] __device__(const double* t) {
     if (first) {
       S[S_RZ] = t[0];
+      S[S_BETA] = 0.0;  // the first matvec's direction is p = z' + 0 p
     } else {
-      S[S_RNEWZ] = t[0];
-      S[S_RZCROSS] = t[1];
-      S[S_BETA] = (t[0] - t[1]) / S[S_RZ];
-      S[S_RZ] = t[0];
-      flags->iters += 1;
+      flex_beta(t, S, flags);
     }
   });
 }
 
-// p = z' + beta p (multigrid.cpp:335-337).
-__global__ void __launch_bounds__(NT) k_pcg_dir(LevelView L, const double* __restrict__ z,
-                                                double* __restrict__ p, const double* S,
-                                                const SolveFlags* flags, int maxit) {
-  pdl_wait();
-  if (stopped(flags, maxit)) return;
-  const double beta = S[S_BETA];
-  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
-    const int c = brick * BR3 + threadIdx.x;
-    p[c] = z[c] + beta * p[c];
-  }
-}
+// The search direction p = z' + beta p_old (multigrid.cpp:335-337) as the
+// matvec stages it: every CTA forms it for its own cells and its halo with
+// the same fma, and the owner stores it.
+struct DirFetch {
+  const double* z;
+  const double* p;
+  double beta;
+  __device__ __forceinline__ double operator()(int n, int, int, int) const { return fma(beta, p[n], z[n]); }
+  __device__ __forceinline__ bool prolongs() const { return false; }
+  __device__ __forceinline__ double at(int n, int, int, int) const { return fma(beta, p[n], z[n]); }
+};
 
-// Ap = A p ; S_PAP = p.Ap ; alpha = rz / pAp or breakdown (multigrid.cpp:303-308).
+// p = z' + beta p_old into pnew ; Ap = A p ; S_PAP = p.Ap ; alpha = rz / pAp
+// or breakdown (multigrid.cpp:303-308, 335-337). pold and pnew alternate from
+// one cycle to the next, so no CTA reads a direction another CTA overwrote.
 template <int NTH>
-__global__ void __launch_bounds__(NTH) k_pcg_matvec(LevelView L, const double* __restrict__ p,
+__global__ void __launch_bounds__(NTH) k_pcg_matvec(LevelView L, const double* __restrict__ z,
+                                                    const double* __restrict__ pold, double* __restrict__ pnew,
                                                     double* __restrict__ Ap, RedBuf rb, double* S,
                                                     SolveFlags* flags, int maxit) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   pdl_wait();
   if (stopped(flags, maxit)) return;
-  DFetch X{p, nullptr};
+  const DirFetch X{z, pold, S[S_BETA]};
   __shared__ double tile[TSN];
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -1175,8 +1230,10 @@ __global__ void __launch_bounds__(NTH) k_pcg_matvec(LevelView L, const double* _
     double pv[CPT];
 #pragma unroll
     for (int q = 0; q < CPT; ++q) {
-      code[q] = L.code[brick * BR3 + threadIdx.x + q * NTH];
-      pv[q] = p[brick * BR3 + threadIdx.x + q * NTH];
+      const int c = brick * BR3 + threadIdx.x + q * NTH;
+      code[q] = L.code[c];
+      pv[q] = X(c, 0, 0, 0);
+      pnew[c] = pv[q];
     }
     fill_halo<double, NTH>(L, brick, tile, X);
     __syncthreads();
@@ -1648,7 +1705,7 @@ void MgSolver::common_alloc() {
     throw ApiError{NB_ERR_UNSUPPORTED, "multigrid hierarchy deeper than " + std::to_string(MAX_LEVELS) + " levels"};
   if (halo_mode_ == 0) build_halo_maps();
   n0_ = static_cast<size_t>(lv_[0].h.nbrick) * BR3;
-  double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &Ap_, &xfin_};
+  double** vecs[] = {&rhs_, &x_, &r_, &rnew_, &z_, &p_, &p2_, &Ap_, &xfin_};
   for (double** v : vecs) {
     *v = static_cast<double*>(alloc(n0_ * sizeof(double)));
     NB_CUDA(cudaMemset(*v, 0, n0_ * sizeof(double)));
@@ -1955,18 +2012,35 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   // post-smoothing: the first sweep folds in the prolongation x += P e
   const XFetch<T> prolonged{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
                             Cd.h.fz, D.d_xfb, D.d_xfo};
-  MG_EMIT("smooth", ncell * (3 * tsz + 1) + ncoarse * tsz,
-          smooth_phase(prolonged, buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[0], 0.0, 0, none),
-          (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
-                      mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+  const bool dots_here = !prog && lvl == 0 && fuse_dots_;  // level 0's last sweep forms z' and the PCG dots
+  const auto kd = tpb_ == 128 ? k_smooth_dots<T, 128> : (tpb_ == 256 ? k_smooth_dots<T, 256> : k_smooth_dots<T, 512>);
+  if (dots_here && sweeps_ == 1) {
+    NB_LAUNCH(lc_, "smooth", s, ncell * (3 * tsz + 1) + ncoarse * tsz - ncell * tsz + ncell * 24,
+              (launch_pdl(pdl_, kd, dim3(grid), dim3(tpb_), 0, s, L, b, prolonged, z_, rnew_, r_, rb_, S_, flags_,
+                          maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+  } else {
+    MG_EMIT("smooth", ncell * (3 * tsz + 1) + ncoarse * tsz,
+            smooth_phase(prolonged, buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[0], 0.0, 0, none),
+            (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
+                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+  }
   cur ^= 1;
-  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)  // Chebyshev: x_prev, after the prolongation with its coarse value
-    MG_EMIT("smooth", ncell * (3 * tsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0),
+  for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1) {  // Chebyshev: x_prev, after the prolongation with its coarse value
+    const double bytes = ncell * (3 * tsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0);
+    if (dots_here && sw + 1 == sweeps_) {  // + z' and the PCG dots (no xout)
+      NB_LAUNCH(lc_, "smooth", s, bytes - ncell * tsz + ncell * 24,
+                (launch_pdl(pdl_, kd, dim3(grid), dim3(tpb_), 0, s, L, b, plain(cur), z_, rnew_, r_, rb_, S_, flags_,
+                            maxit_, static_cast<T>(cheb_c2_[sw]), static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0,
+                            sw == 1 ? prolonged : plain(cur ^ 1))));
+      continue;
+    }
+    MG_EMIT("smooth", bytes,
             smooth_phase(plain(cur), buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[sw], cheb_c1_[sw], cheb_ ? 1 : 0,
                          sw == 1 ? prolonged : plain(cur ^ 1)),
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
                         mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
                         static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1))));
+  }
 #undef MG_EMIT
   *out_x = buf[cur];
   *out_mean_slot = sing ? lvl_slot(lvl, cur) : -1;
@@ -2134,10 +2208,11 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   const double zsz = mixed ? 4.0 : 8.0;
   const auto km = tpb_ == 128 ? k_pcg_matvec<128> : (tpb_ == 256 ? k_pcg_matvec<256> : k_pcg_matvec<512>);
   for (int k = 0; k < count; ++k) {
-    NB_LAUNCH(lc_, "pcg_matvec", s, n * 17,
-              launch_pdl(pdl_, km, dim3(grid), dim3(tpb_), 0, s, L, p_, Ap_, rb_, S_, flags_, maxit));
+    // p_ holds the last direction, p2_ receives this cycle's (swapped below)
+    NB_LAUNCH(lc_, "pcg_matvec", s, n * 33,
+              launch_pdl(pdl_, km, dim3(grid), dim3(tpb_), 0, s, L, z_, p_, p2_, Ap_, rb_, S_, flags_, maxit));
     NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0)),
-              (launch_pdl(pdl_, k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
+              (launch_pdl(pdl_, k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p2_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
                                                 sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol)));
     if (sing) {
       NB_LAUNCH(lc_, "pcg_center", s, n * (17 + (mixed ? 4 : 0)),
@@ -2146,8 +2221,16 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
     }
     void* zx = nullptr;
     int zslot = -1;
+    // non-singular: the V-cycle's last sweep also forms z' and the dots
+    fuse_dots_ = !sing;
     if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
     else vcycle<double>(s, 0, rnew_, -1, nullptr, &zslot, &zx);
+    fuse_dots_ = false;
+    std::swap(p_, p2_);
+    if (!sing) {
+      std::swap(r_, rnew_);
+      continue;
+    }
     const double* m1 = (sing && zslot >= 0) ? S_ + zslot : nullptr;
     const double* m2 = sing ? S_ + S_ZMEAN2 : nullptr;
     if (sing) {
@@ -2168,7 +2251,6 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
       NB_LAUNCH(lc_, "pcg_dots", s, n * (zsz + 8 * 3 + 1),
                 (launch_pdl(pdl_, k_pcg_dots<double>, dim3(grid), dim3(NT), 0, s,L, static_cast<const double*>(zx), m1, m2, z_, p_,
                                                         rnew_, r_, 0, rb_, S_, flags_, maxit)));
-    NB_LAUNCH(lc_, "pcg_dir", s, n * 24, launch_pdl(pdl_, k_pcg_dir, dim3(grid), dim3(NT), 0, s, L, z_, p_, S_, flags_, maxit));
     std::swap(r_, rnew_);
   }
   NB_CUDA(cudaGetLastError());

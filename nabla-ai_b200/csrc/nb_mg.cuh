@@ -189,7 +189,8 @@ class MgSolver {
   size_t n0_ = 0;  // level-0 slots (nbrick * 512)
   // level-0 PCG vectors (FP64)
   double *rhs_ = nullptr, *x_ = nullptr, *r_ = nullptr, *rnew_ = nullptr, *z_ = nullptr,
-         *p_ = nullptr, *Ap_ = nullptr, *xfin_ = nullptr;
+         *p_ = nullptr, *p2_ = nullptr, *Ap_ = nullptr, *xfin_ = nullptr;  // p_ / p2_: last / next direction
+  bool fuse_dots_ = false;  // level 0's last post-sweep also forms z' and the PCG dots (non-singular)
   float* rnew_f_ = nullptr;  // mixed form: FP32 copy of the V-cycle input
   float* z_f_ = nullptr;     // mixed form: FP32 V-cycle output
   double* S_ = nullptr;
