@@ -245,8 +245,15 @@ class AmrCase:
             raise ValueError(f"state sizes {[x.size for x in arrs]} != {list(self.sizes)}")
         self.ctx.check(self.ctx.lib.nb_amr_case_set_state(self.h, *[abi.dptr(x) for x in arrs]), "set_state")
 
-    def get_state(self):
-        out = [np.zeros(n) for n in self.sizes]
+    def get_state(self, out=None):
+        """Face velocities and pressure in the case's layout. `out`: four
+        contiguous float64 arrays of the right sizes to copy into (pinned
+        buffers make the read-back one DMA per array, no host copy)."""
+        if out is None:
+            out = [np.zeros(n) for n in self.sizes]
+        elif [x.size for x in out] != list(self.sizes) or not all(
+                x.dtype == np.float64 and x.flags.c_contiguous and x.flags.writeable for x in out):
+            raise ValueError("get_state: out must be four writeable contiguous float64 arrays of the state sizes")
         self.ctx.check(self.ctx.lib.nb_amr_case_get_state(self.h, *[abi.dptr(x) for x in out]), "get_state")
         return out
 

@@ -176,9 +176,18 @@ class NSSolver:
         self.ctx.check(self.ctx.lib.nb_case_set_state(self.h, *[abi.dptr(a) for a in arrs], step, t,
                                                       dt_last), "setState")
 
-    def get_state(self):
-        nu, nv, nw, np_ = self.grid.sizes()
-        u, v, w, p = np.zeros(nu), np.zeros(nv), np.zeros(nw), np.zeros(np_)
+    def get_state(self, out=None):
+        """u, v, w, p in the reference's MAC layout. `out`: four contiguous
+        float64 arrays of the right sizes to copy into (pinned buffers make
+        the read-back one DMA per array, no host copy)."""
+        sizes = list(self.grid.sizes())
+        if out is None:
+            out = [np.zeros(n) for n in sizes]
+        elif [a.size for a in out] != sizes or not all(
+                a.dtype == np.float64 and a.flags.c_contiguous and a.flags.writeable for a in out):
+            raise NablaError(abi.NB_ERR_BAD_ARG, "get_state: out must be four writeable contiguous float64 arrays "
+                                                 "of the state sizes")
+        u, v, w, p = out
         self.ctx.check(self.ctx.lib.nb_case_get_state(self.h, abi.dptr(u), abi.dptr(v), abi.dptr(w),
                                                       abi.dptr(p)), "get_state")
         return u, v, w, p

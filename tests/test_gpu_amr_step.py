@@ -179,6 +179,12 @@ def test_amr_graph_and_direct_paths_agree_bitwise(ctx):
     assert ra.poisson_iters == rb.poisson_iters
     for x, y in zip(a.get_state(), b.get_state()):
         assert np.array_equal(x, y)
+    # read-back into caller buffers gives the same arrays
+    outs = [np.full(n, np.nan) for n in b.sizes]
+    for x, o in zip(b.get_state(), b.get_state(outs)):
+        assert np.array_equal(x, o)
+    with pytest.raises(ValueError):
+        b.get_state(outs[:3] + [outs[3][:-1]])
 
 
 def test_two_level_mixed_tracks_fp64(ctx):

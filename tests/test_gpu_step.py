@@ -134,6 +134,15 @@ def test_state_roundtrip_and_errors(ctx):
     for x, y in zip(ns.get_state(), st):
         assert np.array_equal(x, y)
     assert ns.clock() == (3, 0.5, 0.1)
+    # read-back into caller buffers (the end-to-end path uses pinned ones)
+    outs = [np.full(x.size, np.nan) for x in st]
+    got = ns.get_state(outs)
+    for x, o, y in zip(got, outs, st):
+        assert x is o and np.array_equal(o, y)
+    with pytest.raises(solver.NablaError):
+        ns.get_state([o[:-1] for o in outs])
+    with pytest.raises(solver.NablaError):
+        ns.get_state([o.astype(np.float32) for o in outs])
     with pytest.raises(solver.NablaError):
         ns.set_state(st[0][:-1], *st[1:])
     bad = cases.Grid(0, 4, 4, 1.0, 1.0, 1.0)
