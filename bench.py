@@ -620,7 +620,8 @@ def run_serve(args, rank, world, local_rank):
     for name, prec in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
         reqs = serve_requests(args, 7 + rank)
         with ClockSampler(local_rank) as clk:
-            st = serving.Server(ctx, hbm_budget=150e9, precision=prec, slots=args.slots).run(
+            st = serving.Server(ctx, hbm_budget=150e9, precision=prec, slots=args.slots,
+                                builders=args.builders).run(
                 reqs, time_limit=args.serve_seconds * 2)
         s = st.summary()
         s["clocks"] = clk.summary()
@@ -635,8 +636,8 @@ def run_serve(args, rank, world, local_rank):
         "config": {"workload": f"serving: Poisson arrivals at {args.rate}/s for {args.serve_seconds} s, each request "
                                f"an octree TGV box (<= {args.max_cells} leaf cells) for {args.min_steps}-"
                                f"{args.max_steps} steps, HBM budget 150 GB, continuous batching "
-                               f"(per-case step graphs overlapped on the device, {args.slots} slots); the loop "
-                               "runs for twice the arrival window",
+                               f"(per-case step graphs overlapped on the device, {args.slots} slots, cases built "
+                               f"on {args.builders} host threads); the loop runs for twice the arrival window",
                    "precision": args.precision or "mixed"},
         "latency": {"p50_s": round(primary["p50_latency_s"], 4), "p99_s": round(primary["p99_latency_s"], 4)},
         "forms": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items() if kk != "clocks"}
@@ -761,6 +762,7 @@ def main():
     ap.add_argument("--max-steps", type=int, default=40)
     ap.add_argument("--max-cells", type=int, default=300_000, help="serve: leaf-cell cap per request")
     ap.add_argument("--slots", type=int, default=32, help="serve: cases in flight at most")
+    ap.add_argument("--builders", type=int, default=2, help="serve: host threads that build admitted cases")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)
