@@ -1749,7 +1749,8 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
   tail_bricks_ = std::min(std::max(t.tail_bricks, 0), 4096);
   // Smoother coefficients per sweep of a phase: damped Jacobi (the reference's,
   // c2 = omega) or, mixed form only, Chebyshev on [lmax / 6, lmax] of D^-1 A
-  // with lmax = 2.05 above the Gershgorin bound 2 (three-term recurrence:
+  // with lmax = 2, the Gershgorin bound (every row of D^-1 A has diagonal 1
+  // and off-diagonal magnitudes summing to at most 1) (three-term recurrence:
   // theta = (lmax + lmin) / 2, delta = (lmax - lmin) / 2, sigma = theta / delta,
   // rho_0 = 1 / sigma, rho_k = 1 / (2 sigma - rho_(k-1)); sweep 0 steps by
   // r / theta, sweep k by 2 rho_k / delta r + rho_k rho_(k-1) times the last step).
@@ -1759,7 +1760,7 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
     cheb_c1_[k] = 0.0;
   }
   if (cheb_) {
-    const double lmax = 2.05, lmin = lmax / 6.0;
+    const double lmax = 2.0, lmin = lmax / 6.0;
     const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
     double rho = 1.0 / sigma;
     cheb_c2_[0] = 1.0 / theta;
