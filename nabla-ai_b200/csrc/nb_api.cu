@@ -299,16 +299,32 @@ void download_lex(nb_case& c, int comp, const double* src, double* host) {
 
 // NSSolver::project (core/src/flow/ns_solver.cpp:475-579) on the current fields.
 // Graph form: the MG-PCG cycle loop is a device-side conditional node.
+// Mixed form with warm_start: the projection of RK stage `stage` starts from
+// the pressure the last projection left (p = phi / dt), scaled to this
+// stage's potential: the stage potentials are about dt P, dt P / 4 and
+// 2 dt P / 3 for a pressure P (the divergence of the stage's u* is that of
+// dt R, dt R / 4 and 2 dt R / 3), so p holds 2 P / 3 before stage 1 (the last
+// step's stage 3), P before stage 2 and P / 4 before stage 3. The FP64 form
+// starts from 0 as the reference does.
+const WarmStart* warm_start(const nb_case& c, int stage, WarmStart* ws) {
+  if (c.precision != NB_PRECISION_MIXED || !c.ctx->tune.warm_start) return nullptr;
+  static constexpr double kAlpha[3] = {1.5, 0.25, 8.0 / 3.0};
+  *ws = WarmStart{c.p, &c.d_blk->dt, kAlpha[stage]};
+  return ws;
+}
+
 void project(nb_case& c, double* const* f, int stage, bool direct) {
   StepBlock* blk = c.d_blk;
+  WarmStart wsv;
+  const WarmStart* ws = warm_start(c, stage, &wsv);
   apply_bc(c, f, true);
   flow_launch(c, "div", ncell_of(c) * 33, [&] { launch_div(c.stream, c.F, f[0], f[1], f[2], c.b); });
   if (direct) {
-    c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage]);
+    c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage], ws);
   } else {
     uint64_t nbody = 0;
     c.mg->capture_solve(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage],
-                        &nbody);
+                        &nbody, ws);
     c.body_kernels = nbody;
   }
   flow_launch(c, "correct", ncell_of(c) * 65,
@@ -354,14 +370,16 @@ void amr_bc(nb_case& c, double* const* f, bool outflow) {
 // NSSolver::project (ns_solver.cpp:475-579) on the composite mesh.
 void project_amr(nb_case& c, double* const* f, int stage, bool direct) {
   StepBlock* blk = c.d_blk;
+  WarmStart wsv;
+  const WarmStart* ws = warm_start(c, stage, &wsv);
   amr_bc(c, f, true);
   flow_launch(c, "div", ncell_of(c) * 33, [&] { launch_amr_div(c.stream, c.AF, f[0], f[1], f[2], c.b); });
   if (direct) {
-    c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage]);
+    c.mg->solve_async(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage], ws);
   } else {
     uint64_t nbody = 0;
     c.mg->capture_solve(c.stream, c.b, c.cfg.poisson_tol, c.cfg.poisson_max_iters, blk->rep[stage],
-                        &nbody);
+                        &nbody, ws);
     c.body_kernels = nbody;
   }
   flow_launch(c, "correct", ncell_of(c) * 65,

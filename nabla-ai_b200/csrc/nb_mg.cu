@@ -1158,6 +1158,62 @@ __global__ void __launch_bounds__(NT) k_pcg_setup(LevelView L, const double* __r
   });
 }
 
+// Setup from an initial guess: x = fluid ? scale * guess : 0 with scale =
+// alpha * (*dt), r = rhs - A x (rhs as k_pcg_setup forms it), the same |rhs|^2
+// and early exit (the stopping test stays relative to |rhs|).
+struct ScaledFetch {
+  const double* g;
+  double s;
+  __device__ __forceinline__ double operator()(int n, int, int, int) const { return s * g[n]; }
+  __device__ __forceinline__ bool prolongs() const { return false; }
+  __device__ __forceinline__ double at(int n, int, int, int) const { return s * g[n]; }
+};
+
+__global__ void __launch_bounds__(NT) k_pcg_setup_warm(LevelView L, const double* __restrict__ b,
+                                                       const double* bmean, const double* __restrict__ guess,
+                                                       const double* __restrict__ dtp, double alpha,
+                                                       double* __restrict__ rhs, double* __restrict__ r,
+                                                       double* __restrict__ x, float* __restrict__ r_f, RedBuf rb,
+                                                       double* S, SolveFlags* flags, double tol) {
+  pdl_wait();
+  const ScaledFetch X{guess, alpha * *dtp};
+  __shared__ double tile[TSN];
+  double part[1] = {0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    fill_halo<double>(L, brick, tile, X);
+    __syncthreads();
+    const int c = brick * BR3 + threadIdx.x;
+    const uint32_t code = L.code[c];
+    double v = 0.0, xv = 0.0, rv = 0.0;
+    if (code_type(code) == CELL_FLUID) {
+      v = bmean ? b[c] - *bmean : b[c];
+      double diag, off;
+      full_row<double>(L, code, tile, brick, c, X, diag, off);
+      xv = tile[tpos_local(threadIdx.x)];
+      rv = v - (diag * xv - off);
+    }
+    rhs[c] = v;
+    r[c] = rv;
+    x[c] = xv;
+    if (r_f) r_f[c] = static_cast<float>(rv);
+    part[0] += cell_weight(L, brick) * (v * v);
+    __syncthreads();
+  }
+  grid_reduce<1>(part, rb, [=] __device__(const double* t) {
+    S[S_BNORM2] = t[0];
+    const double bnorm = sqrt(t[0]) + 1e-300;
+    flags->iters = 0;
+    flags->nan = isnan(t[0]) ? 1 : 0;
+    if (sqrt(t[0]) <= tol * bnorm || isnan(t[0])) {
+      flags->stop = 1;
+      flags->early = 1;
+    } else {
+      flags->stop = 0;
+      flags->early = 0;
+    }
+  });
+}
+
 // z' = fluid ? (z - m1) - m2 : 0 (the smoother's last removeMean, then Minv's,
 // multigrid.cpp:283-288); written to zo (FP64). With `first`, p = z' and
 // S_RZ = r.z'; otherwise S_RNEWZ = z'.rnew, S_RZCROSS = z'.r and the finaliser
@@ -2257,8 +2313,9 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
   NB_CUDA(cudaGetLastError());
 }
 
-void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxit, double* report) {
-  setup(s, b, tol, maxit);
+void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxit, double* report,
+                           const WarmStart* ws) {
+  setup(s, b, tol, maxit, ws);
   // Iterate in batches; every kernel returns at once after convergence, so
   // over-issuing costs only launch latency. The batch grows geometrically.
   int issued = 0, batch = 4;
@@ -2278,8 +2335,8 @@ void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxi
 // cycles (so the r/rnew buffers return to their captured roles) and then sets
 // the loop condition on the device. Must be called while `s` is capturing.
 void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int maxit, double* report,
-                             uint64_t* body_kernels) {
-  setup(s, b, tol, maxit);
+                             uint64_t* body_kernels, const WarmStart* ws) {
+  setup(s, b, tol, maxit, ws);
   cudaStreamCaptureStatus st;
   cudaGraph_t g;
   const cudaGraphNode_t* deps = nullptr;
@@ -2346,7 +2403,7 @@ nb_poisson_report MgSolver::report_from(const double* r, double tol) {
   return rep;
 }
 
-void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit) {
+void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit, const WarmStart* ws) {
   tol_ = tol;
   maxit_ = maxit;
   const LevelView& L = lv_[0].v;
@@ -2359,8 +2416,12 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit) {
     k_fluid_mean<<<grid, NT, 0, s>>>(L, b, nullptr, rb_, S_ + S_BSUM, inv_nf, nullptr, maxit);
     lc_.add();
   }
-  k_pcg_setup<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, rhs_, r_, x_,
-                                  mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);
+  if (ws)
+    k_pcg_setup_warm<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, ws->guess, ws->dt, ws->alpha, rhs_,
+                                         r_, x_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);
+  else
+    k_pcg_setup<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, rhs_, r_, x_,
+                                    mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);
   lc_.add();
   // z = Minv(r) ; p = z ; rz = r.z
   void* zx = nullptr;

@@ -85,6 +85,15 @@ struct TailProg {
   TailPhase ph[MAX_TAIL_PH];
 };
 
+// Initial guess of a solve (instead of x = 0): x0 = alpha * (*dt) * guess on
+// the fluid cells of level 0 (brick layout), e.g. the last projection's
+// pressure scaled to this projection's potential.
+struct WarmStart {
+  const double* guess;
+  const double* dt;  // device scalar
+  double alpha;
+};
+
 class MgSolver {
  public:
   // `tune` sets launch shapes, halo staging, mixed-form sweeps, the exact
@@ -104,7 +113,7 @@ class MgSolver {
   // Same but leaves the report on the device (no host synchronisation);
   // read it later with fetch_report().
   void solve_async(cudaStream_t s, const double* b_dev, double tol, int maxit,
-                   double* report = nullptr);
+                   double* report = nullptr, const WarmStart* ws = nullptr);
   nb_poisson_report fetch_report(cudaStream_t s);
   // Issues the whole solve into stream `s`, which must be capturing a graph:
   // the cycle loop becomes a conditional WHILE node (no host round trip).
@@ -112,7 +121,7 @@ class MgSolver {
   // flag, |rhs|^2, |true residual|^2 and the NaN flag. `body_kernels`
   // receives the kernel count of one loop-body execution.
   void capture_solve(cudaStream_t s, const double* b_dev, double tol, int maxit, double* report,
-                     uint64_t* body_kernels);
+                     uint64_t* body_kernels, const WarmStart* ws = nullptr);
   static nb_poisson_report report_from(const double* r, double tol);
   // Number of loop-body executions so far (device counter).
   unsigned long long* body_execs() const { return body_execs_; }
@@ -142,7 +151,7 @@ class MgSolver {
   void build_tail();
   void launch_tail(cudaStream_t s);
   void iterate(cudaStream_t s, double tol, int maxit, int count);
-  void setup(cudaStream_t s, const double* b, double tol, int maxit);
+  void setup(cudaStream_t s, const double* b, double tol, int maxit, const WarmStart* ws = nullptr);
   void finish(cudaStream_t s, double* report);
   void upload_uniform(DevLevel& D, const int bcs[6]);
   void upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]);

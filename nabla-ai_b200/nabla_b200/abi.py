@@ -136,6 +136,7 @@ class Tuning(C.Structure):
         ("threads_per_brick", C.c_int32),
         ("smoother", C.c_int32),
         ("tail_bricks", C.c_int32),
+        ("warm_start", C.c_int32),
     ]
 
     def as_dict(self):
