@@ -209,8 +209,8 @@ typedef struct nb_tuning {
                                 below the finest with at most n bricks down to the
                                 coarsest solve runs as one thread-block-cluster
                                 launch with those levels in shared memory (0..4096) */
-  int32_t warm_start;        /* mixed form: 1 each projection's MG-PCG starts from the
-                                last pressure scaled to the RK stage, 0 (default) from
+  int32_t warm_start;        /* mixed form: 1 (default) each projection's MG-PCG starts
+                                from the last pressure scaled to the RK stage, 0 from
                                 zero; the FP64 form always starts from zero as the
                                 reference does */
 } nb_tuning;

@@ -101,7 +101,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->threads_per_brick = 512;
   t->smoother = 1;
   t->tail_bricks = 8;
-  t->warm_start = 0;
+  t->warm_start = 1;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {

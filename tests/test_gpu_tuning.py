@@ -134,3 +134,27 @@ def test_chebyshev_on_a_singular_uniform_box(ctx, sweeps):
     uc, it_c = run(abi.PRECISION_MIXED, dict(sweeps=sweeps, smoother=1))
     assert np.abs(uc - u64).max() <= 1e-6 * np.abs(u64).max()
     assert it_c <= it_j
+
+
+def test_mixed_warm_start_tracks_fp64_with_fewer_cycles(ctx):
+    """Mixed form with each projection started from the last pressure (scaled
+    to the RK stage): within 1e-6 of the FP64 form, converged, and no more
+    MG-PCG cycles than starting from zero."""
+    def run(tuning, precision=abi.PRECISION_MIXED):
+        ctx.set_tuning(**tuning)
+        try:
+            ac = _channel(ctx, precision)
+            cycles = 0
+            for _ in range(4):
+                rep = ac.step(0.004)
+                assert rep.converged and rep.divergence_max <= 1e-8
+                cycles += rep.poisson_iters
+            return ac.get_state()[:3], cycles
+        finally:
+            ctx.set_tuning(**solver.default_tuning())
+    ref, _ = run({}, abi.PRECISION_FP64)
+    cold, n_cold = run(dict(warm_start=0))
+    warm, n_warm = run(dict(warm_start=1))
+    for a in range(3):
+        assert np.abs(warm[a] - ref[a]).max() <= 1e-6 * np.abs(ref[0]).max()
+    assert n_warm <= n_cold

@@ -14,7 +14,7 @@ def _lib():
 def test_default_tuning():
     assert solver.default_tuning() == {"mg_ctas_per_sm": 4, "rhs_ctas_per_sm": 4, "halo_mode": 0, "sweeps": 2,
                                        "coarse_direct_max": 256, "pdl": 1, "threads_per_brick": 512,
-                                       "smoother": 1, "tail_bricks": 8, "warm_start": 0}
+                                       "smoother": 1, "tail_bricks": 8, "warm_start": 1}
 
 
 def _tuning(**kw):
