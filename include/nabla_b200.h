@@ -409,9 +409,9 @@ nb_status nb_run_case(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_confi
 
 /* ---- allocation-free operator ---------------------------------------------
  * No counterpart in the reference. The same -Laplacian as nb_apply_laplacian,
- * for callers that cannot call cudaMalloc: code issuing work while a stream is
- * captured into a CUDA graph, and hosts that own all device memory through
- * their own arena or budget. `x` and `out` are the caller's DEVICE arrays of
+ * for callers that cannot call cudaMalloc: hosts that own all device memory
+ * through their own arena or admission budget, and loops that must not stall
+ * on the allocator's implicit synchronisation. `x` and `out` are the caller's DEVICE arrays of
  * nx*ny*nz doubles in lexicographic order; `stream` is a cudaStream_t (NULL =
  * legacy default stream) on the current device. No context is needed and
  * nothing is allocated: the solid mask (grid->solid, host memory, or NULL) is

@@ -1,11 +1,12 @@
 // nb_noalloc.cu — the allocation-free variant of the -Laplacian launch.
 //
-// Who it is for: callers that cannot call cudaMalloc — code that issues work
-// while a stream is being captured into a CUDA graph (allocation is not a
-// capturable operation), and hosts that own every byte of device memory
-// through their own arena or admission budget and forbid libraries from
-// allocating behind their back. They hold x and A x in their own device
-// buffers; this entry point allocates nothing.
+// Who it is for: callers that cannot call cudaMalloc — hosts that own every
+// byte of device memory through their own arena or admission budget (a
+// serving process that has already handed its HBM to resident cases, an
+// embedding application with its own pool allocator) and forbid libraries
+// from allocating behind their back, or loops that must not stall on the
+// allocator's implicit device synchronisation. They hold x and A x in their
+// own device buffers; this entry point allocates nothing.
 //
 // The only scratch the kernel needs — the per-cell solid mask, which the
 // caller describes with a host pointer in nb_grid_desc — lives in a
@@ -121,6 +122,7 @@ extern "C" nb_status nb_apply_laplacian_noalloc(const nb_grid_desc* grid, const 
       grid->nx, grid->ny, grid->nz, grid->face[0].type, grid->face[1].type, grid->face[2].type,
       grid->face[3].type, grid->face[4].type, grid->face[5].type, 1.0 / (grid->dx * grid->dx),
       1.0 / (grid->dy * grid->dy), 1.0 / (grid->dz * grid->dz), mask, x, out);
-  if (cudaGetLastError() != cudaSuccess) return NB_ERR_CUDA;
+  // Peek, not get: an error the caller had not read yet stays pending for it.
+  if (cudaPeekAtLastError() != cudaSuccess) return NB_ERR_CUDA;
   return NB_OK;
 }

@@ -1,12 +1,13 @@
 """The allocation-free -Laplacian entry point (nb_apply_laplacian_noalloc).
 
-It serves callers that cannot call cudaMalloc (work issued under stream
-capture; hosts that own all device memory through their own arena). The test
-allocates the caller's device buffers with torch, calls the entry point
-through the C ABI twice in a row with different grids (the second one without
-a solid mask, so the shared static scratch must be fully rewritten), and
-checks each result against the allocating entry point nb_apply_laplacian at
-the operator tolerance used elsewhere (1e-13 relative).
+It serves callers that cannot call cudaMalloc (hosts that own all device
+memory through their own arena or admission budget). The test allocates the
+caller's device buffers with torch, calls the entry point through the C ABI
+three times in a row with different grids (the second one without a solid
+mask, so the shared static scratch must be fully rewritten; the third a 2-D
+grid, nz = 1, which skips the z coupling as the reference's 2-D case does),
+and checks each result against the allocating entry point nb_apply_laplacian
+at the operator tolerance used elsewhere (1e-13 relative).
 
 This file is collected last so a failure here cannot hide other results.
 """
@@ -32,7 +33,7 @@ def _noalloc(lib, desc, x_np):
     return st, od.cpu().numpy()
 
 
-def test_noalloc_matches_allocating_entry_point_twice():
+def test_noalloc_matches_allocating_entry_point_in_a_row():
     ctx = solver.default_context()
     lib = abi.load()
     # call 1: partial bricks, every BC kind, random solids
@@ -50,6 +51,16 @@ def test_noalloc_matches_allocating_entry_point_twice():
     st, got2 = _noalloc(lib, d2, x2)
     assert st == abi.NB_OK
     assert rel_err(got2, solver.apply_a(g2, x2, ctx)) < 1e-13
+    # call 3: 2-D grid (nz = 1), periodic x, inlet / outlet in y, solids
+    from nabla_b200 import cases
+    faces = [dict(type=abi.BC_PERIODIC), dict(type=abi.BC_PERIODIC), dict(type=abi.BC_INLET),
+             dict(type=abi.BC_OUTLET), dict(type=abi.BC_WALL), dict(type=abi.BC_WALL)]
+    g3 = cases.Grid(19, 14, 1, 0.07, 0.05, 0.05, faces=faces)
+    g3.solid[:] = (np.random.default_rng(33).random(g3.ncell) < 0.1).astype(np.uint8)
+    x3 = np.random.default_rng(34).uniform(-1, 1, g3.ncell)
+    st, got3 = _noalloc(lib, g3.desc(), x3)
+    assert st == abi.NB_OK
+    assert rel_err(got3, solver.apply_a(g3, x3, ctx)) < 1e-13
 
 
 def test_noalloc_rejects_oversize_grid():
