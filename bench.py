@@ -33,6 +33,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 REPO = os.path.dirname(os.path.abspath(__file__))
@@ -132,10 +133,10 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="nb_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -153,13 +154,18 @@ class ClockSampler:
             self.proc.terminate()
             self.proc.wait()
             self.f.close()
+        self.lines = open(self.path).read().splitlines() if os.path.exists(self.path) else []
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
 
     def summary(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in self.lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -243,6 +249,8 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         run.step()
     torch.cuda.synchronize()
+    # the state the timed steps start from (the end-to-end pass replays the same trajectory)
+    start = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in run.get_state()]
     # share of each kernel family (one profiled direct-launch step per family, untimed)
     shares = {}
     for fam in (FAMILIES if args.shares else ["smooth"]):
@@ -274,23 +282,25 @@ def run_ours(args, rank, world, local_rank):
     ms, nl, nb = C.c_double(), C.c_uint64(), C.c_double()
     ctx.lib.nb_ctx_profile_read(ctx.h, C.byref(ms), C.byref(nl), C.byref(nb))
     ctx.lib.nb_ctx_profile(ctx.h, None)
-    # end to end through the C ABI with host buffers (pinned)
-    pinned = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in run.get_state()]
-    outs = [torch.empty(a.size, dtype=torch.float64).pin_memory().numpy() for a in pinned]
-    n_e2e = max(2, args.steps // 2)
-    e2e_ms = 0.0
-    for _ in range(n_e2e):
+    # End to end through the C ABI with host buffers (pinned): the same K steps
+    # from the same starting state as the timed region, every step uploading
+    # the state from host memory and reading the stepped state back into it.
+    host = start
+    e2e_ms, e2e_cycles = 0.0, 0
+    for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        run.set_state(*pinned)
-        run.step()
-        run.get_state(outs)  # straight into the pinned buffers
+        run.set_state(*host)
+        r = run.step()
+        run.get_state(host)  # straight back into the pinned buffers
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-    e2e_value = world * cells * n_e2e / (max_over_ranks(e2e_ms, world, device) * 1e-3) / 1e6
+        e2e_cycles += r.poisson_iters
+    e2e_value = world * cells * args.steps / (max_over_ranks(e2e_ms, world, device) * 1e-3) / 1e6
+    pinned = outs = host
     hbm, peak_kind = peaks()
     achieved = (nb.value / (ms.value * 1e-3) / 1e9) if ms.value > 0 else 0.0
     out = {
@@ -302,10 +312,14 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": run.desc, "cells": cells, "precision": precision, "tuning": ctx.tuning,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed between timed steps (256 MiB write); working set < L2",
-                   "poisson_cycles_per_step": reps[-1].poisson_iters},
+                   "poisson_cycles_per_step": reps[-1].poisson_iters,
+                   "poisson_cycles_timed": sum(r.poisson_iters for r in reps)},
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(a.nbytes for a in pinned)),
-                "d2h_bytes_per_step": int(sum(a.nbytes for a in outs))},
+                "d2h_bytes_per_step": int(sum(a.nbytes for a in outs)),
+                "steps": args.steps, "poisson_cycles": e2e_cycles,
+                "trajectory": "the timed steps replayed from the same starting state, state uploaded from and "
+                              "read back to pinned host memory every step"},
         "gpu_launches": int(launches),
         "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 5),
@@ -321,7 +335,42 @@ def run_ours(args, rank, world, local_rank):
     if args.workload == "channel3":
         out["forms"], out["accuracy"] = other_form_and_accuracy(args, ctx, run, prec, precision, value,
                                                                 stream, flush, world, device)
+        if args.same_case_steps > 0:
+            out["same_case_as_reference_arm"] = same_case_as_reference(args, ctx, flush, world, device)
     return out
+
+
+def same_case_as_reference(args, ctx, flush, world, device):
+    """Both forms on exactly the case the reference arm steps: the uniform-fine
+    256x64x64 version of the channel (dt from the CFL condition every step)."""
+    import torch
+
+    from nabla_b200 import abi, solver, workloads
+    g, cfg, st = workloads.channel_uniform(0)
+    out = {"workload": "uniform-fine 256x64x64 obstacle channel (the reference arm's case), "
+                       "from its initial state", "cells": g.ncell, "steps": args.same_case_steps}
+    for name, prec in (("fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+        ns = solver.NSSolver(g, cfg, precision=prec, ctx=ctx)
+        ns.set_state(*st)
+        ns.step(0.0)
+        torch.cuda.synchronize()
+        el, reps = timed_steps(ns_run(ns), args.same_case_steps, stream_of(ctx, ns), flush)
+        out[name] = round(world * g.ncell * args.same_case_steps / (max_over_ranks(el, world, device) * 1e-3)
+                          / 1e6, 4)
+        out[name + "_divergence_max"] = max(r.divergence_max for r in reps)
+        out[name + "_poisson_cycles_per_step"] = reps[-1].poisson_iters
+        ns.close()
+    return out
+
+
+class ns_run:
+    """A uniform NSSolver stepped with dt from its CFL condition."""
+
+    def __init__(self, ns):
+        self.ns = ns
+
+    def step(self):
+        return self.ns.step(0.0)
 
 
 def other_form_and_accuracy(args, ctx, run, prec, precision, value, stream, flush, world, device):
@@ -651,8 +700,10 @@ def run_serve(args, rank, world, local_rank):
 # CPU baselines (the reference's own code, oracle/_ref)
 # ---------------------------------------------------------------------------
 def reference_case(name):
-    """(grid, config, state, dt or 0, description) of the reference's CPU run."""
-    from nabla_b200 import cases
+    """(grid, config, state, dt or None, description) of the reference's CPU run.
+    Built from seeded numpy inputs only: the process that times the reference
+    never loads this repository's CUDA library."""
+    from nabla_b200 import cases, workloads
     if name == "tgv64":
         g, cfg = cases.taylor_green(64)
         return g, cfg, cases.taylor_green_state(g), None, "the same case"
@@ -660,30 +711,27 @@ def reference_case(name):
         g, cfg = cases.taylor_green(64)
         return g, cfg, cases.taylor_green_state(g), None, \
             "the reference NSSolver on the uniform 64^3 TGV box (the reference has no octree or batched path)"
-    import numpy as np
+    g, cfg, st = workloads.channel_uniform(0)
+    return g, cfg, st, 0.0, "the reference NSSolver on the uniform-fine 256x64x64 version of the case " \
+                            "(same seeded boxes and initial field; the reference has no octree MAC step)"
 
-    from nabla_b200 import abi, workloads
-    w = channel_workload()
-    h = 1.0 / 64.0  # effective fine grid: 256 x 64 x 64
-    nx, ny, nz = 256, 64, 64
-    faces = [dict(type=abi.BC_INLET, profile=abi.PROFILE_UNIFORM, inlet_speed=1.0, inlet_axis=0),
-             dict(type=abi.BC_OUTLET), dict(type=abi.BC_WALL), dict(type=abi.BC_WALL),
-             dict(type=abi.BC_WALL), dict(type=abi.BC_WALL)]
-    g = cases.Grid(nx, ny, nz, h, h, h, faces=faces)
-    zc, yc, xc = np.meshgrid((np.arange(nz) + 0.5) * h, (np.arange(ny) + 0.5) * h, (np.arange(nx) + 0.5) * h,
-                             indexing="ij")
-    g.solid[:] = workloads.inside_boxes(w.boxes, xc.ravel(), yc.ravel(), zc.ravel()).astype(np.uint8)
-    st = []
-    for a, (ex, ey, ez) in enumerate([(nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1)]):
-        off = [0.5, 0.5, 0.5]
-        off[a] = 0.0
-        Z, Y, X = np.meshgrid((np.arange(ez) + off[2]) * h, (np.arange(ey) + off[1]) * h,
-                              (np.arange(ex) + off[0]) * h, indexing="ij")
-        u = w.modes.velocity(X.ravel(), Y.ravel(), Z.ravel())[a]
-        st.append(u + (w.mean_u if a == 0 else 0.0))
-    st.append(np.zeros(g.ncell))
-    return g, w.config, tuple(st), 0.0, "the reference NSSolver on the uniform-fine 256x64x64 version of the case " \
-                                        "(the reference has no octree MAC step)"
+
+def host_info():
+    """CPU model, logical CPUs of the host and CPUs this process may run on."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        usable = os.cpu_count()
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable_cpus": usable,
+            "build": "reference sources compiled with g++ -O3 -march=x86-64-v3 (AVX2)"}
 
 
 def cpu_sample(workload_name, steps):
@@ -733,7 +781,8 @@ def run_reference(args):
         "data": "synthetic", "impl": "reference",
         "config": {"workload": args.workload, "cells": cells, "precision": "fp64", "sample": sample},
         "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{steps} NSSolver::step per process, {cores} independent processes; {sample}"},
+                         "sample": f"{steps} NSSolver::step per process, {cores} independent processes; {sample}",
+                         "host": host_info()},
         "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 1),
     }
@@ -766,6 +815,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--same-case-steps", type=int, default=5,
+                    help="channel3: steps of both forms on the reference arm's uniform-fine case (0: skip)")
     ap.add_argument("--shares", type=int, default=1,
                     help="1: time each kernel family once before the timed region")
     args = ap.parse_args()
@@ -790,7 +841,8 @@ def main():
             s, cells, sample = cpu_sample(args.workload, args.cpu_steps)
             out["cpu_baseline"] = {"value": round(cells / s / 1e6, 5), "unit": UNIT, "cores": 1,
                                    "kind": "reference",
-                                   "sample": f"{args.cpu_steps} NSSolver::step, 1 thread: {sample}"}
+                                   "sample": f"{args.cpu_steps} NSSolver::step, 1 thread: {sample}",
+                                   "host": host_info()}
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch

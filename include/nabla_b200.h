@@ -157,6 +157,12 @@ nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, in
  * concurrently. One step in flight per case; not available while profiling. */
 nb_status nb_step_async(nb_case* c, double dt);
 nb_status nb_step_wait(nb_case* c, nb_step_report* rep);
+/* Non-blocking completion test of the step in flight: *ready = 1 once
+ * nb_step_wait would return without waiting, else 0. Lets a request loop
+ * collect each case as soon as its own step ends, instead of waiting for all
+ * of them in lockstep. No reference counterpart (the reference's job runner,
+ * backend/app/jobs.py:50-140, runs one case at a time to completion). */
+nb_status nb_step_ready(nb_case* c, int* ready);
 /* Replaces SolverBackend::sample (core/include/nabla/adaptive/run.hpp:17), as
  * BaselineBackend implements it (core/src/adaptive/run.cpp:49-62), for n points
  * at once: out[q] = component `component` (0 = u, 1 = v, 2 = w: the average of

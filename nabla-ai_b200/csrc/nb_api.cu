@@ -1200,6 +1200,22 @@ nb_status nb_step_wait(nb_case* c, nb_step_report* rep) {
   });
 }
 
+nb_status nb_step_ready(nb_case* c, int* ready) {
+  if (!c || !ready) return NB_ERR_BAD_ARG;
+  if (!c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "no step of this case is in flight");
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    const cudaError_t e = cudaStreamQuery(c->stream);
+    if (e == cudaErrorNotReady) {
+      *ready = 0;
+      return NB_OK;
+    }
+    NB_CUDA(e);
+    *ready = 1;
+    return NB_OK;
+  });
+}
+
 nb_status nb_step_many(nb_case* c, double dt, int nsteps, nb_step_report* rep) {
   if (!c || nsteps < 0) return NB_ERR_BAD_ARG;
   return guarded(c->ctx, [&] {

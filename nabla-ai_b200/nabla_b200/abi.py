@@ -193,6 +193,7 @@ PROTOTYPES = [
     ("nb_batch_step", C.c_int, [VP, C.POINTER(VP), C.c_int, C.c_double, C.c_int, C.POINTER(StepReport)]),
     ("nb_step_async", C.c_int, [VP, C.c_double]),
     ("nb_step_wait", C.c_int, [VP, C.POINTER(StepReport)]),
+    ("nb_step_ready", C.c_int, [VP, C.POINTER(C.c_int)]),
     ("nb_case_device_bytes", C.c_uint64, [VP]),
     ("nb_case_cell_count", C.c_uint64, [VP]),
     ("nb_case_stream", VP, [VP]),

@@ -256,6 +256,14 @@ def step_wait(case) -> abi.StepReport:
     return rep
 
 
+def step_ready(case) -> bool:
+    """True once the step launched by step_async has finished on the device
+    (step_wait then returns without waiting)."""
+    r = C.c_int()
+    case.ctx.check(case.ctx.lib.nb_step_ready(case.h, C.byref(r)), "nb_step_ready")
+    return bool(r.value)
+
+
 def default_tuning() -> dict:
     t = abi.Tuning()
     abi.load().nb_tuning_default(C.byref(t))

@@ -239,18 +239,34 @@ def tgv_octree(base: int, levels: int = 3):
     return geom, leaves
 
 
-def obstacle_channel(seed: int = 0, lmax: int = 2, n_boxes: int = 6, precision_note: str = "") -> AmrWorkload:
+CHANNEL_FACES = [dict(type=abi.BC_INLET, profile=abi.PROFILE_UNIFORM, inlet_speed=1.0, inlet_axis=0),
+                 dict(type=abi.BC_OUTLET), dict(type=abi.BC_WALL), dict(type=abi.BC_WALL),
+                 dict(type=abi.BC_WALL), dict(type=abi.BC_WALL)]
+
+
+def channel_config():
+    return cases.flow_config(reynolds=1000.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
+                             convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
+
+
+def channel_inputs(seed: int = 0, n_boxes: int = 6):
+    """The seeded inputs of the obstacle channel, drawn in a fixed order from
+    one stream: the solid boxes, then the random vector potential. Pure numpy
+    (no device and no library call), so a CPU-only process can rebuild the
+    same case on any grid."""
     rng = np.random.default_rng(seed)
-    h0 = 1.0 / 16.0
-    nb0 = (8, 2, 2)
-    faces = [dict(type=abi.BC_INLET, profile=abi.PROFILE_UNIFORM, inlet_speed=1.0, inlet_axis=0),
-             dict(type=abi.BC_OUTLET), dict(type=abi.BC_WALL), dict(type=abi.BC_WALL),
-             dict(type=abi.BC_WALL), dict(type=abi.BC_WALL)]
-    geom = amr.make_geom(nb0, (h0, h0, h0), lmax, faces)
     boxes = random_boxes(rng, n_boxes)
     sx = rng.uniform(0, 4, 20000)
     sy, sz = rng.uniform(0, 1, 20000), rng.uniform(0, 1, 20000)
     modes = random_modes(rng, sample=(sx, sy, sz))
+    return boxes, modes
+
+
+def obstacle_channel(seed: int = 0, lmax: int = 2, n_boxes: int = 6, precision_note: str = "") -> AmrWorkload:
+    h0 = 1.0 / 16.0
+    nb0 = (8, 2, 2)
+    geom = amr.make_geom(nb0, (h0, h0, h0), lmax, CHANNEL_FACES)
+    boxes, modes = channel_inputs(seed, n_boxes)
     leaves = amr.base_leaves(nb0)
     for lev in range(lmax):
         w, near = _leaf_metric(modes, boxes, leaves, h0, lmax, 0.05)
@@ -263,11 +279,35 @@ def obstacle_channel(seed: int = 0, lmax: int = 2, n_boxes: int = 6, precision_n
     lev, i, j, k = amr.cell_coords(leaves)
     h = h0 / (2.0 ** lev)
     solid = inside_boxes(boxes, (i + 0.5) * h, (j + 0.5) * h, (k + 0.5) * h).astype(np.uint8)
-    cfg = cases.flow_config(reynolds=1000.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
-                            convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
+    cfg = channel_config()
     nl = np.bincount(leaves[:, 0], minlength=lmax + 1)
     desc = (f"obstacle channel [0,4]x[0,1]^2, octree of 8^3 bricks, base 64x16x16, {lmax + 1} levels "
             f"(effective {64 << lmax}x{16 << lmax}x{16 << lmax}), leaves per level {nl.tolist()}, "
             f"{n_boxes} seeded boxes, inflow U=1 + curl of a k=8 random potential (rms 0.05), "
             f"nu=1/1000, WENO-5, CFL 0.4, MG-PCG to 1e-10, seed {seed}")
     return AmrWorkload(geom, leaves, solid, cfg, modes, boxes, 1.0, desc)
+
+
+def channel_uniform(seed: int = 0, refine: int = 2, n_boxes: int = 6):
+    """The obstacle channel on the uniform grid of its finest level (256x64x64
+    cells for refine = 2, h = 1/64): the same seeded boxes (cells whose centre
+    is inside are solid) and the same initial velocity sampled on the MAC faces.
+    Returns (grid, config, (u, v, w, p)) in the reference's lexicographic
+    layout. Pure numpy: no device and no library call."""
+    boxes, modes = channel_inputs(seed, n_boxes)
+    h = 1.0 / (16 << refine)
+    nx, ny, nz = 64 << refine, 16 << refine, 16 << refine
+    g = cases.Grid(nx, ny, nz, h, h, h, faces=[dict(f) for f in CHANNEL_FACES])
+    zc, yc, xc = np.meshgrid((np.arange(nz) + 0.5) * h, (np.arange(ny) + 0.5) * h, (np.arange(nx) + 0.5) * h,
+                             indexing="ij")
+    g.solid[:] = inside_boxes(boxes, xc.ravel(), yc.ravel(), zc.ravel()).astype(np.uint8)
+    st = []
+    for a, (ex, ey, ez) in enumerate([(nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1)]):
+        off = [0.5, 0.5, 0.5]
+        off[a] = 0.0
+        Z, Y, X = np.meshgrid((np.arange(ez) + off[2]) * h, (np.arange(ey) + off[1]) * h,
+                              (np.arange(ex) + off[0]) * h, indexing="ij")
+        u = modes.velocity(X.ravel(), Y.ravel(), Z.ravel())[a]
+        st.append(u + (1.0 if a == 0 else 0.0))
+    st.append(np.zeros(g.ncell))
+    return g, channel_config(), tuple(st)

@@ -47,6 +47,19 @@ struct orc_amr {
   double* phi[ML];
   double divmax;
   int cg_iters;
+  /* Leaf cells in (L, k, j, i) order and the operator's rows, built once on
+   * the first solve (the mesh never changes): the CG loops walk this list
+   * instead of scanning the dense per-level arrays. Same cells, same order,
+   * same arithmetic, so the results are those of the dense scan bit for bit. */
+  size_t nlc;
+  int* lc_L;
+  size_t* lc_ci;
+  double* lc_vol;     /* h0 * h1 * h2 of the cell's level */
+  size_t* op_off;     /* [nlc + 1] row offsets; a solid row has no entries */
+  int* op_L;
+  size_t* op_ci;
+  double* op_coef;
+  double* op_diag;    /* diagonal in face order; 1 for solid rows */
 };
 
 /* ------------------------------------------------------------------ maps -- */
@@ -436,64 +449,116 @@ typedef struct {
         for (int i = 0; i < (A)->n[L][0]; ++i)                                  \
           if (leaf_level((A), L, (const int[3]){i, j, k}) == L)
 
-/* Per-unit-volume composite operator: out = A x on leaf cells (dense per-level x). */
-static void apply_op(orc_amr* A, double* const* x, double* const* out, double* const* diagout) {
+/* The leaf-cell list and the rows of the per-unit-volume composite operator
+ * (out = A x on leaf cells): faces in order -x, +x, -y, +y, -z, +z; a same-level
+ * neighbour 1/h^2, a coarser one 1/(1.5 h^2), each of four finer ones
+ * 1/(3 h^2); a solid neighbour is skipped; an outlet face adds 2/h^2 to the
+ * diagonal; solid rows are identity. */
+static void build_rows(orc_amr* A) {
+  if (A->lc_L) return;
+  size_t n = 0;
+  FOR_LEAF_CELLS(A, L, i, j, k) { ++n; }
+  A->nlc = n;
+  A->lc_L = malloc(n * sizeof(int));
+  A->lc_ci = malloc(n * sizeof(size_t));
+  A->lc_vol = malloc(n * sizeof(double));
+  A->op_off = malloc((n + 1) * sizeof(size_t));
+  A->op_diag = malloc(n * sizeof(double));
+  size_t cap = 8 * n + 16, ne = 0;
+  A->op_L = malloc(cap * sizeof(int));
+  A->op_ci = malloc(cap * sizeof(size_t));
+  A->op_coef = malloc(cap * sizeof(double));
+  size_t q = 0;
+#define PUSH(LL, CC, CO)                                              \
+  do {                                                                \
+    if (ne == cap) {                                                  \
+      cap *= 2;                                                       \
+      A->op_L = realloc(A->op_L, cap * sizeof(int));                  \
+      A->op_ci = realloc(A->op_ci, cap * sizeof(size_t));             \
+      A->op_coef = realloc(A->op_coef, cap * sizeof(double));         \
+    }                                                                 \
+    A->op_L[ne] = (LL);                                               \
+    A->op_ci[ne] = (CC);                                              \
+    A->op_coef[ne] = (CO);                                            \
+    ++ne;                                                             \
+  } while (0)
   FOR_LEAF_CELLS(A, L, i, j, k) {
     const size_t ci = cidx(A, L, i, j, k);
     const int c[3] = {i, j, k};
+    A->lc_L[q] = L;
+    A->lc_ci[q] = ci;
+    A->lc_vol[q] = A->h[L][0] * A->h[L][1] * A->h[L][2];
+    A->op_off[q] = ne;
     if (A->solid[L][ci]) {
-      out[L][ci] = x[L][ci];
-      if (diagout) diagout[L][ci] = 1.0;
+      A->op_diag[q++] = 1.0;
       continue;
     }
-    double diag = 0.0, off = 0.0;
+    double diag = 0.0;
     for (int f = 0; f < 6; ++f) {
       const int a = f >> 1, s = (f & 1) ? 1 : -1;
       const double ih2 = 1.0 / (A->h[L][a] * A->h[L][a]);
-      int q[3] = {c[0], c[1], c[2]};
-      q[a] += s;
-      if (!in_domain(A, L, q)) {
+      int qq[3] = {c[0], c[1], c[2]};
+      qq[a] += s;
+      if (!in_domain(A, L, qq)) {
         if (A->g.face[2 * a + (s > 0)].type == NB_BC_OUTLET) diag += 2.0 * ih2;
         continue;
       }
-      const int lev = leaf_level(A, L, q);
+      const int lev = leaf_level(A, L, qq);
       if (lev == L) {
-        if (A->solid[L][cidx(A, L, q[0], q[1], q[2])]) continue;
+        if (A->solid[L][cidx(A, L, qq[0], qq[1], qq[2])]) continue;
         diag += ih2;
-        off += ih2 * x[L][cidx(A, L, q[0], q[1], q[2])];
+        PUSH(L, cidx(A, L, qq[0], qq[1], qq[2]), ih2);
       } else if (lev == L - 1) {
-        const int cq[3] = {q[0] >> 1, q[1] >> 1, q[2] >> 1};
-        const size_t cc = cidx(A, L - 1, cq[0], cq[1], cq[2]);
+        const size_t cc = cidx(A, L - 1, qq[0] >> 1, qq[1] >> 1, qq[2] >> 1);
         if (A->solid[L - 1][cc]) continue;
         const double coef = ih2 / 1.5;
         diag += coef;
-        off += coef * x[L - 1][cc];
+        PUSH(L - 1, cc, coef);
       } else {
         const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
         for (int d2 = 0; d2 < 2; ++d2)
           for (int d1 = 0; d1 < 2; ++d1) {
             int fq[3];
-            fq[a] = s > 0 ? 2 * q[a] : 2 * q[a] + 1;
+            fq[a] = s > 0 ? 2 * qq[a] : 2 * qq[a] + 1;
             fq[t1] = 2 * c[t1] + d1;
             fq[t2] = 2 * c[t2] + d2;
             const size_t fc = cidx(A, L + 1, fq[0], fq[1], fq[2]);
             if (A->solid[L + 1][fc]) continue;
             const double coef = ih2 / 3.0;
             diag += coef;
-            off += coef * x[L + 1][fc];
+            PUSH(L + 1, fc, coef);
           }
       }
     }
-    out[L][ci] = diag * x[L][ci] - off;
-    if (diagout) diagout[L][ci] = diag > 0.0 ? diag : 1.0;
+    A->op_diag[q++] = diag;
+  }
+#undef PUSH
+  A->op_off[n] = ne;
+}
+
+/* out = A x from the recorded rows. */
+static void apply_rows(orc_amr* A, double* const* x, double* const* out) {
+  /* rows are independent: threads change nothing in any row's arithmetic */
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < A->nlc; ++q) {
+    const int L = A->lc_L[q];
+    const size_t ci = A->lc_ci[q];
+    if (A->solid[L][ci]) {
+      out[L][ci] = x[L][ci];
+      continue;
+    }
+    double off = 0.0;
+    for (size_t e = A->op_off[q]; e < A->op_off[q + 1]; ++e) off += A->op_coef[e] * x[A->op_L[e]][A->op_ci[e]];
+    out[L][ci] = A->op_diag[q] * x[L][ci] - off;
   }
 }
 
 static double vdot(orc_amr* A, double* const* x, double* const* y) {
   double s = 0.0;
-  FOR_LEAF_CELLS(A, L, i, j, k) {
-    const size_t ci = cidx(A, L, i, j, k);
-    s += A->h[L][0] * A->h[L][1] * A->h[L][2] * x[L][ci] * y[L][ci];
+  for (size_t q = 0; q < A->nlc; ++q) {
+    const int L = A->lc_L[q];
+    const size_t ci = A->lc_ci[q];
+    s += A->lc_vol[q] * x[L][ci] * y[L][ci];
   }
   return s;
 }
@@ -506,39 +571,44 @@ static int has_outlet(const orc_amr* A) {
 
 static void remove_fluid_mean(orc_amr* A, double* const* x) {
   double s = 0.0, v = 0.0;
-  FOR_LEAF_CELLS(A, L, i, j, k) {
-    const size_t ci = cidx(A, L, i, j, k);
+  for (size_t q = 0; q < A->nlc; ++q) {
+    const int L = A->lc_L[q];
+    const size_t ci = A->lc_ci[q];
     if (A->solid[L][ci]) continue;
-    const double vol = A->h[L][0] * A->h[L][1] * A->h[L][2];
+    const double vol = A->lc_vol[q];
     s += vol * x[L][ci];
     v += vol;
   }
   const double m = v > 0.0 ? s / v : 0.0;
-  FOR_LEAF_CELLS(A, L, i, j, k) {
-    const size_t ci = cidx(A, L, i, j, k);
+  for (size_t q = 0; q < A->nlc; ++q) {
+    const int L = A->lc_L[q];
+    const size_t ci = A->lc_ci[q];
     if (!A->solid[L][ci]) x[L][ci] -= m;
   }
 }
 
 /* Volume-weighted Jacobi-CG on the composite operator; b is overwritten. */
 static int solve_pressure(orc_amr* A, double* const* b, double* const* x, double tol) {
-  double *r[ML], *z[ML], *pp[ML], *Ap[ML], *dg[ML];
+  build_rows(A);
+  double *r[ML], *z[ML], *pp[ML], *Ap[ML];
   for (int L = 0; L < A->nl; ++L) {
     const size_t n = (size_t)A->n[L][0] * A->n[L][1] * A->n[L][2];
     r[L] = calloc(n, 8);
     z[L] = calloc(n, 8);
     pp[L] = calloc(n, 8);
     Ap[L] = calloc(n, 8);
-    dg[L] = calloc(n, 8);
     memset(x[L], 0, n * 8);
   }
   const int sing = !has_outlet(A);
   if (sing) remove_fluid_mean(A, b);
-  apply_op(A, x, Ap, dg);
-  FOR_LEAF_CELLS(A, L, i, j, k) {
-    const size_t ci = cidx(A, L, i, j, k);
+  /* Jacobi diagonal: diag > 0 ? diag : 1 (1 on solid rows) */
+  double* dg = malloc(A->nlc * sizeof(double));
+  for (size_t q = 0; q < A->nlc; ++q) dg[q] = A->op_diag[q] > 0.0 ? A->op_diag[q] : 1.0;
+  for (size_t q = 0; q < A->nlc; ++q) {
+    const int L = A->lc_L[q];
+    const size_t ci = A->lc_ci[q];
     r[L][ci] = A->solid[L][ci] ? 0.0 : b[L][ci];
-    z[L][ci] = r[L][ci] / dg[L][ci];
+    z[L][ci] = r[L][ci] / dg[q];
     pp[L][ci] = z[L][ci];
   }
   const double bnorm = sqrt(vdot(A, r, r)) + 1e-300;
@@ -546,35 +616,38 @@ static int solve_pressure(orc_amr* A, double* const* b, double* const* x, double
   int it = 0;
   for (; it < 20000; ++it) {
     if (sqrt(vdot(A, r, r)) <= tol * bnorm) break;
-    apply_op(A, pp, Ap, NULL);
+    apply_rows(A, pp, Ap);
     const double pap = vdot(A, pp, Ap);
     if (fabs(pap) < 1e-300) break;
     const double alpha = rz / pap;
-    FOR_LEAF_CELLS(A, L, i, j, k) {
-      const size_t ci = cidx(A, L, i, j, k);
+    for (size_t q = 0; q < A->nlc; ++q) {
+      const int L = A->lc_L[q];
+      const size_t ci = A->lc_ci[q];
       x[L][ci] += alpha * pp[L][ci];
       r[L][ci] -= alpha * Ap[L][ci];
     }
     if (sing) remove_fluid_mean(A, r);
-    FOR_LEAF_CELLS(A, L, i, j, k) {
-      const size_t ci = cidx(A, L, i, j, k);
-      z[L][ci] = r[L][ci] / dg[L][ci];
+    for (size_t q = 0; q < A->nlc; ++q) {
+      const int L = A->lc_L[q];
+      const size_t ci = A->lc_ci[q];
+      z[L][ci] = r[L][ci] / dg[q];
     }
     const double rzn = vdot(A, r, z);
     const double beta = rzn / rz;
     rz = rzn;
-    FOR_LEAF_CELLS(A, L, i, j, k) {
-      const size_t ci = cidx(A, L, i, j, k);
+    for (size_t q = 0; q < A->nlc; ++q) {
+      const int L = A->lc_L[q];
+      const size_t ci = A->lc_ci[q];
       pp[L][ci] = z[L][ci] + beta * pp[L][ci];
     }
   }
   if (sing) remove_fluid_mean(A, x);
+  free(dg);
   for (int L = 0; L < A->nl; ++L) {
     free(r[L]);
     free(z[L]);
     free(pp[L]);
     free(Ap[L]);
-    free(dg[L]);
   }
   return it;
 }
@@ -704,6 +777,14 @@ orc_amr* orc_amr_create(const nb_amr_geom* g, const int32_t* leaves, int64_t n, 
 void orc_amr_destroy(orc_amr* A) {
   if (!A) return;
   free(A->leaf);
+  free(A->lc_L);
+  free(A->lc_ci);
+  free(A->lc_vol);
+  free(A->op_off);
+  free(A->op_L);
+  free(A->op_ci);
+  free(A->op_coef);
+  free(A->op_diag);
   for (int L = 0; L < A->nl; ++L) {
     free(A->solid[L]);
     free(A->p[L]);

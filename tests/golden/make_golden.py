@@ -1,6 +1,6 @@
 """Generate the golden fixtures from the reference's own CPU code.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle REF=<reference checkout> ref && python tests/golden/make_golden.py
 
 Runs the reference (oracle/_ref/libnabla_ref.so, compiled in place from the
 reference tree by oracle/Makefile) on small seeded inputs and stores inputs
