@@ -249,8 +249,6 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         run.step()
     torch.cuda.synchronize()
-    # the state the timed steps start from (the end-to-end pass replays the same trajectory)
-    start = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in run.get_state()]
     # share of each kernel family (one profiled direct-launch step per family, untimed)
     shares = {}
     for fam in (FAMILIES if args.shares else ["smooth"]):
@@ -258,6 +256,8 @@ def run_ours(args, rank, world, local_rank):
         shares[fam] = {"ms": ms, "launches": nl, "bytes": nb}
     total = sum(v["ms"] for v in shares.values()) or 1.0
     top = max(shares, key=lambda k: shares[k]["ms"])
+    # the state the timed steps start from (the end-to-end pass replays the same trajectory)
+    start = [torch.from_numpy(a.copy()).pin_memory().numpy() for a in run.get_state()]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()

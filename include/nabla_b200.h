@@ -306,6 +306,44 @@ nb_status nb_amr_apply_laplacian(nb_ctx* ctx, nb_amr_mesh* m, const double* x, d
 nb_status nb_amr_poisson_solve(nb_ctx* ctx, nb_amr_mesh* m, const double* b, double* x, double tol,
                                int max_cycles, int precision, nb_poisson_report* rep);
 
+/* ---- integer maps of octree brick meshes ------------------------------------
+ * Keys: the Morton key of a leaf's anchor on the finest level (leaf (L, b)
+ * anchors at b << (lmax - L)), with x in the lowest bit of each triple: the
+ * key of core/include/nabla/mesh/morton.hpp:19-48 (mortonEncode/Decode), 21
+ * bits per axis. Rank order = ascending key.
+ * Face-neighbour table: for rank r and face d (0 -x, 1 +x, 2 -y, 3 +y, 4 -z,
+ * 5 +z), nnbr[6r+d] neighbours in nbr[24r+4d .. +3] (unused entries -1): the
+ * rule of Octree::faceNeighbors (core/src/mesh/octree.cpp:229-283) at brick
+ * granularity: the coarser-or-equal leaf holding the brick across the face,
+ * else the 2x2 leaves one level finer on the touching side, in the
+ * reference's order (k1 over axis (d/2+1)%3 outer, k2 over axis (d/2+2)%3
+ * inner); none across a non-periodic domain face; periodic axes wrap. */
+uint64_t nb_morton_encode(uint32_t x, uint32_t y, uint32_t z);
+void nb_morton_decode(uint64_t key, uint32_t* x, uint32_t* y, uint32_t* z);
+/* Builds the rank order and the face-neighbour table of a leaf list (any
+ * order, any 2:1 face balance) on the device: keys (n, sorted), order (n:
+ * input position of rank r), nbr (24n), nnbr (6n), all host arrays. A leaf
+ * outside the geometry or two leaves with one anchor: NB_ERR_BAD_ARG. */
+nb_status nb_amr_build_maps(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* leaves, int64_t n, uint64_t* keys,
+                            int32_t* order, int32_t* nbr, int32_t* nnbr);
+/* The same keys and table of an existing mesh, read from the host tree its
+ * kernels' maps are built from (rank order, per-level lookup tables). */
+nb_status nb_amr_mesh_maps(const nb_amr_mesh* m, uint64_t* keys, int32_t* nbr, int32_t* nnbr);
+/* Host only (no device, no context): the tree nb_amr_mesh_create would build
+ * from this leaf list (coverage and 26-neighbour balance validated,
+ * NB_ERR_BAD_ARG otherwise), its keys, its leaves in rank order (ranked: 4n)
+ * and its face-neighbour table. */
+nb_status nb_amr_tree_maps(const nb_amr_geom* g, const int32_t* leaves, int64_t n, uint64_t* keys, int32_t* ranked,
+                           int32_t* nbr, int32_t* nnbr);
+/* The coarse-fine couplings of the mesh's composite operator: CSR over the
+ * mesh's cells (off: cells+1 entries), each coupling a neighbour cell index
+ * (rank * 512 + local cell) and its per-unit-volume coefficient (the face
+ * rule of OctreePoisson::faceCoeff, core/src/flow/octree_poisson.cpp:24-32,
+ * over the cell volume). *count always receives the number of couplings;
+ * pass NULL arrays to query it, else cap >= *count. */
+nb_status nb_amr_mesh_couplings(const nb_amr_mesh* m, int64_t* count, int32_t* off, int32_t* nbr, double* coef,
+                                int64_t cap);
+
 /* ---- MAC step on an octree-AMR mesh ------------------------------------------
  * NSSolver (core/include/nabla/flow/ns_solver.hpp:58-96) on the composite
  * mesh: the same SSP-RK3 / WENO-5 / MG-PCG step, with the octree face rule of

@@ -228,6 +228,16 @@ PROTOTYPES = [
     ("nb_amr_mesh_destroy", None, [VP]),
     ("nb_amr_mesh_leaf_count", C.c_int64, [VP]),
     ("nb_amr_mesh_leaves", C.c_int, [VP, C.POINTER(C.c_int32)]),
+    ("nb_morton_encode", C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32]),
+    ("nb_morton_decode", None, [C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("nb_amr_build_maps", C.c_int, [VP, C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64,
+                                    C.POINTER(C.c_uint64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int32)]),
+    ("nb_amr_mesh_maps", C.c_int, [VP, C.POINTER(C.c_uint64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("nb_amr_tree_maps", C.c_int, [C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("nb_amr_mesh_couplings", C.c_int, [VP, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        DP, C.c_int64]),
     ("nb_amr_apply_laplacian", C.c_int, [VP, VP, DP, DP]),
     ("nb_amr_poisson_solve", C.c_int, [VP, VP, DP, DP, C.c_double, C.c_int, C.c_int, C.POINTER(PoissonReport)]),
     ("nb_amr_case_create", C.c_int, [VP, VP, C.POINTER(FlowConfig), C.c_int, C.POINTER(VP)]),

@@ -75,6 +75,52 @@ def coarsen(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray) -> np.ndar
     return out[:need.value].copy()
 
 
+def morton_encode(x: int, y: int, z: int) -> int:
+    """The library's Morton key (nb_morton.h through the C ABI)."""
+    return int(abi.load().nb_morton_encode(x, y, z))
+
+
+def morton_decode(key: int):
+    x, y, z = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    abi.load().nb_morton_decode(key, C.byref(x), C.byref(y), C.byref(z))
+    return x.value, y.value, z.value
+
+
+def _map_arrays(n):
+    return (np.zeros(n, dtype=np.uint64), np.zeros((n, 4), dtype=np.int32), np.zeros((n, 6, 4), dtype=np.int32),
+            np.zeros((n, 6), dtype=np.int32))
+
+
+def tree_maps(geom: abi.AmrGeom, leaves: np.ndarray):
+    """Host-only: (keys, leaves in rank order, face-neighbour ranks [n,6,4], counts [n,6])
+    of the tree nb_amr_mesh_create builds from `leaves` (nb_amr_tree_maps)."""
+    leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+    n = leaves.shape[0]
+    keys, ranked, nbr, cnt = _map_arrays(n)
+    I32 = C.POINTER(C.c_int32)
+    st = abi.load().nb_amr_tree_maps(C.byref(geom), leaves.ctypes.data_as(I32), n,
+                                     keys.ctypes.data_as(C.POINTER(C.c_uint64)), ranked.ctypes.data_as(I32),
+                                     nbr.ctypes.data_as(I32), cnt.ctypes.data_as(I32))
+    if st != abi.NB_OK:
+        raise NablaError(st, "nb_amr_tree_maps rejected the leaf list")
+    return keys, ranked, nbr, cnt
+
+
+def build_maps(geom: abi.AmrGeom, leaves: np.ndarray, ctx: Context | None = None):
+    """Device-built (keys, order, face-neighbour ranks [n,6,4], counts [n,6]) of any
+    leaf list (nb_amr_build_maps); order[r] is the input position of rank r."""
+    ctx = ctx or default_context()
+    leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+    n = leaves.shape[0]
+    keys, _, nbr, cnt = _map_arrays(n)
+    order = np.zeros(n, dtype=np.int32)
+    I32 = C.POINTER(C.c_int32)
+    ctx.check(ctx.lib.nb_amr_build_maps(ctx.h, C.byref(geom), leaves.ctypes.data_as(I32), n,
+                                        keys.ctypes.data_as(C.POINTER(C.c_uint64)), order.ctypes.data_as(I32),
+                                        nbr.ctypes.data_as(I32), cnt.ctypes.data_as(I32)), "nb_amr_build_maps")
+    return keys, order, nbr, cnt
+
+
 def cell_coords(leaves: np.ndarray):
     """(level, i, j, k) of every cell, leaves x 512, in array order."""
     l = np.arange(512)
@@ -116,6 +162,30 @@ class AmrMesh:
 
     def __del__(self):
         self.close()
+
+    def maps(self):
+        """(keys, face-neighbour ranks [n,6,4], counts [n,6]) of the mesh's own tree."""
+        n = self.leaves.shape[0]
+        keys, _, nbr, cnt = _map_arrays(n)
+        I32 = C.POINTER(C.c_int32)
+        self.ctx.check(self.ctx.lib.nb_amr_mesh_maps(self.h, keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                     nbr.ctypes.data_as(I32), cnt.ctypes.data_as(I32)),
+                       "nb_amr_mesh_maps")
+        return keys, nbr, cnt
+
+    def couplings(self):
+        """Coarse-fine couplings of the composite operator: (off [cells+1], nbr, coef)."""
+        cnt = C.c_int64()
+        lib = self.ctx.lib
+        self.ctx.check(lib.nb_amr_mesh_couplings(self.h, C.byref(cnt), None, None, None, 0), "couplings")
+        off = np.zeros(self.ncell + 1, dtype=np.int32)
+        nbr = np.zeros(max(cnt.value, 1), dtype=np.int32)
+        coef = np.zeros(max(cnt.value, 1))
+        I32 = C.POINTER(C.c_int32)
+        self.ctx.check(lib.nb_amr_mesh_couplings(self.h, C.byref(cnt), off.ctypes.data_as(I32),
+                                                 nbr.ctypes.data_as(I32), abi.dptr(coef), nbr.size),
+                       "couplings")
+        return off, nbr[:cnt.value], coef[:cnt.value]
 
     def cell_size(self):
         """Per-cell (hx, hy, hz) arrays."""
