@@ -45,7 +45,7 @@ UNIT = "Mcell-steps/s"
 # same launches the roofline averages, from one ncu capture of this workload
 # (profiles/channel3_launches_and_captures.md: 40 consecutive k_smooth launches).
 NCU_TRAFFIC = {("channel3", "smooth"): 2.159e6}
-FAMILIES = ["rhs_rk", "smooth", "resid_restrict", "coarse_cg", "vtail", "pcg_matvec", "pcg_update",
+FAMILIES = ["rhs_rk", "vgrid", "smooth", "resid_restrict", "coarse_cg", "vtail", "pcg_matvec", "pcg_update",
             "pcg_center", "pcg_mean", "pcg_dots", "div", "correct", "diag", "sync"]
 
 

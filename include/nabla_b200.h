@@ -219,6 +219,12 @@ typedef struct nb_tuning {
                                 from the last pressure scaled to the RK stage, 0 from
                                 zero; the FP64 form always starts from zero as the
                                 reference does */
+  int32_t vgrid;             /* 0 (default): one launch per sweep (and the cluster
+                                tail); 1: each V-cycle (all levels and the coarsest
+                                solve) is ONE cooperative launch whose CTAs run the
+                                sweeps, restrictions and prolongations phase by phase
+                                with a grid barrier between phases (a barrier that waits
+                                over a second ends the solve with NB_ERR_DEVICE_TIMEOUT) */
 } nb_tuning;
 
 typedef struct nb_tune_report {

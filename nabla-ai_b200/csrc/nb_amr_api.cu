@@ -192,6 +192,7 @@ nb_status nb_amr_poisson_solve(nb_ctx* ctx, nb_amr_mesh* m, const double* b, dou
     NB_CUDA(cudaMemcpyAsync(ctx->stage_a, b, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     mg.solve_async(ctx->stream, ctx->stage_a, tol, max_cycles);
     const nb_poisson_report r = mg.fetch_report(ctx->stream);
+    if (mg.timed_out()) throw ApiError{NB_ERR_DEVICE_TIMEOUT, "a device-side barrier wait gave up"};
     NB_CUDA(cudaMemcpyAsync(x, mg.phi(), n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     NB_CUDA(cudaStreamSynchronize(ctx->stream));
     if (rep) *rep = r;

@@ -509,6 +509,14 @@ void do_step(nb_case& c, double dt, nb_step_report* rep) {
   complete_step(c, rep);
 }
 
+// True when a bounded device-side wait of the step's pressure solves gave up
+// (a grid-resident V-cycle's barrier, stop code STOP_TIMEOUT).
+bool step_timed_out(const nb_case& c) {
+  for (int s = 0; s < 3; ++s)
+    if (c.h_blk->rep[s][1] == static_cast<double>(STOP_TIMEOUT)) return true;
+  return false;
+}
+
 // Host side of a finished step once c.h_blk holds its results: clock, state
 // parity and the StepReport (ns_solver.cpp:797-823).
 void finish_step(nb_case& c, nb_step_report* rep) {
@@ -927,6 +935,8 @@ nb_status nb_batch_step(nb_ctx* ctx, nb_case* const* cases, int n, double dt, in
         }
       batch_step(ctx, cases, n, cfl_dt, reports);
     }
+    for (int q = 0; q < n; ++q)
+      if (step_timed_out(*cases[q])) return fail(ctx, NB_ERR_DEVICE_TIMEOUT, "a device-side barrier wait gave up");
     if (reports)
       for (int q = 0; q < n; ++q)
         if (std::isnan(reports[q].momentum_residual)) return fail(ctx, NB_ERR_NAN, "NaN in the step diagnostics");
@@ -1169,6 +1179,7 @@ nb_status nb_step(nb_case* c, double dt, nb_step_report* rep) {
     nb_step_report r{};
     do_step(*c, dt, &r);
     if (rep) *rep = r;
+    if (step_timed_out(*c)) return fail(c->ctx, NB_ERR_DEVICE_TIMEOUT, "a device-side barrier wait gave up");
     if (std::isnan(r.momentum_residual) || std::isnan(r.continuity_residual))
       return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");
     return NB_OK;
@@ -1194,6 +1205,7 @@ nb_status nb_step_wait(nb_case* c, nb_step_report* rep) {
     nb_step_report r{};
     complete_step(*c, &r);
     if (rep) *rep = r;
+    if (step_timed_out(*c)) return fail(c->ctx, NB_ERR_DEVICE_TIMEOUT, "a device-side barrier wait gave up");
     if (std::isnan(r.momentum_residual) || std::isnan(r.continuity_residual))
       return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");
     return NB_OK;
@@ -1221,7 +1233,10 @@ nb_status nb_step_many(nb_case* c, double dt, int nsteps, nb_step_report* rep) {
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
     nb_step_report r{};
-    for (int i = 0; i < nsteps; ++i) do_step(*c, dt, &r);
+    for (int i = 0; i < nsteps; ++i) {
+      do_step(*c, dt, &r);
+      if (step_timed_out(*c)) return fail(c->ctx, NB_ERR_DEVICE_TIMEOUT, "a device-side barrier wait gave up");
+    }
     if (rep) *rep = r;
     if (std::isnan(r.momentum_residual)) return fail(c->ctx, NB_ERR_NAN, "NaN in the step diagnostics");
     return NB_OK;
@@ -1245,6 +1260,7 @@ nb_status nb_poisson_solve(nb_ctx* ctx, const nb_grid_desc* grid, const double* 
     ctx->launches++;
     mg.solve_async(ctx->stream, ctx->stage_b, tol, max_cycles);
     const nb_poisson_report r = mg.fetch_report(ctx->stream);
+    if (mg.timed_out()) throw ApiError{NB_ERR_DEVICE_TIMEOUT, "a device-side barrier wait gave up"};
     launch_convert(ctx->stream, F, 3, 1, mg.phi(), ctx->stage_a);
     ctx->launches++;
     NB_CUDA(cudaMemcpyAsync(x, ctx->stage_a, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

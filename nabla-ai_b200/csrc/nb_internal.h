@@ -143,8 +143,9 @@ enum Slot : int {
 };
 inline int lvl_slot(int level, int which) { return S_LVL_MEAN + level * 4 + which; }
 
+constexpr int STOP_TIMEOUT = 3;  // a bounded device-side wait gave up
 struct SolveFlags {
-  int stop;      // 0 running, 1 converged, 2 breakdown (|pAp| < 1e-300)
+  int stop;      // 0 running, 1 converged, 2 breakdown (|pAp| < 1e-300), 3 STOP_TIMEOUT
   int iters;     // completed MG-PCG cycles
   int early;     // rhs already below tolerance
   int nan;       // NaN seen in a reduction

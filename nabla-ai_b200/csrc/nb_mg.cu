@@ -1053,6 +1053,184 @@ __global__ void __launch_bounds__(NT) k_vtail(const TailProg* __restrict__ prog,
 }
 
 // ---------------------------------------------------------------------------
+// Grid-resident V-cycle. Each sweep as its own kernel costs a launch, the
+// scheduling of its CTAs and the drain of its stores, several microseconds on
+// levels whose data movement takes one; a V-cycle has 15-20 of them. Here one
+// cooperative launch (every CTA resident) runs the V-cycle's phase program:
+// each phase is the launch path's own per-brick code (smooth_bricks,
+// resid_restrict_bricks, the coarsest solves) over bricks blockIdx.x,
+// blockIdx.x + gridDim.x, ..., and consecutive phases are separated by a grid
+// barrier. Level vectors stay in global memory and are read through L2
+// (ld.global.cg), since L1 is not coherent across SMs within a launch. A
+// phase with a pending mean writes one partial per CTA; after the barrier
+// every CTA sums the partials in the same fixed order and writes the same
+// mean, so no second barrier is needed. Barrier waits are bounded: after about
+// a second a CTA marks the launch aborted, sets the solve's stop code to
+// STOP_TIMEOUT and every CTA returns.
+// ---------------------------------------------------------------------------
+struct GCAcc {
+  static constexpr bool kCG = true;  // pending means are written inside the launch
+  template <typename T>
+  __device__ __forceinline__ T ld(const T* p, int n) const { return __ldcg(p + n); }
+  template <typename T>
+  __device__ __forceinline__ void st(T* p, int n, T v) const { p[n] = v; }
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The k-th barrier of the launch (k = 1, 2, ...): every CTA arrives once.
+// Returns false if the launch was aborted (this CTA or another gave up).
+__device__ __forceinline__ bool grid_barrier(const GridProg* prog, unsigned k, int* sh_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned* cnt = prog->sync;
+    unsigned* abort = prog->sync + 1;
+    __threadfence();
+    atomicAdd(cnt, 1u);
+    const unsigned target = k * gridDim.x;
+    const unsigned long long t0 = global_ns();
+    int ok = 1;
+    while (ld_acquire_u32(cnt) < target) {
+      if (ld_acquire_u32(abort)) {
+        ok = 0;
+        break;
+      }
+      if (global_ns() - t0 > 1000000000ull) {  // about a second: give up
+        atomicExch(abort, 1u);
+        prog->flags->stop = STOP_TIMEOUT;
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    *sh_ok = ok;
+  }
+  __syncthreads();
+  return *sh_ok != 0;
+}
+
+template <typename T>
+__device__ __forceinline__ XFetchT<T, const LevelView*, GCAcc> grid_fetch(const TailFetch& f, const LevelView* lv) {
+  return XFetchT<T, const LevelView*, GCAcc>{static_cast<const T*>(f.x), f.xmean, static_cast<const T*>(f.ec),
+                                             f.ecmean, f.clvl >= 0 ? lv + f.clvl : lv, f.fx, f.fy, f.fz, f.xfb,
+                                             f.xfo, GCAcc{}};
+}
+
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH, 1024 / NTH) k_vgrid(const GridProg* __restrict__ prog, const SolveFlags* flags, int maxit) {
+  if (stopped(flags, maxit)) return;  // the same answer in every CTA: nothing writes the flags meanwhile
+  __shared__ T tile[TSN];
+  __shared__ T rs[BR3];
+  __shared__ uint8_t fl[BR3];
+  __shared__ double red[128];
+  __shared__ int sh_ok;
+  // dynamic shared memory: [level views | phases | coarsest-solve scratch]
+  extern __shared__ __align__(16) double gdsm_all[];
+  const int nlev = prog->nlev, nph = prog->nphase;
+  LevelView* lv = reinterpret_cast<LevelView*>(gdsm_all);
+  TailPhase* sph = reinterpret_cast<TailPhase*>(lv + nlev);
+  double* gdsm = reinterpret_cast<double*>(sph + nph);
+  {  // the program is read in every phase: one copy per CTA up front
+    const int* src = reinterpret_cast<const int*>(prog->lv);
+    int* dst = reinterpret_cast<int*>(lv);
+    for (int i = threadIdx.x; i < nlev * static_cast<int>(sizeof(LevelView) / 4); i += NTH) dst[i] = src[i];
+    src = reinterpret_cast<const int*>(prog->ph);
+    dst = reinterpret_cast<int*>(sph);
+    for (int i = threadIdx.x; i < nph * static_cast<int>(sizeof(TailPhase) / 4); i += NTH) dst[i] = src[i];
+  }
+  __syncthreads();
+  const GCAcc acc{};
+  unsigned nbar = 0;
+  for (int p = 0; p < nph; ++p) {
+    const TailPhase& ph = sph[p];
+    const LevelView& L = lv[ph.lvl];
+    double part = 0.0;
+    if (ph.op == TAIL_SMOOTH) {
+      SweepOut<T, GCAcc> sink{static_cast<T*>(ph.out), acc};
+      smooth_bricks<T, NTH>(L, static_cast<const T*>(ph.b), ph.bmean, grid_fetch<T>(ph.X, lv), sink,
+                            static_cast<T>(ph.c2), static_cast<T>(ph.c1), ph.prev_mode, grid_fetch<T>(ph.P, lv),
+                            blockIdx.x, gridDim.x, tile, acc);
+      part = sink.part;
+    } else if (ph.op == TAIL_RESID) {
+      part = resid_restrict_bricks<T, NTH>(L, static_cast<const T*>(ph.b), ph.bmean, grid_fetch<T>(ph.X, lv),
+                                           lv[ph.clvl], ph.fx, ph.fy, ph.fz, static_cast<T*>(ph.out), blockIdx.x,
+                                           gridDim.x, tile, rs, fl, acc);
+    } else if (ph.op == TAIL_DIRECT) {
+      // the exact coarsest solve: every CTA stages the rhs, the rows of the
+      // dense inverse are spread over all warps of the grid, then (after a
+      // barrier) every CTA scatters its share of the level
+      const int nf = prog->nf, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = NTH >> 5;
+      const T* b = static_cast<const T*>(ph.b);
+      const double bm = ph.bmean ? __ldcg(ph.bmean) : 0.0;
+      double* rh = gdsm;
+      double sum = 0.0;
+      for (int q = tid; q < nf; q += NTH) {
+        const double v = static_cast<double>(acc.ld(b, prog->fmap[q])) - bm;
+        rh[q] = v;
+        sum += v;
+      }
+      if (prog->singular && nf > 0) {  // poisson.cpp:160-178 (rhs projected to zero mean)
+        const double mean = bsum_bcast(sum, red) / nf;
+        for (int q = tid; q < nf; q += NTH) rh[q] -= mean;
+      }
+      __syncthreads();
+      for (int q = blockIdx.x * nwarp + warp; q < nf; q += gridDim.x * nwarp) {
+        const double* row = prog->inv + static_cast<size_t>(q) * nf;
+        double a = 0.0;
+        for (int c = lane; c < nf; c += 32) a += row[c] * rh[c];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+        if (lane == 0) prog->xs[q] = a;
+      }
+      if (!grid_barrier(prog, ++nbar, &sh_ok)) return;
+      double mean = 0.0;
+      if (prog->singular && nf > 0) {
+        double t = 0.0;
+        for (int q = tid; q < nf; q += NTH) t += __ldcg(prog->xs + q);
+        mean = bsum_bcast(t, red) / nf;
+      }
+      const int n = L.nx * L.ny * L.nz;
+      T* xout = static_cast<T*>(ph.out);
+      for (int m = blockIdx.x * NTH + tid; m < n; m += gridDim.x * NTH) {
+        const int q = prog->lexpos[m];
+        const double v = q >= 0 ? __ldcg(prog->xs + q) : 0.0;
+        acc.st(xout, prog->lexcell[m], static_cast<T>(q >= 0 && prog->singular ? v - mean : v));
+      }
+    } else if (blockIdx.x == 0) {  // TAIL_CG: CgPoisson(1e-6, 500) on one CTA
+      coarse_cg_body<T>(L, static_cast<const T*>(ph.b), ph.bmean, static_cast<T*>(ph.out), prog->singular, 1e-6,
+                        500, gdsm, acc);
+    }
+    // partials alternate between two halves by phase parity: a CTA that has
+    // moved on cannot overwrite what a slower one is still summing
+    double* parts = prog->partials + (p & 1) * gridDim.x;
+    if (ph.mean_out) {
+      double a[1] = {part};
+      block_reduce<1>(a, red);
+      if (threadIdx.x == 0) parts[blockIdx.x] = a[0];
+    }
+    if (p + 1 == nph && !ph.mean_out) break;  // the end of the launch orders the last phase
+    if (!grid_barrier(prog, ++nbar, &sh_ok)) return;
+    if (ph.mean_out) {  // every CTA forms the same mean from the partials, in the same order
+      double a[1] = {0.0};
+      for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += NTH) a[0] += __ldcg(parts + i);
+      block_reduce<1>(a, red);
+      if (threadIdx.x == 0) *ph.mean_out = a[0] * ph.inv_nf;
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // PCG vector kernels on level 0 (FP64).
 // ---------------------------------------------------------------------------
 struct DFetch {
@@ -1803,6 +1981,7 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
   halo_mode_ = t.halo_mode == 1 ? 1 : 0;
   direct_max_ = std::min(std::max(t.coarse_direct_max, 0), 512);
   tail_bricks_ = std::min(std::max(t.tail_bricks, 0), 4096);
+  vgrid_ = t.vgrid != 0;
   // Smoother coefficients per sweep of a phase: damped Jacobi (the reference's,
   // c2 = omega) or, mixed form only, Chebyshev on [lmax / 6, lmax] of D^-1 A
   // with lmax = 2, the Gershgorin bound (every row of D^-1 A has diagonal 1
@@ -1845,6 +2024,7 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc, const
   }
   common_alloc();
   build_tail();
+  build_grid();
 }
 
 // Composite hierarchy: MG level m+1 merges the finest octree level of level m
@@ -1914,6 +2094,7 @@ MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc, co
   // coarsest level is solved exactly instead of by CgPoisson(1e-6, 500).
   if (fine.tree.nlev > 1) build_dense_coarse();
   build_tail();
+  build_grid();
 }
 
 MgSolver::~MgSolver() {
@@ -2253,6 +2434,117 @@ void MgSolver::launch_tail(cudaStream_t s) {
     NB_LAUNCH(lc_, "vtail", s, tail_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vtail<double>, prog, flags_, maxit_)));
 }
 
+// Records the whole V-cycle from level 0 (every level, the coarsest solve
+// included) as one grid program when the device can hold a cooperative grid
+// of the program's kernel; otherwise leaves the per-sweep launches in place.
+void MgSolver::build_grid() {
+  grid_prog_ = nullptr;
+  if (!vgrid_) return;
+  const int last = static_cast<int>(lv_.size()) - 1;
+  if (last + 1 > MAX_GRID_LEV) return;
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  constexpr int GT = 256;  // threads per CTA: two cells per thread, four CTAs per SM
+  const void* fn = mixed ? reinterpret_cast<const void*>(k_vgrid<float, GT>)
+                         : reinterpret_cast<const void*>(k_vgrid<double, GT>);
+  int dev = 0, nsm = 0, coop = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  NB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  NB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return;
+  const size_t nco = static_cast<size_t>(lv_[last].v.nx) * lv_[last].v.ny * lv_[last].v.nz;
+  // the phase count of a V-cycle over these levels (recorded below)
+  std::vector<TailPhase> ph;
+  {
+    const int saved_tail = tail_lvl_;
+    tail_lvl_ = 0;  // phases' levels relative to level 0; no cluster tail inside
+    const double saved_bytes = tail_bytes_;
+    tail_bytes_ = 0.0;
+    if (mixed) vcycle<float>(nullptr, 0, rnew_f_, -1, nullptr, &grid_slot_, &grid_x_, &ph);
+    else vcycle<double>(nullptr, 0, rnew_, -1, nullptr, &grid_slot_, &grid_x_, &ph);
+    grid_bytes_ = tail_bytes_;
+    tail_bytes_ = saved_bytes;
+    tail_lvl_ = saved_tail;
+  }
+  if (ph.size() > static_cast<size_t>(MAX_GRID_PH)) return;
+  static_assert(sizeof(LevelView) % 8 == 0 && sizeof(TailPhase) % 8 == 0, "program staged in 8-byte units");
+  const size_t smem = sizeof(LevelView) * (last + 1) + sizeof(TailPhase) * ph.size() +
+                      (dense_ ? sizeof(double) * dense_nf_ : coarse_smem(nco));
+  int optin = 0;
+  NB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  NB_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if (smem + fa.sharedSizeBytes > static_cast<size_t>(optin)) return;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - static_cast<int>(fa.sharedSizeBytes)) !=
+          cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, GT, smem) != cudaSuccess || per_sm < 1) {
+    (void)cudaGetLastError();
+    return;
+  }
+  // no more CTAs than the largest level has bricks, and never more than can be resident
+  int widest = 1;
+  for (const DevLevel& D : lv_) widest = std::max(widest, D.h.nbrick);
+  const int ctas = std::min(per_sm * nsm, std::min(widest, MAX_GRID));
+  GridProg h{};
+  h.nlev = last + 1;
+  h.nphase = static_cast<int>(ph.size());
+  h.singular = singular_ ? 1 : 0;
+  h.nf = dense_ ? dense_nf_ : 0;
+  h.inv = dense_inv_;
+  h.fmap = dense_fmap_;
+  h.lexpos = dense_lexpos_;
+  h.lexcell = dense_lexcell_;
+  h.xs = dense_ ? static_cast<double*>(alloc(sizeof(double) * dense_nf_)) : nullptr;
+  grid_sync_ = static_cast<unsigned*>(alloc(2 * sizeof(unsigned)));
+  NB_CUDA(cudaMemset(grid_sync_, 0, 2 * sizeof(unsigned)));
+  h.sync = grid_sync_;
+  h.partials = static_cast<double*>(alloc(2 * sizeof(double) * ctas));
+  h.flags = flags_;
+  for (int l = 0; l <= last; ++l) h.lv[l] = lv_[l].v;
+  for (size_t q = 0; q < ph.size(); ++q) h.ph[q] = ph[q];
+  GridProg* d = static_cast<GridProg*>(alloc(sizeof(GridProg)));
+  NB_CUDA(cudaMemcpy(d, &h, sizeof(GridProg), cudaMemcpyHostToDevice));
+  grid_b_ = mixed ? static_cast<const void*>(rnew_f_) : static_cast<const void*>(rnew_);
+  grid_prog_alt_ = nullptr;
+  if (!mixed) {
+    // FP64: the V-cycle reads rnew in place and the PCG swaps r and rnew every
+    // cycle, so a second program reads the other buffer
+    for (int q = 0; q < h.nphase; ++q)
+      if (h.ph[q].b == rnew_) h.ph[q].b = r_;
+    grid_prog_alt_ = static_cast<GridProg*>(alloc(sizeof(GridProg)));
+    NB_CUDA(cudaMemcpy(grid_prog_alt_, &h, sizeof(GridProg), cudaMemcpyHostToDevice));
+  }
+  grid_prog_ = d;
+  grid_ctas_ = ctas;
+  grid_smem_ = smem;
+}
+
+// One grid V-cycle: the barrier counters are zeroed by a memset node, then the
+// cooperative launch (no programmatic overlap: its CTAs must all be resident).
+void MgSolver::launch_grid(cudaStream_t s, const void* b) {
+  NB_CUDA(cudaMemsetAsync(grid_sync_, 0, 2 * sizeof(unsigned), s));  // arrivals and the abort flag
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid_ctas_);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = grid_smem_;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  const GridProg* prog = (mixed || b == grid_b_) ? grid_prog_ : grid_prog_alt_;
+  if (mixed)
+    NB_LAUNCH(lc_, "vgrid", s, grid_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vgrid<float, 256>, prog, flags_, maxit_)));
+  else
+    NB_LAUNCH(lc_, "vgrid", s, grid_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vgrid<double, 256>, prog, flags_, maxit_)));
+}
+
 // Minv: z = V-cycle(r) (+ Minv's removeMean), then either p = z, rz = r.z
 // (first) or the flexible-beta dots, then p = z + beta p.
 void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
@@ -2278,13 +2570,20 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
     }
     void* zx = nullptr;
     int zslot = -1;
-    // non-singular: the V-cycle's last sweep also forms z' and the dots
-    fuse_dots_ = !sing;
-    if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
-    else vcycle<double>(s, 0, rnew_, -1, nullptr, &zslot, &zx);
-    fuse_dots_ = false;
+    const bool fused = !sing && !grid_prog_;
+    if (grid_prog_) {
+      launch_grid(s, mixed ? static_cast<const void*>(rnew_f_) : static_cast<const void*>(rnew_));
+      zx = grid_x_;
+      zslot = grid_slot_;
+    } else {
+      // non-singular: the V-cycle's last sweep also forms z' and the dots
+      fuse_dots_ = !sing;
+      if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
+      else vcycle<double>(s, 0, rnew_, -1, nullptr, &zslot, &zx);
+      fuse_dots_ = false;
+    }
     std::swap(p_, p2_);
-    if (!sing) {
+    if (fused) {
       std::swap(r_, rnew_);
       continue;
     }
@@ -2426,8 +2725,15 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit, con
   // z = Minv(r) ; p = z ; rz = r.z
   void* zx = nullptr;
   int zslot = -1;
-  if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
-  else vcycle<double>(s, 0, r_, -1, nullptr, &zslot, &zx);
+  if (grid_prog_) {
+    launch_grid(s, mixed ? static_cast<const void*>(rnew_f_) : static_cast<const void*>(r_));
+    zx = grid_x_;
+    zslot = grid_slot_;
+  } else if (mixed) {
+    vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
+  } else {
+    vcycle<double>(s, 0, r_, -1, nullptr, &zslot, &zx);
+  }
   const double* m1 = (sing && zslot >= 0) ? S_ + zslot : nullptr;
   const double* m2 = sing ? S_ + S_ZMEAN2 : nullptr;
   if (sing) {
@@ -2448,6 +2754,8 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit, con
   lc_.add();
   NB_CUDA(cudaGetLastError());
 }
+
+bool MgSolver::timed_out() const { return h_flags_ && h_flags_->stop == STOP_TIMEOUT; }
 
 nb_poisson_report MgSolver::fetch_report(cudaStream_t s) {
   NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));

@@ -85,6 +85,26 @@ struct TailProg {
   TailPhase ph[MAX_TAIL_PH];
 };
 
+// Grid-resident V-cycle: one cooperative launch runs the whole V-cycle (every
+// level, the coarsest solve included) as a list of phases over all CTAs, with
+// a bounded grid barrier between phases. Vectors stay in global memory (L2);
+// the phases are the launch path's own per-brick code.
+constexpr int MAX_GRID_LEV = 12;
+constexpr int MAX_GRID_PH = 160;
+struct GridProg {
+  int nlev, nphase, singular, nf;
+  const double* inv;  // exact coarsest solve (TAIL_DIRECT)
+  const int* fmap;
+  const int* lexpos;
+  const int* lexcell;
+  double* xs;          // [nf] scratch of the exact coarsest solve
+  unsigned* sync;      // [0] barrier arrivals (zeroed before every launch), [1] abort flag
+  double* partials;    // [grid] per-CTA partial sums of a phase's pending mean
+  SolveFlags* flags;   // stop = STOP_TIMEOUT when a barrier gives up
+  LevelView lv[MAX_GRID_LEV];
+  TailPhase ph[MAX_GRID_PH];
+};
+
 // Initial guess of a solve (instead of x = 0): x0 = alpha * (*dt) * guess on
 // the fluid cells of level 0 (brick layout), e.g. the last projection's
 // pressure scaled to this projection's potential.
@@ -115,6 +135,8 @@ class MgSolver {
   void solve_async(cudaStream_t s, const double* b_dev, double tol, int maxit,
                    double* report = nullptr, const WarmStart* ws = nullptr);
   nb_poisson_report fetch_report(cudaStream_t s);
+  // After fetch_report: a bounded device-side wait of the solve gave up.
+  bool timed_out() const;
   // Issues the whole solve into stream `s`, which must be capturing a graph:
   // the cycle loop becomes a conditional WHILE node (no host round trip).
   // `report` (6 doubles, device) receives iterations, stop code, early-exit
@@ -150,6 +172,8 @@ class MgSolver {
               int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog = nullptr);
   void build_tail();
   void launch_tail(cudaStream_t s);
+  void build_grid();
+  void launch_grid(cudaStream_t s, const void* b);
   void iterate(cudaStream_t s, double tol, int maxit, int count);
   void setup(cudaStream_t s, const double* b, double tol, int maxit, const WarmStart* ws = nullptr);
   void finish(cudaStream_t s, double* report);
@@ -175,6 +199,16 @@ class MgSolver {
   void* tail_x_ = nullptr;         // tail level's result and its pending-mean slot
   int tail_slot_ = -1;
   double tail_bytes_ = 0.0;        // algorithmic bytes of one tail launch
+  bool vgrid_ = false;          // tuning: run each V-cycle as one grid-resident launch
+  GridProg* grid_prog_ = nullptr;  // device; nullptr: per-sweep launches
+  GridProg* grid_prog_alt_ = nullptr;  // FP64: the same program on the other residual buffer
+  const void* grid_b_ = nullptr;       // level-0 rhs grid_prog_ reads
+  int grid_ctas_ = 0;
+  size_t grid_smem_ = 0;
+  double grid_bytes_ = 0.0;       // algorithmic bytes of one grid V-cycle
+  void* grid_x_ = nullptr;        // level-0 result of the grid V-cycle and its pending-mean slot
+  int grid_slot_ = -1;
+  unsigned* grid_sync_ = nullptr;
   bool cheb_ = false;     // mixed form: Chebyshev smoothing instead of damped Jacobi
   double cheb_c2_[4] = {0.8, 0.8, 0.8, 0.8};  // residual weight per sweep of a phase
   double cheb_c1_[4] = {0.0, 0.0, 0.0, 0.0};  // weight of the last step per sweep

@@ -39,6 +39,7 @@ bool tuning_ok(const nb_tuning& t, std::string& why) {
   else if (t.smoother != 0 && t.smoother != 1) why = "smoother must be 0 or 1";
   else if (t.tail_bricks < 0 || t.tail_bricks > 4096) why = "tail_bricks must be in 0..4096";
   else if (t.warm_start != 0 && t.warm_start != 1) why = "warm_start must be 0 or 1";
+  else if (t.vgrid != 0 && t.vgrid != 1) why = "vgrid must be 0 or 1";
   else return true;
   return false;
 }
@@ -61,12 +62,12 @@ std::string tune_key(nb_ctx* ctx, const nb_case* c) {
   return s;
 }
 
-// One cache line: key and the ten fields, then ms per step.
+// One cache line: key and the eleven fields, then ms per step.
 bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double& ms) {
   std::istringstream in(line);
   if (!(in >> key >> t.mg_ctas_per_sm >> t.rhs_ctas_per_sm >> t.halo_mode >> t.sweeps >> t.coarse_direct_max >>
         t.pdl >> t.threads_per_brick >> t.smoother >> t.tail_bricks >>
-        t.warm_start >> ms))
+        t.warm_start >> t.vgrid >> ms))
     return false;
   std::string why;
   return tuning_ok(t, why);
@@ -74,9 +75,9 @@ bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double&
 
 std::string format_line(const std::string& key, const nb_tuning& t, double ms) {
   char buf[320];
-  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
+  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
                 t.rhs_ctas_per_sm, t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, t.smoother,
-                t.tail_bricks, t.warm_start, ms);
+                t.tail_bricks, t.warm_start, t.vgrid, ms);
   return buf;
 }
 
@@ -102,6 +103,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->smoother = 1;
   t->tail_bricks = 8;
   t->warm_start = 1;
+  t->vgrid = 0;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {
@@ -275,7 +277,8 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
     int32_t nb_tuning::*field;
     std::vector<int32_t> values;
   };
-  std::vector<Knob> knobs = {{&nb_tuning::tail_bricks, {0, 8, 32, 128}},
+  std::vector<Knob> knobs = {{&nb_tuning::vgrid, {0, 1}},
+                             {&nb_tuning::tail_bricks, {0, 8, 32, 128}},
                              {&nb_tuning::rhs_ctas_per_sm, {1, 2, 3, 4}},
                              {&nb_tuning::halo_mode, {0, 1}},
                              {&nb_tuning::pdl, {0, 1}}};

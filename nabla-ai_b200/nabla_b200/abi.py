@@ -137,6 +137,7 @@ class Tuning(C.Structure):
         ("smoother", C.c_int32),
         ("tail_bricks", C.c_int32),
         ("warm_start", C.c_int32),
+        ("vgrid", C.c_int32),
     ]
 
     def as_dict(self):

@@ -30,9 +30,16 @@ def replay_into_reference(ref, nb0, lmax, leaves, extra_levels=0):
     for L, bx, by, bz in np.asarray(leaves).tolist():
         s = lmax - L
         a = (bx << s << extra_levels, by << s << extra_levels, bz << s << extra_levels)
-        for m in range(k0, k0 + L + extra_levels):
+        for m in range(k0, k0 + L):  # the leaf's ancestors
             mask = ~((1 << (M - m)) - 1)
             need[m].add(ref.morton_encode(a[0] & mask, a[1] & mask, a[2] & mask))
+        size = 1 << (M - (k0 + L))  # the leaf's extent on the finest grid
+        for m in range(k0 + L, k0 + L + extra_levels):  # every node inside the leaf above its cells
+            step = 1 << (M - m)
+            for z in range(a[2], a[2] + size, step):
+                for y in range(a[1], a[1] + size, step):
+                    for x in range(a[0], a[0] + size, step):
+                        need[m].add(ref.morton_encode(x, y, z))
     for m in range(k0, M):
         if not need[m]:
             continue

@@ -68,9 +68,10 @@ def test_device_maps_equal_reference_on_reference_built_trees(ctx, ref):
         if lev[i] < M:
             t.refine_morton(int(keys[i]))
     keys, lev, _ = t.cells()
+    keys, lev = [int(k) for k in keys], [int(v) for v in lev]
     for i in range(0, len(keys), 8):
         if lev[i] > 2:
-            t.coarsen(int(keys[i]) & ~((1 << (3 * (M - lev[i] + 1))) - 1), int(lev[i]) - 1)
+            t.coarsen(keys[i] & ~((1 << (3 * (M - lev[i] + 1))) - 1), lev[i] - 1)
     assert t.is_balanced()
     keys, lev, _ = t.cells()
     keys, lev = keys.tolist(), lev.tolist()

@@ -171,7 +171,7 @@ def test_graph_and_direct_launch_paths_agree_bitwise(ctx):
     b.initialize()
     for _ in range(3):
         ra = a.step()
-    ctx.lib.nb_ctx_profile(ctx.h, b"smooth")
+    ctx.lib.nb_ctx_profile(ctx.h, b"vgrid" if ctx.tuning["vgrid"] else b"smooth")
     try:
         for _ in range(3):
             rb = b.step()

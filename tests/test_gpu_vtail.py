@@ -52,8 +52,8 @@ def _channel_run(ctx, precision, nsteps=3):
 @pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
 @pytest.mark.parametrize("tail", [2, 16])
 def test_channel_tail_is_bitwise_equal(ctx, precision, tail):
-    ref, it_ref, n_ref = _with_tuning(ctx, dict(tail_bricks=0), lambda: _channel_run(ctx, precision))
-    got, it_got, n_got = _with_tuning(ctx, dict(tail_bricks=tail), lambda: _channel_run(ctx, precision))
+    ref, it_ref, n_ref = _with_tuning(ctx, dict(vgrid=0, tail_bricks=0), lambda: _channel_run(ctx, precision))
+    got, it_got, n_got = _with_tuning(ctx, dict(vgrid=0, tail_bricks=tail), lambda: _channel_run(ctx, precision))
     assert it_got == it_ref
     for a in range(4):
         assert np.array_equal(got[a], ref[a])
@@ -72,8 +72,8 @@ def test_singular_uniform_box_with_cg_coarsest(ctx, precision, tol):
             rep = ns.step(0.05)
             assert rep.converged
         return ns.u_face(), ns.pressure()
-    u0, p0 = _with_tuning(ctx, dict(tail_bricks=0), run)
-    u1, p1 = _with_tuning(ctx, dict(tail_bricks=8), run)
+    u0, p0 = _with_tuning(ctx, dict(vgrid=0, tail_bricks=0), run)
+    u1, p1 = _with_tuning(ctx, dict(vgrid=0, tail_bricks=8), run)
     assert np.abs(u1 - u0).max() <= tol * np.abs(u0).max()
     assert np.abs(p1 - p0).max() <= tol * np.abs(p0).max()
 
@@ -102,8 +102,8 @@ def test_singular_three_level_box_whole_hierarchy_in_the_tail(ctx, precision, to
             rep = ac.step(0.004)
             assert rep.converged and rep.divergence_max <= 1e-8
         return ac.get_state()
-    ref = _with_tuning(ctx, dict(tail_bricks=0), run)
-    got = _with_tuning(ctx, dict(tail_bricks=4096), run)
+    ref = _with_tuning(ctx, dict(vgrid=0, tail_bricks=0), run)
+    got = _with_tuning(ctx, dict(vgrid=0, tail_bricks=4096), run)
     scale = max(np.abs(ref[a]).max() for a in range(3))
     for a in range(3):
         assert np.abs(got[a] - ref[a]).max() <= tol * scale
