@@ -337,6 +337,13 @@ def run_ours(args, rank, world, local_rank):
                                                                 stream, flush, world, device)
         if args.same_case_steps > 0:
             out["same_case_as_reference_arm"] = same_case_as_reference(args, ctx, flush, world, device)
+        if args.serve_seconds > 0:
+            srv = serve_once(args, ctx, prec, 7 + rank, args.serve_seconds + args.serve_grace)
+            out["serving"] = {"workload": serve_config(args), "precision": precision,
+                              **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in srv.items()}}
+            out["latency"] = {"p50_s": round(srv["p50_latency_s"], 4), "p99_s": round(srv["p99_latency_s"], 4),
+                              "served": srv["served"], "arrived": srv["arrived"],
+                              "note": "arrival-to-result latency of the served requests of the `serving` run"}
     return out
 
 
@@ -627,67 +634,89 @@ def run_poisson(args, rank, world, local_rank):
 # serving: open-loop Poisson arrivals through the continuous-batching loop
 # ---------------------------------------------------------------------------
 def serve_requests(args, seed):
+    """Open-loop Poisson arrivals of config-3-sized requests: each a 3-level
+    octree of the periodic Taylor-Green box at effective 128^3, 256^3 or 512^3
+    (165 k, 821 k or 9.58 M leaf cells, drawn uniformly) stepped for U[min, max]
+    SSP-RK3 steps from the Taylor-Green state. Returns (requests, meshes): the
+    payloads exist before the clock starts, as a client's case description
+    would; one mesh per size is built on first use and shared by its cases."""
+    import threading
+
     import numpy as np
 
-    from nabla_b200 import amr, serving, workloads
+    from nabla_b200 import abi, amr, cases, serving, workloads
     rng = np.random.default_rng(seed)
     arrivals = serving.poisson_arrivals(args.rate, args.serve_seconds, seed)
-    # request payloads (mesh leaves, solids, config) exist before the clock
-    # starts, as a client's case description would
-    pool = []
-    s = 0
-    while len(pool) < 64:
-        w = workloads.tgv_box_case(s)
-        if len(w.leaves) * 512 <= args.max_cells:
-            pool.append(w)
-        s += 1
+    bases = [b for b in (32, 64, 128) if b * 4 <= args.max_effective]
+    payloads = {b: workloads.tgv_octree(b) for b in bases}
+    cfg = cases.flow_config(reynolds=1600.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
+                            convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
+    meshes, lock = {}, threading.Lock()
 
-    def builder(w):
+    def builder(base):
         def build(ctx, precision):
-            mesh = amr.AmrMesh(w.geom, w.leaves, solid=w.solid, ctx=ctx)
-            case = amr.AmrCase(mesh, w.config, precision=precision)
-            case.set_state(*w.initial_state(case))
-            case._mesh_keepalive = mesh
+            with lock:
+                if base not in meshes:
+                    geom, leaves = payloads[base]
+                    meshes[base] = amr.AmrMesh(geom, leaves, ctx=ctx)
+            case = amr.AmrCase(meshes[base], cfg, precision=precision)
+            st = []
+            for a in range(3):
+                x, y, z = case.face_positions(a)
+                st.append(np.sin(x) * np.cos(y) * np.cos(z) if a == 0 else
+                          (-np.cos(x) * np.sin(y) * np.cos(z) if a == 1 else np.zeros_like(x)))
+            st.append(np.zeros(case.sizes[3]))
+            case.set_state(*st)
             return case
         return build
 
     reqs = []
     for i, t in enumerate(arrivals):
-        w = pool[int(rng.integers(len(pool)))]
+        base = bases[int(rng.integers(len(bases)))]
         steps = int(rng.integers(args.min_steps, args.max_steps + 1))
-        reqs.append(serving.Request(i, float(t), steps, builder(w), len(w.leaves) * 512))
-    return reqs
+        reqs.append(serving.Request(i, float(t), steps, builder(base), len(payloads[base][1]) * 512))
+    return reqs, meshes
+
+
+def serve_once(args, ctx, prec, seed, time_limit):
+    from nabla_b200 import serving
+    reqs, meshes = serve_requests(args, seed)
+    st = serving.Server(ctx, hbm_budget=150e9, precision=prec, slots=args.slots,
+                        builders=args.builders).run(reqs, time_limit=time_limit)
+    for m in meshes.values():
+        m.close()
+    s = st.summary()
+    s["unfinished"] = s["arrived"] - s["served"] - s["cancelled"]
+    return s
+
+
+def serve_config(args):
+    return (f"serving: open-loop Poisson arrivals at {args.rate}/s for {args.serve_seconds} s; each request a 3-level "
+            f"octree of the periodic Taylor-Green box at effective 128^3, 256^3 or 512^3 (config-3 meshes, 165 k / "
+            f"821 k / 9.58 M leaf cells), {args.min_steps}-{args.max_steps} steps, HBM budget 150 GB, continuous "
+            f"batching ({args.slots} slots, each case collected and relaunched on its own completion, cases built on "
+            f"{args.builders} host threads); the loop stops {args.serve_grace} s after the last arrival")
 
 
 def run_serve(args, rank, world, local_rank):
     import torch
 
-    from nabla_b200 import abi, serving, solver
+    from nabla_b200 import abi, solver
     torch.cuda.set_device(local_rank)
     ctx = solver.Context(local_rank)
     forms = {}
     for name, prec in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
-        reqs = serve_requests(args, 7 + rank)
         with ClockSampler(local_rank) as clk:
-            st = serving.Server(ctx, hbm_budget=150e9, precision=prec, slots=args.slots,
-                                builders=args.builders).run(
-                reqs, time_limit=args.serve_seconds * 2)
-        s = st.summary()
+            s = serve_once(args, ctx, prec, 7 + rank, args.serve_seconds + args.serve_grace)
         s["clocks"] = clk.summary()
-        s["divergence_max"] = None
         forms[name] = s
     primary = forms[args.precision or "mixed"]
     return {
         "metric": METRIC, "value": round(primary["mcell_steps_per_s"], 4), "unit": UNIT, "n_gpus": world,
         "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if (args.precision or "mixed") == "mixed" else "f64",
-        "data": "synthetic (seeded Poisson arrivals of seeded octree TGV boxes)",
-        "config": {"workload": f"serving: Poisson arrivals at {args.rate}/s for {args.serve_seconds} s, each request "
-                               f"an octree TGV box (<= {args.max_cells} leaf cells) for {args.min_steps}-"
-                               f"{args.max_steps} steps, HBM budget 150 GB, continuous batching "
-                               f"(per-case step graphs overlapped on the device, {args.slots} slots, cases built "
-                               f"on {args.builders} host threads); the loop runs for twice the arrival window",
-                   "precision": args.precision or "mixed"},
+        "data": "synthetic (seeded Poisson arrivals of Taylor-Green octree requests)",
+        "config": {"workload": serve_config(args), "precision": args.precision or "mixed"},
         "latency": {"p50_s": round(primary["p50_latency_s"], 4), "p99_s": round(primary["p99_latency_s"], 4)},
         "forms": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items() if kk != "clocks"}
                   for k, v in forms.items()},
@@ -806,12 +835,14 @@ def main():
                     default=None, help="fixed nb_tuning fields, e.g. threads_per_brick=128,mg_ctas_per_sm=9 "
                     "(channel3, tgv64, batch96)")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
-    ap.add_argument("--serve-seconds", type=float, default=20.0, help="serve: arrival window")
+    ap.add_argument("--serve-seconds", type=float, default=20.0,
+                    help="serve (and the default line's serving key, 0 skips it): arrival window")
+    ap.add_argument("--serve-grace", type=float, default=10.0, help="serve: seconds the loop runs after the window")
     ap.add_argument("--min-steps", type=int, default=10)
-    ap.add_argument("--max-steps", type=int, default=40)
-    ap.add_argument("--max-cells", type=int, default=300_000, help="serve: leaf-cell cap per request")
+    ap.add_argument("--max-steps", type=int, default=200)
+    ap.add_argument("--max-effective", type=int, default=512, help="serve: largest effective request size (128/256/512)")
     ap.add_argument("--slots", type=int, default=32, help="serve: cases in flight at most")
-    ap.add_argument("--builders", type=int, default=2, help="serve: host threads that build admitted cases")
+    ap.add_argument("--builders", type=int, default=4, help="serve: host threads that build admitted cases")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)

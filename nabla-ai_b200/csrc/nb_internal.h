@@ -138,6 +138,8 @@ enum Slot : int {
   S_FY,
   S_MASS,
   S_MAXINV,
+  S_IRRES2,     // iterative refinement: true residual sum of squares
+  S_IRMEAN,     // iterative refinement: fluid mean of the true residual (singular)
   S_LVL_MEAN = 24,  // [MAX_LEVELS][4]: per-level pending means (x ping, x pong, b)
   S_COUNT = S_LVL_MEAN + MAX_LEVELS * 4
 };
@@ -149,6 +151,8 @@ struct SolveFlags {
   int iters;     // completed MG-PCG cycles
   int early;     // rhs already below tolerance
   int nan;       // NaN seen in a reduction
+  int restarts;  // iterative-refinement restarts of this solve (mixed form)
+  int checked;   // the true residual met the tolerance: no further refinement checks
 };
 
 // Reduction scratch: per-block partials + a ticket counter (last-block

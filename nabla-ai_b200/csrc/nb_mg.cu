@@ -1325,6 +1325,8 @@ __global__ void __launch_bounds__(NT) k_pcg_setup(LevelView L, const double* __r
     S[S_BNORM2] = t[0];
     const double bnorm = sqrt(t[0]) + 1e-300;
     flags->iters = 0;
+    flags->restarts = 0;
+    flags->checked = 0;
     flags->nan = isnan(t[0]) ? 1 : 0;
     if (sqrt(t[0]) <= tol * bnorm || isnan(t[0])) {
       flags->stop = 1;
@@ -1381,6 +1383,8 @@ __global__ void __launch_bounds__(NT) k_pcg_setup_warm(LevelView L, const double
     S[S_BNORM2] = t[0];
     const double bnorm = sqrt(t[0]) + 1e-300;
     flags->iters = 0;
+    flags->restarts = 0;
+    flags->checked = 0;
     flags->nan = isnan(t[0]) ? 1 : 0;
     if (sqrt(t[0]) <= tol * bnorm || isnan(t[0])) {
       flags->stop = 1;
@@ -1601,6 +1605,83 @@ __global__ void __launch_bounds__(NT) k_true_residual(LevelView L, const double*
 
 // Loop condition of the graph form: keep cycling while not converged, not
 // broken down and under the cycle cap.
+// Outer iterative refinement (mixed form). The flexible PCG updates its FP64
+// residual recursively; once it stops converged, the FP64 true residual
+// rhs - A x decides: above tol |rhs| (and within kMaxRefine restarts and the
+// cycle cap) the solve restarts from x with that residual, mean-removed on
+// singular systems (multigrid.cpp:341-353 computes the same residual, for
+// the report only). k_ir_residual forms the residual into `rt` and decides in
+// its finaliser (stop back to 0 and restarts + 1 to restart); inside a graph
+// it also sets the restart branch (h_if) and the second cycle loop (h_loop).
+constexpr int kMaxRefine = 2;
+__global__ void __launch_bounds__(NT) k_ir_residual(LevelView L, const double* __restrict__ x,
+                                                    const double* __restrict__ rhs, double* __restrict__ rt,
+                                                    RedBuf rb, double* S, SolveFlags* flags, double tol, int maxit,
+                                                    double inv_nf, int cond, cudaGraphConditionalHandle h_if,
+                                                    cudaGraphConditionalHandle h_loop) {
+  pdl_wait();
+  const bool act = flags->stop == 1 && !flags->early && !flags->checked && flags->iters < maxit &&
+                   flags->restarts < kMaxRefine;
+  if (!act) {
+    if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
+      cudaGraphSetConditional(h_if, 0u);
+      cudaGraphSetConditional(h_loop, 0u);
+    }
+    return;
+  }
+  DFetch X{x, nullptr};
+  __shared__ double tile[TSN];
+  double part[2] = {0.0, 0.0};
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    fill_halo<double>(L, brick, tile, X);
+    __syncthreads();
+    const int c = brick * BR3 + threadIdx.x;
+    const uint32_t code = L.code[c];
+    double e = 0.0;
+    if (code_type(code) == CELL_FLUID) {
+      double diag, off;
+      full_row<double>(L, code, tile, brick, c, X, diag, off);
+      e = rhs[c] - (diag * tile[tpos_local(threadIdx.x)] - off);
+    }
+    rt[c] = e;
+    const double w = cell_weight(L, brick);
+    part[0] += w * (e * e);
+    part[1] += w * e;
+    __syncthreads();
+  }
+  grid_reduce<2>(part, rb, [=] __device__(const double* t) {
+    S[S_IRRES2] = t[0];
+    S[S_IRMEAN] = t[1] * inv_nf;
+    const bool again = t[0] > tol * tol * S[S_BNORM2];
+    if (again) {
+      flags->stop = 0;
+      flags->restarts += 1;
+    } else {
+      flags->checked = 1;
+    }
+    if (cond) {
+      cudaGraphSetConditional(h_if, again ? 1u : 0u);
+      cudaGraphSetConditional(h_loop, again ? 1u : 0u);
+    }
+  });
+}
+
+// The restart: r = true residual (fluid mean removed when singular) and its
+// FP32 copy for the V-cycle; then the first direction as at the start.
+__global__ void __launch_bounds__(NT) k_ir_restart(LevelView L, const double* __restrict__ rt, double* __restrict__ r,
+                                                   float* __restrict__ rf, const double* S, const SolveFlags* flags,
+                                                   int sing, int maxit) {
+  pdl_wait();
+  if (stopped(flags, maxit)) return;
+  const double m = sing ? S[S_IRMEAN] : 0.0;
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int c = brick * BR3 + threadIdx.x;
+    const double v = L.type[c] == CELL_FLUID ? rt[c] - m : 0.0;
+    r[c] = v;
+    if (rf) rf[c] = static_cast<float>(v);
+  }
+}
+
 __global__ void k_set_cond(cudaGraphConditionalHandle h, const SolveFlags* f, int maxit,
                            unsigned long long* execs) {
   cudaGraphSetConditional(h, (f->stop == 0 && f->iters < maxit) ? 1u : 0u);
@@ -2617,15 +2698,33 @@ void MgSolver::solve_async(cudaStream_t s, const double* b, double tol, int maxi
   setup(s, b, tol, maxit, ws);
   // Iterate in batches; every kernel returns at once after convergence, so
   // over-issuing costs only launch latency. The batch grows geometrically.
+  // The mixed form then checks the true residual and may restart (outer
+  // iterative refinement, at most kMaxRefine times).
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  const LevelView& L = lv_[0].v;
+  const int grid = grid_of(L.nbrick);
+  const bool sing = singular_ && lv_[0].h.nfluid > 0;
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
   int issued = 0, batch = 4;
-  while (issued < maxit) {
-    const int cnt = std::min(batch, maxit - issued + (maxit - issued) % 2);
-    iterate(s, tol, maxit, cnt);
-    issued += cnt;
+  for (int round = 0;; ++round) {
+    while (issued < maxit) {
+      const int cnt = std::min(batch, maxit - issued + (maxit - issued) % 2);
+      iterate(s, tol, maxit, cnt);
+      issued += cnt;
+      NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
+      NB_CUDA(cudaStreamSynchronize(s));
+      if (h_flags_->stop != 0 || h_flags_->iters >= maxit) break;
+      batch = std::min(batch * 2, 16);
+    }
+    if (!mixed || round >= kMaxRefine) break;
+    NB_LAUNCH(lc_, "ir_residual", s, lv_[0].ncell * 27,
+              (k_ir_residual<<<grid, NT, 0, s>>>(L, x_, rhs_, rnew_, rb_, S_, flags_, tol, maxit, inv_nf, 0, 0, 0)));
     NB_CUDA(cudaMemcpyAsync(h_flags_, flags_, sizeof(SolveFlags), cudaMemcpyDeviceToHost, s));
     NB_CUDA(cudaStreamSynchronize(s));
-    if (h_flags_->stop != 0 || h_flags_->iters >= maxit) break;
-    batch = std::min(batch * 2, 16);
+    if (h_flags_->stop != 0 || h_flags_->iters >= maxit) break;  // no restart (converged on the true residual too)
+    k_ir_restart<<<grid, NT, 0, s>>>(L, rnew_, r_, rnew_f_, S_, flags_, sing ? 1 : 0, maxit);
+    lc_.add();
+    first_direction(s);
   }
   finish(s, report);
 }
@@ -2665,7 +2764,65 @@ void MgSolver::capture_solve(cudaStream_t s, const double* b, double tol, int ma
   lc_.count = saved;
   if (body_kernels) *body_kernels = nbody.load();
   NB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  if (precision_ == NB_PRECISION_MIXED)
+    for (int k = 0; k < kMaxRefine; ++k) capture_refinement(s, tol, maxit);
   finish(s, report);
+}
+
+// Outer iterative refinement inside the captured solve (mixed form): the true
+// residual decides (k_ir_residual), an IF node holds the restart (residual,
+// first direction) and a second WHILE node the cycles after it. Their bodies'
+// kernels run only after a restart and are not counted as launches of a
+// normal solve.
+void MgSolver::capture_refinement(cudaStream_t s, double tol, int maxit) {
+  const LevelView& L = lv_[0].v;
+  const int grid = grid_of(L.nbrick);
+  const bool sing = singular_ && lv_[0].h.nfluid > 0;
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  NB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphConditionalHandle h_if, h_loop;
+  NB_CUDA(cudaGraphConditionalHandleCreate(&h_if, g, 0, cudaGraphCondAssignDefault));
+  NB_CUDA(cudaGraphConditionalHandleCreate(&h_loop, g, 0, cudaGraphCondAssignDefault));
+  NB_LAUNCH(lc_, "ir_residual", s, lv_[0].ncell * 27,
+            (k_ir_residual<<<grid, NT, 0, s>>>(L, x_, rhs_, rnew_, rb_, S_, flags_, tol, maxit, inv_nf, 1, h_if,
+                                                h_loop)));
+  std::atomic<uint64_t>* saved = lc_.count;
+  std::atomic<uint64_t> rare{0};
+  // IF: the restart
+  NB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams pi{};
+  pi.type = cudaGraphNodeTypeConditional;
+  pi.conditional.handle = h_if;
+  pi.conditional.type = cudaGraphCondTypeIf;
+  pi.conditional.size = 1;
+  cudaGraphNode_t if_node;
+  NB_CUDA(cudaGraphAddNode(&if_node, g, deps, nd, &pi));
+  lc_.count = &rare;
+  NB_CUDA(cudaStreamBeginCaptureToGraph(side_, pi.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeRelaxed));
+  k_ir_restart<<<grid, NT, 0, side_>>>(L, rnew_, r_, rnew_f_, S_, flags_, sing ? 1 : 0, maxit);
+  first_direction(side_);
+  cudaGraph_t out = nullptr;
+  NB_CUDA(cudaStreamEndCapture(side_, &out));
+  // WHILE: the cycles after a restart
+  cudaGraphNodeParams pw{};
+  pw.type = cudaGraphNodeTypeConditional;
+  pw.conditional.handle = h_loop;
+  pw.conditional.type = cudaGraphCondTypeWhile;
+  pw.conditional.size = 1;
+  cudaGraphNode_t loop_node;
+  NB_CUDA(cudaGraphAddNode(&loop_node, g, &if_node, 1, &pw));
+  NB_CUDA(cudaStreamBeginCaptureToGraph(side_, pw.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeRelaxed));
+  iterate(side_, tol, maxit, 2);
+  k_set_cond<<<1, 1, 0, side_>>>(h_loop, flags_, maxit, nullptr);
+  NB_CUDA(cudaStreamEndCapture(side_, &out));
+  lc_.count = saved;
+  NB_CUDA(cudaStreamUpdateCaptureDependencies(s, &loop_node, 1, cudaStreamSetCaptureDependencies));
 }
 
 void MgSolver::finish(cudaStream_t s, double* report) {
@@ -2722,7 +2879,17 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit, con
     k_pcg_setup<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, rhs_, r_, x_,
                                     mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);
   lc_.add();
-  // z = Minv(r) ; p = z ; rz = r.z
+  first_direction(s);
+}
+
+// z = Minv(r) ; p = z ; rz = r.z (the first cycle, and every refinement restart)
+void MgSolver::first_direction(cudaStream_t s) {
+  const LevelView& L = lv_[0].v;
+  const int grid = grid_of(L.nbrick);
+  const double inv_nf = lv_[0].h.nfluid ? 1.0 / lv_[0].wfluid : 0.0;
+  const bool sing = singular_ && lv_[0].h.nfluid > 0;
+  const bool mixed = precision_ == NB_PRECISION_MIXED;
+  const int maxit = maxit_;
   void* zx = nullptr;
   int zslot = -1;
   if (grid_prog_) {

@@ -176,6 +176,8 @@ class MgSolver {
   void launch_grid(cudaStream_t s, const void* b);
   void iterate(cudaStream_t s, double tol, int maxit, int count);
   void setup(cudaStream_t s, const double* b, double tol, int maxit, const WarmStart* ws = nullptr);
+  void first_direction(cudaStream_t s);
+  void capture_refinement(cudaStream_t s, double tol, int maxit);
   void finish(cudaStream_t s, double* report);
   void upload_uniform(DevLevel& D, const int bcs[6]);
   void upload_amr(DevLevel& D, const AmrLevelHost& A, const int bcs[6]);
