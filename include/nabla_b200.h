@@ -350,6 +350,18 @@ nb_status nb_amr_tree_maps(const nb_amr_geom* g, const int32_t* leaves, int64_t 
 nb_status nb_amr_mesh_couplings(const nb_amr_mesh* m, int64_t* count, int32_t* off, int32_t* nbr, double* coef,
                                 int64_t cap);
 
+/* The same refinement as nb_amr_refine (split the flagged leaves below lmax,
+ * then restore 26-neighbour 2:1 balance), computed on the device: leaves are
+ * ranked by a device sort of their keys, every split leaf marks the touching
+ * leaves two or more levels coarser than its children through binary searches
+ * in the sorted keys, round by round until nothing changes (at most lmax + 1
+ * rounds), and the new leaves are emitted and ranked on the device. `out`
+ * receives them in rank order; same error and capacity convention as
+ * nb_amr_refine. Replaces Octree::refineByMorton with its balance
+ * (core/src/mesh/octree.cpp:325-356) at brick granularity. */
+nb_status nb_amr_refine_device(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* leaves, int64_t n,
+                               const uint8_t* flags, int32_t* out, int64_t cap, int64_t* n_out);
+
 /* ---- MAC step on an octree-AMR mesh ------------------------------------------
  * NSSolver (core/include/nabla/flow/ns_solver.hpp:58-96) on the composite
  * mesh: the same SSP-RK3 / WENO-5 / MG-PCG step, with the octree face rule of
@@ -381,6 +393,14 @@ nb_status nb_amr_coarsen(const nb_amr_geom* g, const int32_t* leaves, int64_t n,
  * leaf r's fluid cells of |vorticity|, sqrt(2 S:S), Q and |grad p| (cell-centred
  * values, central differences inside the brick, one-sided on its faces). */
 nb_status nb_amr_case_sensors(nb_case* c, double* out);
+/* Regrid refinement on the device: the case's sensors (as nb_amr_case_sensors,
+ * never leaving the device) flag the leaves whose sensor `sensor` exceeds
+ * `above` (below lmax), and nb_amr_refine_device's split, balance and ranking
+ * run on them. `out` receives the new leaves in rank order (4 int32 each);
+ * `n_out` always receives their count (NB_ERR_BAD_ARG if cap is too small).
+ * The sensor and split rules of PhysicalSensorEvaluator / Octree::refine
+ * (core/src/adaptive/adaptive_core.cpp:96-113, core/src/mesh/octree.cpp:288-356). */
+nb_status nb_amr_case_refine(nb_case* c, int sensor, double above, int32_t* out, int64_t cap, int64_t* n_out);
 /* Regrid transfer: dst (a fresh case on a mesh from nb_amr_refine or
  * nb_amr_coarsen of src's mesh: same geometry, at most one level apart at every
  * leaf) takes src's state and step clock. Every face dst stores takes src's

@@ -14,6 +14,7 @@
 #include "nb_amr_flow.cuh"
 #include "nb_amr_mesh.h"
 #include "nb_ctx.h"
+#include "nb_maps.h"
 #include "nb_flow.cuh"
 #include "nb_mg.cuh"
 
@@ -1073,6 +1074,28 @@ nb_status nb_amr_case_sensors(nb_case* c, double* out) {
     ++c->ctx->launches;
     NB_CUDA(cudaMemcpyAsync(out, c->ctx->stage_a, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NB_OK;
+  });
+}
+
+nb_status nb_amr_case_refine(nb_case* c, int sensor, double above, int32_t* out, int64_t cap, int64_t* n_out) {
+  if (!c || !c->amr || sensor < 0 || sensor > 3 || !n_out) return NB_ERR_BAD_ARG;
+  if (c->pending) return fail(c->ctx, NB_ERR_BAD_ARG, "nb_amr_case_refine: the case has a step in flight");
+  return guarded(c->ctx, [&] {
+    NB_CUDA(cudaSetDevice(c->ctx->device));
+    const int n = c->fm.nbrick;
+    ensure_staging(c->ctx, static_cast<size_t>(n) * 4);
+    double** f = c->uvw[c->cur];
+    launch_amr_sensors(c->stream, c->AF, f[0], f[1], f[2], c->p, c->ctx->stage_a);
+    ++c->ctx->launches;
+    const auto& L = c->mesh->lvl.tree.leaves;
+    std::vector<int32_t> h(4 * static_cast<size_t>(n));
+    for (int r = 0; r < n; ++r) {
+      h[4 * r] = L[r].level;
+      for (int a = 0; a < 3; ++a) h[4 * r + 1 + a] = L[r].b[a];
+    }
+    refine_from_sensors(c->ctx, c->stream, c->mesh->geom, h.data(), n, c->ctx->stage_a, sensor, above, out, cap,
+                        n_out);
     return NB_OK;
   });
 }

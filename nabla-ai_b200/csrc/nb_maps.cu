@@ -20,6 +20,10 @@
 // Host export (nb_amr_mesh_maps): the same table from a mesh's own tree, its
 // rank order and per-level lookup tables (the maps the flow and multigrid
 // kernels are built from), so the two routes check each other.
+// Device refinement (nb_amr_refine_device, nb_amr_case_refine): split marks by
+// rank, rounds of 26-neighbour 2:1 balance through the same binary searches,
+// a one-CTA scan of the output counts, the children emitted, then ranked by
+// the same sort.
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -28,6 +32,7 @@
 #include "nb_amr_level.h"
 #include "nb_amr_mesh.h"
 #include "nb_ctx.h"
+#include "nb_maps.h"
 #include "nb_morton.h"
 
 using namespace nb;
@@ -155,6 +160,102 @@ __global__ void k_face_nbrs(int n, const unsigned long long* keys, const int4* r
   for (int q = 0; q < 4; ++q) nbr[4 * t + q] = out[q];
 }
 
+// ---- refinement on the device ----------------------------------------------
+// The leaf of level <= L holding level-L brick c (coarser-or-equal search),
+// or -1 when finer leaves cover it.
+__device__ int holder(const unsigned long long* keys, const int* lev, int n, const MapGeom& g, int L, const int c[3]) {
+  for (int l = L; l >= 0; --l) {
+    const int s = L - l, u = g.lmax - l;
+    const unsigned long long key = morton_encode(static_cast<uint32_t>(c[0] >> s) << u,
+                                                 static_cast<uint32_t>(c[1] >> s) << u,
+                                                 static_cast<uint32_t>(c[2] >> s) << u);
+    const int q = find_leaf(keys, lev, n, key, l);
+    if (q >= 0) return q;
+  }
+  return -1;
+}
+
+// Split marks by rank: mark[r] = flag of the input leaf, below lmax only.
+__global__ void k_rank_marks(int n, const int* pos, const uint8_t* flags, const int* lev, int lmax, uint8_t* mark) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n) mark[r] = (flags[pos[r]] != 0 && lev[r] < lmax) ? 1 : 0;
+}
+
+// One round of 26-neighbour 2:1 balance: a leaf that splits (children at
+// L+1) forces every touching leaf of level <= L-1 to split too (the closure
+// nb_amr_refine's host balance reaches; Octree::refineByMorton's rule,
+// core/src/mesh/octree.cpp:325-356, over faces, edges and corners).
+__global__ void k_balance_round(int n, const unsigned long long* keys, const int4* ranked, const int* lev, MapGeom g,
+                                uint8_t* mark, int* changed) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n || !mark[r]) return;
+  const int4 f = ranked[r];
+  const int L = f.x;
+  if (L == 0) return;
+  for (int d = 0; d < 27; ++d) {
+    if (d == 13) continue;
+    int c[3] = {f.y + d % 3 - 1, f.z + (d / 3) % 3 - 1, f.w + d / 9 - 1};
+    bool inside = true;
+    for (int a = 0; a < 3; ++a) {
+      const int ext = g.nb0[a] << L;
+      if (c[a] < 0 || c[a] >= ext) {
+        if (g.per[a]) c[a] = (c[a] + ext) % ext;
+        else inside = false;
+      }
+    }
+    if (!inside) continue;
+    const int q = holder(keys, lev, n, g, L, c);
+    if (q >= 0 && lev[q] <= L - 1 && !mark[q]) {
+      mark[q] = 1;
+      *changed = 1;
+    }
+  }
+}
+
+// Exclusive scan of the output counts (8 for a split leaf, 1 otherwise) in
+// one CTA: each thread sums a contiguous run of ranks, the CTA scans the run
+// sums, each thread writes its run's offsets. total[0] = the new leaf count.
+__global__ void __launch_bounds__(1024) k_emit_offsets(int n, const uint8_t* mark, int* off, int* total) {
+  __shared__ int sums[1024];
+  const int t = threadIdx.x, per = (n + 1023) / 1024;
+  const int lo = min(n, t * per), hi = min(n, lo + per);
+  int acc = 0;
+  for (int r = lo; r < hi; ++r) acc += mark[r] ? 8 : 1;
+  sums[t] = acc;
+  __syncthreads();
+  for (int w = 1; w < 1024; w <<= 1) {  // inclusive Hillis-Steele scan
+    const int v = t >= w ? sums[t - w] : 0;
+    __syncthreads();
+    sums[t] += v;
+    __syncthreads();
+  }
+  int run = t ? sums[t - 1] : 0;
+  for (int r = lo; r < hi; ++r) {
+    off[r] = run;
+    run += mark[r] ? 8 : 1;
+  }
+  if (t == 1023) *total = sums[1023];
+}
+
+__global__ void k_emit_leaves(int n, const int4* ranked, const uint8_t* mark, const int* off, int4* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int4 f = ranked[r];
+  if (!mark[r]) {
+    out[off[r]] = f;
+    return;
+  }
+  for (int o = 0; o < 8; ++o)
+    out[off[r] + o] = make_int4(f.x + 1, 2 * f.y + (o & 1), 2 * f.z + ((o >> 1) & 1), 2 * f.w + (o >> 2));
+}
+
+// Marks from a per-leaf sensor array (4 values per leaf in rank order).
+__global__ void k_sensor_marks(int n, const double* sensors, int which, double above, const int4* ranked, int lmax,
+                               uint8_t* flags) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n) flags[r] = (sensors[4 * r + which] > above && ranked[r].x < lmax) ? 1 : 0;
+}
+
 MapGeom map_geom(const nb_amr_geom& g) {
   MapGeom m{};
   for (int a = 0; a < 3; ++a) {
@@ -227,7 +328,133 @@ void export_tree_maps(const AmrTree& t, uint64_t* keys, int32_t* ranked, int32_t
   }
 }
 
+// Device buffers of one call, freed after the stream has drained.
+class DevArena {
+ public:
+  explicit DevArena(cudaStream_t s) : s_(s) {}
+  ~DevArena() {
+    cudaStreamSynchronize(s_);
+    for (void* q : bufs_) cudaFree(q);
+  }
+  template <typename T>
+  T* get(size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, count ? count * sizeof(T) : 16) != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw ApiError{NB_ERR_OOM, "octree maps: device allocation failed"};
+    }
+    bufs_.push_back(p);
+    return static_cast<T*>(p);
+  }
+
+ private:
+  cudaStream_t s_;
+  std::vector<void*> bufs_;
+};
+
+struct Sorted {
+  unsigned long long* keys;  // [npad], ascending; the first n are the leaves' keys
+  int* pos;                  // [npad] input position of rank r
+  int4* ranked;              // [n] leaves in rank order
+  int* lev;                  // [n] their levels
+};
+
+unsigned blocks_of(long long m) { return static_cast<unsigned>((m + 255) / 256); }
+
+// Keys, the bitonic rank sort, the unique-anchor check and the ranked leaves.
+Sorted sort_leaves(nb_ctx* ctx, cudaStream_t s, const MapGeom& g, const int4* d_leaves, int n, int* d_err,
+                   DevArena& A) {
+  int npad = 1;
+  while (npad < n) npad <<= 1;
+  Sorted S{A.get<unsigned long long>(npad), A.get<int>(npad), A.get<int4>(n), A.get<int>(n)};
+  k_keys<<<blocks_of(npad), 256, 0, s>>>(n, npad, d_leaves, g, S.keys, S.pos, d_err);
+  ctx->launches++;
+  for (int k = 2; k <= npad; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      k_bitonic<<<blocks_of(npad), 256, 0, s>>>(npad, j, k, S.keys, S.pos);
+      ctx->launches++;
+    }
+  k_unique<<<blocks_of(n), 256, 0, s>>>(n, S.keys, d_err);
+  k_ranked<<<blocks_of(n), 256, 0, s>>>(n, S.pos, d_leaves, S.ranked, S.lev);
+  ctx->launches += 2;
+  NB_CUDA(cudaGetLastError());
+  return S;
+}
+
+void face_table(nb_ctx* ctx, cudaStream_t s, const MapGeom& g, const Sorted& S, int n, int* d_nbr, int* d_nnbr) {
+  k_face_nbrs<<<blocks_of(6LL * n), 256, 0, s>>>(n, S.keys, S.ranked, S.lev, g, d_nbr, d_nnbr);
+  ctx->launches++;
+  NB_CUDA(cudaGetLastError());
+}
+
+void check_err(int h_err, const char* who) {
+  if (h_err == 2) throw ApiError{NB_ERR_BAD_ARG, std::string(who) + ": a leaf lies outside the geometry"};
+  if (h_err == 1) throw ApiError{NB_ERR_BAD_ARG, std::string(who) + ": two leaves share an anchor"};
+}
+
+// Splits the flagged leaves and restores 26-neighbour 2:1 balance on the
+// device, then ranks the new leaves; writes them to the host array `out` in
+// rank order. `flags_ranked`: the flags are per rank of the input (already
+// sorted) instead of per input position.
+void refine_on_device(nb_ctx* ctx, cudaStream_t s, const MapGeom& g, const int4* d_leaves, int n,
+                      const uint8_t* d_flags, bool flags_ranked, int* d_err, DevArena& A, int32_t* out, int64_t cap,
+                      int64_t* n_out) {
+  const Sorted S = sort_leaves(ctx, s, g, d_leaves, n, d_err, A);
+  uint8_t* mark = A.get<uint8_t>(n);
+  if (flags_ranked) {
+    NB_CUDA(cudaMemcpyAsync(mark, d_flags, n, cudaMemcpyDeviceToDevice, s));
+  } else {
+    k_rank_marks<<<blocks_of(n), 256, 0, s>>>(n, S.pos, d_flags, S.lev, g.lmax, mark);
+    ctx->launches++;
+  }
+  int* changed = A.get<int>(1);
+  int h_changed = 1;
+  // every round moves the splits at least one level coarser: lmax rounds settle it
+  for (int round = 0; h_changed && round <= g.lmax + 1; ++round) {
+    NB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int), s));
+    k_balance_round<<<blocks_of(n), 256, 0, s>>>(n, S.keys, S.ranked, S.lev, g, mark, changed);
+    ctx->launches++;
+    NB_CUDA(cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaStreamSynchronize(s));
+  }
+  if (h_changed) throw ApiError{NB_ERR_BAD_ARG, "octree refinement: balance did not settle (unbalanced input)"};
+  int* off = A.get<int>(n);
+  int* total = A.get<int>(1);
+  k_emit_offsets<<<1, 1024, 0, s>>>(n, mark, off, total);
+  int m = 0;
+  NB_CUDA(cudaMemcpyAsync(&m, total, sizeof(int), cudaMemcpyDeviceToHost, s));
+  NB_CUDA(cudaStreamSynchronize(s));
+  int4* fresh = A.get<int4>(m);
+  k_emit_leaves<<<blocks_of(n), 256, 0, s>>>(n, S.ranked, mark, off, fresh);
+  ctx->launches += 2;
+  const Sorted R = sort_leaves(ctx, s, g, fresh, m, d_err, A);
+  int h_err = 0;
+  NB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  NB_CUDA(cudaStreamSynchronize(s));
+  check_err(h_err, "octree refinement");
+  *n_out = m;
+  if (!out || cap < m) throw ApiError{NB_ERR_BAD_ARG, "octree refinement: output capacity too small"};
+  NB_CUDA(cudaMemcpyAsync(out, R.ranked, sizeof(int4) * m, cudaMemcpyDeviceToHost, s));
+  NB_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace
+
+void nb::refine_from_sensors(nb_ctx* ctx, cudaStream_t s, const nb_amr_geom& g, const int32_t* leaves, int n,
+                             const double* d_sensors, int which, double above, int32_t* out, int64_t cap,
+                             int64_t* n_out) {
+  const MapGeom mg = map_geom(g);
+  DevArena A(s);
+  int4* d_leaves = A.get<int4>(n);
+  uint8_t* d_flags = A.get<uint8_t>(n);
+  int* d_err = A.get<int>(1);
+  NB_CUDA(cudaMemcpyAsync(d_leaves, leaves, sizeof(int4) * n, cudaMemcpyHostToDevice, s));
+  NB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  k_sensor_marks<<<blocks_of(n), 256, 0, s>>>(n, d_sensors, which, above, d_leaves, mg.lmax, d_flags);
+  ctx->launches++;
+  // the mesh's leaves are already in rank order, so the flags are by rank
+  refine_on_device(ctx, s, mg, d_leaves, n, d_flags, true, d_err, A, out, cap, n_out);
+}
 
 extern "C" {
 
@@ -248,61 +475,45 @@ nb_status nb_amr_build_maps(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* le
   return guarded(ctx, [&] {
     NB_CUDA(cudaSetDevice(ctx->device));
     const int nn = static_cast<int>(n);
-    int npad = 1;
-    while (npad < nn) npad <<= 1;
     const MapGeom mg = map_geom(*g);
-    std::vector<void*> bufs;
-    auto dalloc = [&](size_t bytes) {
-      void* p = nullptr;
-      if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) {
-        (void)cudaGetLastError();
-        for (void* q : bufs) cudaFree(q);
-        throw ApiError{NB_ERR_OOM, "nb_amr_build_maps: device allocation failed"};
-      }
-      bufs.push_back(p);
-      return p;
-    };
-    int4* d_leaves = static_cast<int4*>(dalloc(sizeof(int4) * nn));
-    int4* d_ranked = static_cast<int4*>(dalloc(sizeof(int4) * nn));
-    unsigned long long* d_keys = static_cast<unsigned long long*>(dalloc(sizeof(unsigned long long) * npad));
-    int* d_pos = static_cast<int*>(dalloc(sizeof(int) * npad));
-    int* d_lev = static_cast<int*>(dalloc(sizeof(int) * nn));
-    int* d_nbr = static_cast<int*>(dalloc(sizeof(int) * 24 * static_cast<size_t>(nn)));
-    int* d_nnbr = static_cast<int*>(dalloc(sizeof(int) * 6 * static_cast<size_t>(nn)));
-    int* d_err = static_cast<int*>(dalloc(sizeof(int)));
+    cudaStream_t s = ctx->stream;
+    DevArena A(s);
+    int4* d_leaves = A.get<int4>(nn);
+    int* d_nbr = A.get<int>(24 * static_cast<size_t>(nn));
+    int* d_nnbr = A.get<int>(6 * static_cast<size_t>(nn));
+    int* d_err = A.get<int>(1);
+    NB_CUDA(cudaMemcpyAsync(d_leaves, leaves, sizeof(int4) * nn, cudaMemcpyHostToDevice, s));
+    NB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+    const Sorted S = sort_leaves(ctx, s, mg, d_leaves, nn, d_err, A);
+    face_table(ctx, s, mg, S, nn, d_nbr, d_nnbr);
     int h_err = 0;
-    try {
-      cudaStream_t s = ctx->stream;
-      NB_CUDA(cudaMemcpyAsync(d_leaves, leaves, sizeof(int4) * nn, cudaMemcpyHostToDevice, s));
-      NB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s));
-      const int T = 256;
-      auto blocks = [&](long long m) { return static_cast<unsigned>((m + T - 1) / T); };
-      k_keys<<<blocks(npad), T, 0, s>>>(nn, npad, d_leaves, mg, d_keys, d_pos, d_err);
-      ctx->launches++;
-      for (int k = 2; k <= npad; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          k_bitonic<<<blocks(npad), T, 0, s>>>(npad, j, k, d_keys, d_pos);
-          ctx->launches++;
-        }
-      k_unique<<<blocks(nn), T, 0, s>>>(nn, d_keys, d_err);
-      k_ranked<<<blocks(nn), T, 0, s>>>(nn, d_pos, d_leaves, d_ranked, d_lev);
-      k_face_nbrs<<<blocks(6LL * nn), T, 0, s>>>(nn, d_keys, d_ranked, d_lev, mg, d_nbr, d_nnbr);
-      ctx->launches += 3;
-      NB_CUDA(cudaGetLastError());
-      NB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
-      NB_CUDA(cudaMemcpyAsync(keys, d_keys, sizeof(uint64_t) * nn, cudaMemcpyDeviceToHost, s));
-      NB_CUDA(cudaMemcpyAsync(order, d_pos, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
-      NB_CUDA(cudaMemcpyAsync(nbr, d_nbr, sizeof(int) * 24 * static_cast<size_t>(nn), cudaMemcpyDeviceToHost, s));
-      NB_CUDA(cudaMemcpyAsync(nnbr, d_nnbr, sizeof(int) * 6 * static_cast<size_t>(nn), cudaMemcpyDeviceToHost, s));
-      NB_CUDA(cudaStreamSynchronize(s));
-    } catch (...) {
-      cudaStreamSynchronize(ctx->stream);
-      for (void* q : bufs) cudaFree(q);
-      throw;
-    }
-    for (void* q : bufs) cudaFree(q);
-    if (h_err == 2) throw ApiError{NB_ERR_BAD_ARG, "nb_amr_build_maps: a leaf lies outside the geometry"};
-    if (h_err == 1) throw ApiError{NB_ERR_BAD_ARG, "nb_amr_build_maps: two leaves share an anchor"};
+    NB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaMemcpyAsync(keys, S.keys, sizeof(uint64_t) * nn, cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaMemcpyAsync(order, S.pos, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaMemcpyAsync(nbr, d_nbr, sizeof(int) * 24 * static_cast<size_t>(nn), cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaMemcpyAsync(nnbr, d_nnbr, sizeof(int) * 6 * static_cast<size_t>(nn), cudaMemcpyDeviceToHost, s));
+    NB_CUDA(cudaStreamSynchronize(s));
+    check_err(h_err, "nb_amr_build_maps");
+    return NB_OK;
+  });
+}
+
+nb_status nb_amr_refine_device(nb_ctx* ctx, const nb_amr_geom* g, const int32_t* leaves, int64_t n,
+                               const uint8_t* flags, int32_t* out, int64_t cap, int64_t* n_out) {
+  if (!ctx || !leaves || n <= 0 || n > (1 << 22) || !flags || !n_out) return NB_ERR_BAD_ARG;
+  if (!map_geom_ok(g)) return fail(ctx, NB_ERR_BAD_ARG, "nb_amr_refine_device: bad geometry");
+  return guarded(ctx, [&] {
+    NB_CUDA(cudaSetDevice(ctx->device));
+    const int nn = static_cast<int>(n);
+    cudaStream_t s = ctx->stream;
+    DevArena A(s);
+    int4* d_leaves = A.get<int4>(nn);
+    uint8_t* d_flags = A.get<uint8_t>(nn);
+    int* d_err = A.get<int>(1);
+    NB_CUDA(cudaMemcpyAsync(d_leaves, leaves, sizeof(int4) * nn, cudaMemcpyHostToDevice, s));
+    NB_CUDA(cudaMemcpyAsync(d_flags, flags, nn, cudaMemcpyHostToDevice, s));
+    NB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+    refine_on_device(ctx, s, map_geom(*g), d_leaves, nn, d_flags, false, d_err, A, out, cap, n_out);
     return NB_OK;
   });
 }

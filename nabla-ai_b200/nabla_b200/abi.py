@@ -237,6 +237,11 @@ PROTOTYPES = [
     ("nb_amr_mesh_maps", C.c_int, [VP, C.POINTER(C.c_uint64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("nb_amr_tree_maps", C.c_int, [C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("nb_amr_refine_device", C.c_int, [VP, C.POINTER(AmrGeom), C.POINTER(C.c_int32), C.c_int64,
+                                       C.POINTER(C.c_uint8), C.POINTER(C.c_int32), C.c_int64,
+                                       C.POINTER(C.c_int64)]),
+    ("nb_amr_case_refine", C.c_int, [VP, C.c_int, C.c_double, C.POINTER(C.c_int32), C.c_int64,
+                                     C.POINTER(C.c_int64)]),
     ("nb_amr_mesh_couplings", C.c_int, [VP, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         DP, C.c_int64]),
     ("nb_amr_apply_laplacian", C.c_int, [VP, VP, DP, DP]),

@@ -58,6 +58,23 @@ def refine(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray) -> np.ndarr
         raise NablaError(st, "nb_amr_refine failed")
 
 
+def refine_device(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray, ctx: Context | None = None) -> np.ndarray:
+    """The same refinement as refine(), computed on the device (nb_amr_refine_device);
+    the new leaves come back in rank order."""
+    ctx = ctx or default_context()
+    leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+    flags = np.ascontiguousarray(flags, dtype=np.uint8)
+    n = leaves.shape[0]
+    need = C.c_int64()
+    cap = max(8 * n, 64)
+    out = np.zeros((cap, 4), dtype=np.int32)
+    ctx.check(ctx.lib.nb_amr_refine_device(ctx.h, C.byref(geom), leaves.ctypes.data_as(C.POINTER(C.c_int32)), n,
+                                           flags.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                           out.ctypes.data_as(C.POINTER(C.c_int32)), cap, C.byref(need)),
+              "nb_amr_refine_device")
+    return out[:need.value].copy()
+
+
 def coarsen(geom: abi.AmrGeom, leaves: np.ndarray, flags: np.ndarray) -> np.ndarray:
     """Merge complete flagged sibling octets into their parents where the 2:1
     balance allows (nb_amr_coarsen)."""
@@ -252,6 +269,19 @@ class AmrCase:
                        "nb_case_sample")
         return out
 
+    def refine_leaves(self, sensor: int, above: float) -> np.ndarray:
+        """The mesh's leaves refined on the device where sensor `sensor` exceeds
+        `above` (nb_amr_case_refine: sensors, split, balance and ranking on the
+        GPU); rank order."""
+        n = self.mesh.leaves.shape[0]
+        need = C.c_int64()
+        cap = 8 * n
+        out = np.zeros((cap, 4), dtype=np.int32)
+        self.ctx.check(self.ctx.lib.nb_amr_case_refine(self.h, sensor, above,
+                                                       out.ctypes.data_as(C.POINTER(C.c_int32)), cap,
+                                                       C.byref(need)), "nb_amr_case_refine")
+        return out[:need.value].copy()
+
     def sensors(self) -> np.ndarray:
         """Per-leaf max |vorticity|, strain magnitude, Q, |grad p| (nb_amr_case_sensors), shape (nleaf, 4)."""
         out = np.zeros((self.mesh.leaves.shape[0], 4))
@@ -347,17 +377,22 @@ class AmrCase:
         return self.ctx.lib.nb_case_cell_count(self.h)
 
 
-def regrid(case: AmrCase, refine_above: float, coarsen_below: float, sensor: int = 0, solid_fn=None) -> AmrCase:
+def regrid(case: AmrCase, refine_above: float, coarsen_below: float, sensor: int = 0, solid_fn=None,
+           device: bool = True) -> AmrCase:
     """One regrid pass on the device sensors: leaves whose sensor `sensor`
     (0 |vorticity|, 1 strain, 2 Q, 3 |grad p|) exceeds refine_above are split
-    (2:1 balance restored), then complete octets of untouched leaves below
+    (2:1 balance restored; on the device by default, nb_amr_case_refine, else
+    by the host maps), then complete octets of untouched leaves below
     coarsen_below are merged; a new case on the new mesh takes the state
     conservatively. solid_fn(leaves) -> per-cell solid flags (leaves x 512, in
     leaf order) or None. Returns the new case (the old one is left as it was)."""
     mesh = case.mesh
     geom, leaves = mesh.geom, mesh.leaves
     s = case.sensors()[:, sensor]
-    refined = refine(geom, leaves, (s > refine_above) & (leaves[:, 0] < geom.lmax))
+    if device:
+        refined = case.refine_leaves(sensor, refine_above)
+    else:
+        refined = refine(geom, leaves, (s > refine_above) & (leaves[:, 0] < geom.lmax))
     # leaves the refinement left alone keep their sensor value; new ones are not coarsened
     old = {tuple(l): v for l, v in zip(map(tuple, leaves), s)}
     flags = np.array([old.get(tuple(l), np.inf) < coarsen_below for l in refined], dtype=np.uint8)
