@@ -337,6 +337,8 @@ def run_ours(args, rank, world, local_rank):
                                                                 stream, flush, world, device)
         if args.same_case_steps > 0:
             out["same_case_as_reference_arm"] = same_case_as_reference(args, ctx, flush, world, device)
+        if args.large_steps > 0:
+            out["large_case"] = large_case(args, ctx, flush, world, device)
         if args.serve_seconds > 0:
             srv = serve_once(args, ctx, prec, 7 + rank, args.serve_seconds + args.serve_grace)
             out["serving"] = {"workload": serve_config(args), "precision": precision,
@@ -370,8 +372,51 @@ def same_case_as_reference(args, ctx, flush, world, device):
     return out
 
 
+def large_case(args, ctx, flush, world, device):
+    """Both forms on the largest config-3 mesh: the 3-level octree of the
+    periodic Taylor-Green box at effective 512^3 (18,712 leaves, 9.58 M leaf
+    cells), stepped from the Taylor-Green state with dt from the CFL condition,
+    MG-PCG to 1e-10; and the dominant kernel family's roofline on it (direct-
+    launch profiled step), where every level has thousands of bricks."""
+    import torch
+
+    from nabla_b200 import abi, amr, cases, workloads
+    geom, leaves = workloads.tgv_octree(128)
+    mesh = amr.AmrMesh(geom, leaves, ctx=ctx)
+    cfg = cases.flow_config(reynolds=1600.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
+                            convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
+    hbm, peak_kind = peaks()
+    out = {"workload": "3-level octree of the periodic Taylor-Green box at effective 512^3 (the largest config-3 "
+                       "mesh), nu=1/1600, WENO-5, CFL 0.4, MG-PCG to 1e-10, from the Taylor-Green state",
+           "cells": mesh.ncell, "steps": args.large_steps}
+    for name, prec in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
+        case = amr.AmrCase(mesh, cfg, precision=prec)
+        case.set_state(*workloads.tgv_face_state(case))
+        run = ns_run(case)
+        run.step()
+        torch.cuda.synchronize()
+        el, reps = timed_steps(run, args.large_steps, stream_of(ctx, case), flush)
+        out[name] = round(world * mesh.ncell * args.large_steps / (max_over_ranks(el, world, device) * 1e-3) / 1e6,
+                          4)
+        out[name + "_ms_per_step"] = round(el / args.large_steps, 3)
+        out[name + "_divergence_max"] = max(r.divergence_max for r in reps)
+        out[name + "_poisson_cycles_per_step"] = reps[-1].poisson_iters
+        shares = {fam: profile_step(ctx, run, fam) for fam in ("smooth", "resid_restrict", "rhs_rk", "pcg_update")}
+        top = max(shares, key=lambda k: shares[k][0])
+        ms, nl, nb = shares[top]
+        ach = nb / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        out[name + "_roofline"] = {"kernel": top, "bound": "hbm", "achieved": round(ach, 2), "peak": hbm,
+                                   "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                                   "launches": int(nl), "avg_launch_us": round(ms * 1e3 / max(nl, 1), 3),
+                                   "bytes_per_launch": nb / max(nl, 1)}
+        case.close()
+    out["mixed_over_fp64"] = round(out["mixed"] / out["fp64"], 3)
+    mesh.close()
+    return out
+
+
 class ns_run:
-    """A uniform NSSolver stepped with dt from its CFL condition."""
+    """A uniform NSSolver or an octree case stepped with dt from its CFL condition."""
 
     def __init__(self, ns):
         self.ns = ns
@@ -660,13 +705,7 @@ def serve_requests(args, seed):
                     geom, leaves = payloads[base]
                     meshes[base] = amr.AmrMesh(geom, leaves, ctx=ctx)
             case = amr.AmrCase(meshes[base], cfg, precision=precision)
-            st = []
-            for a in range(3):
-                x, y, z = case.face_positions(a)
-                st.append(np.sin(x) * np.cos(y) * np.cos(z) if a == 0 else
-                          (-np.cos(x) * np.sin(y) * np.cos(z) if a == 1 else np.zeros_like(x)))
-            st.append(np.zeros(case.sizes[3]))
-            case.set_state(*st)
+            case.set_state(*workloads.tgv_face_state(case))
             return case
         return build
 
@@ -846,6 +885,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--large-steps", type=int, default=5,
+                    help="channel3: steps of both forms on the 512^3-effective octree (0: skip)")
     ap.add_argument("--same-case-steps", type=int, default=5,
                     help="channel3: steps of both forms on the reference arm's uniform-fine case (0: skip)")
     ap.add_argument("--shares", type=int, default=1,

@@ -145,6 +145,22 @@ def _tgv_vorticity(x, y, z):
     return np.sqrt(wx * wx + wy * wy + wz * wz)
 
 
+def tgv_face_state(case: amr.AmrCase):
+    """The Taylor-Green state u = sin x cos y cos z, v = -cos x sin y cos z, w = 0
+    on an octree case's stored faces, p = 0."""
+    st = []
+    for a in range(3):
+        x, y, z = case.face_positions(a)
+        if a == 0:
+            st.append(np.sin(x) * np.cos(y) * np.cos(z))
+        elif a == 1:
+            st.append(-np.cos(x) * np.sin(y) * np.cos(z))
+        else:
+            st.append(np.zeros_like(x))
+    st.append(np.zeros(case.sizes[3]))
+    return st
+
+
 @dataclass
 class TgvBoxWorkload:
     geom: abi.AmrGeom
@@ -156,17 +172,7 @@ class TgvBoxWorkload:
     n_boxes: int
 
     def initial_state(self, case: amr.AmrCase):
-        st = []
-        for a in range(3):
-            x, y, z = case.face_positions(a)
-            if a == 0:
-                st.append(np.sin(x) * np.cos(y) * np.cos(z))
-            elif a == 1:
-                st.append(-np.cos(x) * np.sin(y) * np.cos(z))
-            else:
-                st.append(np.zeros_like(x))
-        st.append(np.zeros(case.sizes[3]))
-        return st
+        return tgv_face_state(case)
 
 
 def tgv_box_case(seed: int) -> TgvBoxWorkload:
