@@ -880,7 +880,7 @@ def main():
     ap.add_argument("--min-steps", type=int, default=10)
     ap.add_argument("--max-steps", type=int, default=200)
     ap.add_argument("--max-effective", type=int, default=512, help="serve: largest effective request size (128/256/512)")
-    ap.add_argument("--slots", type=int, default=32, help="serve: cases in flight at most")
+    ap.add_argument("--slots", type=int, default=8, help="serve: cases in flight at most")
     ap.add_argument("--builders", type=int, default=4, help="serve: host threads that build admitted cases")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")

@@ -225,6 +225,11 @@ typedef struct nb_tuning {
                                 sweeps, restrictions and prolongations phase by phase
                                 with a grid barrier between phases (a barrier that waits
                                 over a second ends the solve with NB_ERR_DEVICE_TIMEOUT) */
+  int32_t coarse_bf16;       /* mixed form: 1 stores the restricted residual of the
+                                multigrid levels between the finest and the cluster tail
+                                in BF16 (rounded to nearest; BF16 keeps FP32's exponent
+                                range, so no per-brick scale is needed), 0 (default)
+                                FP32; arithmetic stays FP32 and the PCG FP64 */
 } nb_tuning;
 
 typedef struct nb_tune_report {

@@ -17,6 +17,7 @@
 #include <cstring>
 
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 
 #include "nb_mg.cuh"
 #include "nb_reduce.cuh"
@@ -64,6 +65,19 @@ struct GAcc {
   template <typename T>
   __device__ __forceinline__ void st(T* p, int n, T v) const { p[n] = v; }
 };
+// BF16 storage of a coarse level's restricted residual (mixed form, optional):
+// the value is rounded to nearest on the store and widened on the load; BF16
+// keeps FP32's 8-bit exponent, so no scaling is needed for range.
+template <typename T>
+__device__ __forceinline__ T ld_b16(const T* p, int n) {
+  return static_cast<T>(__bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[n]));
+}
+template <typename T>
+__device__ __forceinline__ T st_b16(T* p, int n, T v) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(static_cast<float>(v));
+  reinterpret_cast<__nv_bfloat16*>(p)[n] = h;
+  return static_cast<T>(__bfloat162float(h));
+}
 // Level vectors distributed over the shared memory of a thread-block
 // cluster: brick g of a vector lives in CTA g mod cs at slot g / cs of the
 // vector's array, and a vector "pointer" is that array's byte offset in every
@@ -375,7 +389,7 @@ struct SweepOut {
 template <typename T, int NTH, class ACC, class FX, class FP, class OUT>
 __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, const double* bmean, const FX& X,
                                              OUT& sink, T c2, T c1, int prev_mode, const FP& P, int first,
-                                             int stride, T* tile, const ACC& acc) {
+                                             int stride, T* tile, const ACC& acc, int b16 = 0) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   const bool staged = X.x || X.ec;
   for (int brick = first; brick < L.nbrick; brick += stride) {
@@ -385,7 +399,7 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
     for (int q = 0; q < CPT; ++q) {
       const int c = brick * BR3 + threadIdx.x + q * NTH;
       code[q] = L.code[c];
-      bv[q] = acc.ld(b, c);
+      bv[q] = b16 ? ld_b16(b, c) : acc.ld(b, c);
     }
     if (staged) fill_halo<T, NTH>(L, brick, tile, X);
     __syncthreads();
@@ -450,13 +464,13 @@ __global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict
                                                 const double* bmean, XFetch<T> X, T* xout,
                                                 RedBuf rb, double* mean_out, double inv_nfluid,
                                                 const SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
-                                                XFetch<T> P) {
+                                                XFetch<T> P, int b16) {
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   const GAcc acc{};
   SweepOut<T, GAcc> sink{xout, acc};
-  smooth_bricks<T, NTH>(L, b, bmean, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, acc);
+  smooth_bricks<T, NTH>(L, b, bmean, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, acc, b16);
   if (mean_out) {
     double part[1] = {sink.part};
     grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
@@ -505,7 +519,7 @@ template <typename T, int NTH, class ACC, class FX>
 __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, const T* b, const double* bmean,
                                                        const FX& X, const LevelView& C, int fx, int fy, int fz,
                                                        T* rc, int first, int stride, T* tile, T* rs, uint8_t* fl,
-                                                       const ACC& acc) {
+                                                       const ACC& acc, int bio = 0) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   double part = 0.0;
   const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
@@ -516,7 +530,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
     for (int q = 0; q < CPT; ++q) {
       const int c = brick * BR3 + threadIdx.x + q * NTH;
       code[q] = F.code[c];
-      bv[q] = acc.ld(b, c);
+      bv[q] = (bio & 1) ? ld_b16(b, c) : acc.ld(b, c);
     }
     fill_halo<T, NTH>(F, brick, tile, X);
     __syncthreads();
@@ -545,8 +559,8 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
       if (oct < 0) {
         for (int t = threadIdx.x; t < BR3; t += NTH) {
           const T val = fl[t] ? rs[t] : T(0);
-          acc.st(rc, cb * BR3 + t, val);
-          part += wc * static_cast<double>(val);
+          const T sv = (bio & 2) ? st_b16(rc, cb * BR3 + t, val) : (acc.st(rc, cb * BR3 + t, val), val);
+          part += wc * static_cast<double>(sv);
         }
       } else {
         for (int t = threadIdx.x; t < 64; t += NTH) {
@@ -564,8 +578,9 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
               }
           const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
           const int ci = (oct & 1) * 4 + lci, cj = ((oct >> 1) & 1) * 4 + lcj, ck = (oct >> 2) * 4 + lck;
-          acc.st(rc, cb * BR3 + ((ck << 6) | (cj << 3) | ci), val);
-          part += wc * static_cast<double>(val);
+          const int at = cb * BR3 + ((ck << 6) | (cj << 3) | ci);
+          const T sv = (bio & 2) ? st_b16(rc, at, val) : (acc.st(rc, at, val), val);
+          part += wc * static_cast<double>(sv);
         }
       }
     } else {
@@ -587,8 +602,9 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
                 }
               }
           const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
-          acc.st(rc, cell_index(C, gci, gcj, gck), val);
-          part += static_cast<double>(val);
+          const int at = cell_index(C, gci, gcj, gck);
+          const T sv = (bio & 2) ? st_b16(rc, at, val) : (acc.st(rc, at, val), val);
+          part += static_cast<double>(sv);
         }
       }
     }
@@ -602,14 +618,14 @@ __global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __
                                                         const double* bmean, XFetch<T> X, LevelView C,
                                                         int fx, int fy, int fz, T* __restrict__ rc,
                                                         RedBuf rb, double* mean_out, double inv_nfluid_c,
-                                                        const SolveFlags* flags, int maxit) {
+                                                        const SolveFlags* flags, int maxit, int bio) {
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   __shared__ T rs[BR3];
   __shared__ uint8_t fl[BR3];
   double part[1] = {resid_restrict_bricks<T, NTH>(F, b, bmean, X, C, fx, fy, fz, rc, blockIdx.x, gridDim.x, tile,
-                                                  rs, fl, GAcc{})};
+                                                  rs, fl, GAcc{}, bio)};
   if (mean_out) {
     grid_reduce<1>(part, rb, [=] __device__(const double* tt) { *mean_out = tt[0] * inv_nfluid_c; });
   }
@@ -2063,6 +2079,7 @@ void MgSolver::set_tuning(const nb_tuning* tune) {
   direct_max_ = std::min(std::max(t.coarse_direct_max, 0), 512);
   tail_bricks_ = std::min(std::max(t.tail_bricks, 0), 4096);
   vgrid_ = t.vgrid != 0;
+  coarse_bf16_ = precision_ == NB_PRECISION_MIXED && t.coarse_bf16 != 0;
   // Smoother coefficients per sweep of a phase: damped Jacobi (the reference's,
   // c2 = omega) or, mixed form only, Chebyshev on [lmax / 6, lmax] of D^-1 A
   // with lmax = 2, the Gershgorin bound (every row of D^-1 A has diagonal 1
@@ -2106,6 +2123,7 @@ MgSolver::MgSolver(const nb_grid_desc& g, int precision, LaunchCounter lc, const
   common_alloc();
   build_tail();
   build_grid();
+  mark_bf16();
 }
 
 // Composite hierarchy: MG level m+1 merges the finest octree level of level m
@@ -2176,6 +2194,7 @@ MgSolver::MgSolver(const AmrLevelHost& fine, int precision, LaunchCounter lc, co
   if (fine.tree.nlev > 1) build_dense_coarse();
   build_tail();
   build_grid();
+  mark_bf16();
 }
 
 MgSolver::~MgSolver() {
@@ -2289,17 +2308,23 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
     ph.c1 = c1;
     return ph;
   };
+  // BF16 residual storage (recorded phases never carry it: the option leaves
+  // the tail and the grid program's levels in FP32)
+  const int b16 = (!prog && D.b16) ? 1 : 0;
+  const int bio = b16 | ((!prog && Cd.b16) ? 2 : 0);
+  const double bsz = b16 ? 2.0 : tsz;           // bytes of one b value of this level
+  const double csz = (bio & 2) ? 2.0 : tsz;     // bytes of one coarse b value
   // pre-smoothing (sweeps_ sweeps; 2 as the reference), the first from x = 0
-  MG_EMIT("smooth", ncell * (2 * tsz + 1), smooth_phase(none, buf[cur], mean[cur], cheb_c2_[0], 0.0, 0, none),
+  MG_EMIT("smooth", ncell * (tsz + bsz + 1), smooth_phase(none, buf[cur], mean[cur], cheb_c2_[0], 0.0, 0, none),
           (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, none, buf[cur], rb_, mean[cur], inv_nf,
-                      flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+                      flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none, b16)));
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1)  // a Chebyshev step from sweep 2 on also reads x_prev
-    MG_EMIT("smooth", ncell * (3 * tsz + 1) + (cheb_ && sw >= 2 ? ncell * tsz : 0.0),
+    MG_EMIT("smooth", ncell * (2 * tsz + bsz + 1) + (cheb_ && sw >= 2 ? ncell * tsz : 0.0),
             smooth_phase(plain(cur), buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[sw], cheb_c1_[sw],
                          cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1)),
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
                         mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
-                        static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1))));
+                        static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1), b16)));
   // residual + restriction
   const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
@@ -2319,10 +2344,10 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
     ph.fx = Cd.h.fx;
     ph.fy = Cd.h.fy;
     ph.fz = Cd.h.fz;
-    MG_EMIT("resid_restrict", ncell * (2 * tsz + 1) + ncoarse * tsz, ph,
+    MG_EMIT("resid_restrict", ncell * (tsz + bsz + 1) + ncoarse * csz, ph,
             (launch_pdl(pdl_, kr, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                         XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, C, Cd.h.fx, Cd.h.fy,
-                        Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_)));
+                        Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_, bio)));
   }
   void* ec = nullptr;
   int ec_slot = -1;
@@ -2338,14 +2363,14 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
               (launch_pdl(pdl_, kd, dim3(grid), dim3(tpb_), 0, s, L, b, prolonged, z_, rnew_, r_, rb_, S_, flags_,
                           maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
   } else {
-    MG_EMIT("smooth", ncell * (3 * tsz + 1) + ncoarse * tsz,
+    MG_EMIT("smooth", ncell * (2 * tsz + bsz + 1) + ncoarse * tsz,
             smooth_phase(prolonged, buf[cur ^ 1], mean[cur ^ 1], cheb_c2_[0], 0.0, 0, none),
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, prolonged, buf[cur ^ 1], rb_,
-                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none)));
+                        mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none, b16)));
   }
   cur ^= 1;
   for (int sw = 1; sw < sweeps_; ++sw, cur ^= 1) {  // Chebyshev: x_prev, after the prolongation with its coarse value
-    const double bytes = ncell * (3 * tsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0);
+    const double bytes = ncell * (2 * tsz + bsz + 1) + (cheb_ ? ncell * tsz + (sw == 1 ? ncoarse * tsz : 0.0) : 0.0);
     if (dots_here && sw + 1 == sweeps_) {  // + z' and the PCG dots (no xout)
       NB_LAUNCH(lc_, "smooth", s, bytes - ncell * tsz + ncell * 24,
                 (launch_pdl(pdl_, kd, dim3(grid), dim3(tpb_), 0, s, L, b, plain(cur), z_, rnew_, r_, rb_, S_, flags_,
@@ -2358,7 +2383,7 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
                          sw == 1 ? prolonged : plain(cur ^ 1)),
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
                         mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
-                        static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1))));
+                        static_cast<T>(cheb_c1_[sw]), cheb_ ? 1 : 0, sw == 1 ? prolonged : plain(cur ^ 1), b16)));
   }
 #undef MG_EMIT
   *out_x = buf[cur];
@@ -2513,6 +2538,14 @@ void MgSolver::launch_tail(cudaStream_t s) {
     NB_LAUNCH(lc_, "vtail", s, tail_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vtail<float>, prog, flags_, maxit_)));
   else
     NB_LAUNCH(lc_, "vtail", s, tail_bytes_, NB_CUDA(cudaLaunchKernelEx(&cfg, k_vtail<double>, prog, flags_, maxit_)));
+}
+
+// BF16 residual storage: the levels below the finest and above the cluster
+// tail (and above the coarsest level), per-sweep launches only.
+void MgSolver::mark_bf16() {
+  const int last = static_cast<int>(lv_.size()) - 1;
+  for (int l = 0; l <= last; ++l)
+    lv_[l].b16 = coarse_bf16_ && !grid_prog_ && l >= 1 && l < last && (tail_lvl_ < 0 || l < tail_lvl_);
 }
 
 // Records the whole V-cycle from level 0 (every level, the coarsest solve

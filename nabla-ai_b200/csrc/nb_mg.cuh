@@ -35,6 +35,7 @@ struct DevLevel {
   void* b = nullptr;
   void* x0 = nullptr;
   void* x1 = nullptr;
+  bool b16 = false;  // b stored as BF16 (mixed form, nb_tuning.coarse_bf16)
 };
 
 // Cluster-resident V-cycle tail: one launch runs the V-cycle from level
@@ -173,6 +174,7 @@ class MgSolver {
   void build_tail();
   void launch_tail(cudaStream_t s);
   void build_grid();
+  void mark_bf16();
   void launch_grid(cudaStream_t s, const void* b);
   void iterate(cudaStream_t s, double tol, int maxit, int count);
   void setup(cudaStream_t s, const double* b, double tol, int maxit, const WarmStart* ws = nullptr);
@@ -202,6 +204,7 @@ class MgSolver {
   int tail_slot_ = -1;
   double tail_bytes_ = 0.0;        // algorithmic bytes of one tail launch
   bool vgrid_ = false;          // tuning: run each V-cycle as one grid-resident launch
+  bool coarse_bf16_ = false;    // tuning: BF16 residuals on the levels between the finest and the tail
   GridProg* grid_prog_ = nullptr;  // device; nullptr: per-sweep launches
   GridProg* grid_prog_alt_ = nullptr;  // FP64: the same program on the other residual buffer
   const void* grid_b_ = nullptr;       // level-0 rhs grid_prog_ reads

@@ -40,6 +40,7 @@ bool tuning_ok(const nb_tuning& t, std::string& why) {
   else if (t.tail_bricks < 0 || t.tail_bricks > 4096) why = "tail_bricks must be in 0..4096";
   else if (t.warm_start != 0 && t.warm_start != 1) why = "warm_start must be 0 or 1";
   else if (t.vgrid != 0 && t.vgrid != 1) why = "vgrid must be 0 or 1";
+  else if (t.coarse_bf16 != 0 && t.coarse_bf16 != 1) why = "coarse_bf16 must be 0 or 1";
   else return true;
   return false;
 }
@@ -62,12 +63,12 @@ std::string tune_key(nb_ctx* ctx, const nb_case* c) {
   return s;
 }
 
-// One cache line: key and the eleven fields, then ms per step.
+// One cache line: key and the twelve fields, then ms per step.
 bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double& ms) {
   std::istringstream in(line);
   if (!(in >> key >> t.mg_ctas_per_sm >> t.rhs_ctas_per_sm >> t.halo_mode >> t.sweeps >> t.coarse_direct_max >>
         t.pdl >> t.threads_per_brick >> t.smoother >> t.tail_bricks >>
-        t.warm_start >> t.vgrid >> ms))
+        t.warm_start >> t.vgrid >> t.coarse_bf16 >> ms))
     return false;
   std::string why;
   return tuning_ok(t, why);
@@ -75,9 +76,9 @@ bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double&
 
 std::string format_line(const std::string& key, const nb_tuning& t, double ms) {
   char buf[320];
-  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
+  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
                 t.rhs_ctas_per_sm, t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, t.smoother,
-                t.tail_bricks, t.warm_start, t.vgrid, ms);
+                t.tail_bricks, t.warm_start, t.vgrid, t.coarse_bf16, ms);
   return buf;
 }
 
@@ -104,6 +105,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->tail_bricks = 8;
   t->warm_start = 1;
   t->vgrid = 0;
+  t->coarse_bf16 = 0;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {
@@ -286,6 +288,7 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
     knobs.push_back({&nb_tuning::smoother, {0, 1}});
     knobs.push_back({&nb_tuning::sweeps, {1, 2, 3}});
     knobs.push_back({&nb_tuning::warm_start, {0, 1}});
+    knobs.push_back({&nb_tuning::coarse_bf16, {0, 1}});
   }
   if (amr && lev > 1) knobs.push_back({&nb_tuning::coarse_direct_max, {0, 256, 512}});
   for (const Knob& k : knobs)

@@ -138,6 +138,7 @@ class Tuning(C.Structure):
         ("tail_bricks", C.c_int32),
         ("warm_start", C.c_int32),
         ("vgrid", C.c_int32),
+        ("coarse_bf16", C.c_int32),
     ]
 
     def as_dict(self):
