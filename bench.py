@@ -823,6 +823,28 @@ def _ref_worker(q, workload_name, steps):
     q.put((s, cells, sample))
 
 
+def run_large(args, rank, world, local_rank):
+    """Both forms on the 512^3-effective octree alone (the `large_case` key of
+    the default line as its own workload)."""
+    import torch
+
+    from nabla_b200 import solver
+    device = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    ctx = solver.Context(local_rank)
+    if args.tuning:
+        ctx.set_tuning(**args.tuning)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    args.large_steps = args.steps
+    lc = large_case(args, ctx, flush, world, device)
+    return {"metric": METRIC, "value": lc["mixed"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": 1, "ms_per_step": lc["mixed_ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (analytic Taylor-Green state)",
+            "config": {"workload": lc["workload"], "cells": lc["cells"], "tuning": ctx.tuning},
+            "forms": {"mixed": lc["mixed"], "fp64": lc["fp64"], "mixed_over_fp64": lc["mixed_over_fp64"]},
+            "roofline": lc["mixed_roofline"], "large_case": lc, "gpu_launches": int(ctx.launches)}
+
+
 def run_reference(args):
     """Reference arm: the reference's serial CPU step run as one independent
     case per host core (it has no threading), aggregate Mcell-steps/s."""
@@ -862,7 +884,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96", "serve", "poisson3"])
+    ap.add_argument("--workload", default="channel3", choices=["channel3", "tgv64", "batch96", "serve", "poisson3", "large"])
     ap.add_argument("--poisson-bases", type=int, nargs="+", default=[32, 64, 128],
                     help="poisson3: base grids (effective = 4x)")
     ap.add_argument("--batch", type=int, default=96, help="cases of the batch96 workload")
@@ -906,10 +928,11 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
-    runner = {"batch96": run_batch, "serve": run_serve, "poisson3": run_poisson}.get(args.workload, run_ours)
+    runner = {"batch96": run_batch, "serve": run_serve, "poisson3": run_poisson,
+              "large": run_large}.get(args.workload, run_ours)
     out = runner(args, rank, world, local_rank)
     if rank == 0:
-        if args.cpu_steps > 0 and args.workload != "poisson3":
+        if args.cpu_steps > 0 and args.workload not in ("poisson3", "large"):
             s, cells, sample = cpu_sample(args.workload, args.cpu_steps)
             out["cpu_baseline"] = {"value": round(cells / s / 1e6, 5), "unit": UNIT, "cores": 1,
                                    "kind": "reference",
