@@ -260,18 +260,19 @@ __device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T*
     halo[q] = T(0);
     hpos[q] = -1;
     if (h < 384) {
+      // face f = 2a + s, position (u, w) on it: the tile position just outside
+      // the brick and the facing cell of the neighbour brick (the two
+      // tangential axes take u then w, in increasing axis order); selects
+      // rather than arrays indexed by a, which would live in local memory
       const int f = h >> 6, m = h & 63, u = m & 7, w = m >> 3, a = f >> 1, s = f & 1;
-      const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
-      int tc[3], lc[3];
-      tc[a] = s ? 8 : -1;
-      lc[a] = s ? 0 : 7;
-      tc[t1] = lc[t1] = u;
-      tc[t2] = lc[t2] = w;
-      hpos[q] = tpos(tc[0], tc[1], tc[2]);
+      const int et = s ? 8 : -1, el = s ? 0 : 7;
+      const int ti = a == 0 ? et : u, tj = a == 1 ? et : (a == 0 ? u : w), tk = a == 2 ? et : w;
+      const int li = a == 0 ? el : u, lj = a == 1 ? el : (a == 0 ? u : w), lk = a == 2 ? el : w;
+      hpos[q] = tpos(ti, tj, tk);
       const int nb = L.nbr6[brick * 6 + f];
       if (nb >= 0) {
         const int npb = pro ? L.npar6[brick * 6 + f] : 0, npo = pro ? L.npoct6[brick * 6 + f] : -1;
-        halo[q] = fx.at(nb * BR3 + ((lc[2] << 6) | (lc[1] << 3) | lc[0]), npb, npo, L.amr);
+        halo[q] = fx.at(nb * BR3 + ((lk << 6) | (lj << 3) | li), npb, npo, L.amr);
       }
     }
   }
@@ -433,7 +434,10 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
         if (bmean) bc = bc - static_cast<T>(ldv<ACC::kCG>(bmean));
         const T Ax = diag * xc - off;
         const T dM = diag > T(0) ? diag : T(1);
-        out = xc + c2 * (bc - Ax) / dM;
+        if constexpr (sizeof(T) == 4)  // FP32 smoother (a preconditioner): the fast division
+          out = xc + c2 * __fdividef(bc - Ax, dM);
+        else  // FP64: the reference's omega * r / diag
+          out = xc + c2 * (bc - Ax) / dM;
         if (prev_mode) {
           T xp = T(0);
           if (prev_mode == 1) {
@@ -614,7 +618,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
 }
 
 template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH) k_resid_restrict(LevelView F, const T* __restrict__ b,
+__global__ void __launch_bounds__(NTH, NTH == 512 ? 4 : 1) k_resid_restrict(LevelView F, const T* __restrict__ b,
                                                         const double* bmean, XFetch<T> X, LevelView C,
                                                         int fx, int fy, int fz, T* __restrict__ rc,
                                                         RedBuf rb, double* mean_out, double inv_nfluid_c,
