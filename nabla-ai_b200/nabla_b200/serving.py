@@ -78,6 +78,7 @@ class ServeStats:
     queue_samples: list = field(default_factory=list)
     peak_bytes: int = 0
     build_s: float = 0.0  # host time spent creating admitted cases
+    divergence_max: float = 0.0  # largest post-projection divergence of a served request's last step
 
     def summary(self) -> dict:
         lat = np.array(self.latencies) if self.latencies else np.zeros(1)
@@ -88,7 +89,8 @@ class ServeStats:
                 "mcell_steps_per_s": self.cell_steps / max(self.wall_s, 1e-9) / 1e6, "wall_s": self.wall_s,
                 "offered_mcell_steps_per_s": self.offered_cell_steps / max(self.window_s, 1e-9) / 1e6,
                 "max_active": self.max_active, "max_queue": self.max_queue,
-                "mean_queue": float(q.mean()), "peak_device_bytes": self.peak_bytes}
+                "mean_queue": float(q.mean()), "peak_device_bytes": self.peak_bytes,
+                "divergence_max": self.divergence_max}
 
 
 def poisson_arrivals(rate: float, duration: float, seed: int) -> np.ndarray:
@@ -207,6 +209,7 @@ class Server:
                         st.cancelled += 1
                     elif r.steps_done >= r.steps:
                         r.report = rep
+                        st.divergence_max = max(st.divergence_max, rep.divergence_max)
                         if self.keep:
                             r.result = case.get_state()
                         retire(r, case, "done")
