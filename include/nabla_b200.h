@@ -215,10 +215,17 @@ typedef struct nb_tuning {
                                 below the finest with at most n bricks down to the
                                 coarsest solve runs as one thread-block-cluster
                                 launch with those levels in shared memory (0..4096) */
-  int32_t warm_start;        /* mixed form: 1 (default) each projection's MG-PCG starts
-                                from the last pressure scaled to the RK stage, 0 from
-                                zero; the FP64 form always starts from zero as the
-                                reference does */
+  int32_t warm_start;        /* mixed form, the initial guess of each projection's MG-PCG:
+                                0 zero; 1 the last pressure scaled to the RK stage;
+                                2 the same RK stage's pressure extrapolated linearly in
+                                time over the last two steps; 3 (default) that stage's
+                                pressure one step ago plus the change of the previous
+                                stage's pressure since, scaled to this stage. 2 and 3 are
+                                scaled by this step's dt, use form 1 until two steps of
+                                history are held, and restart their history on a new
+                                state (so a checkpoint restart agrees with the continuous
+                                run to the solver tolerance, not bitwise). The FP64 form
+                                always starts from zero as the reference does */
   int32_t vgrid;             /* 0 (default): one launch per sweep (and the cluster
                                 tail); 1: each V-cycle (all levels and the coarsest
                                 solve) is ONE cooperative launch whose CTAs run the

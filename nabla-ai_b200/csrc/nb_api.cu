@@ -51,6 +51,11 @@ struct nb_case {
   double* uvw0[3] = {nullptr, nullptr, nullptr};
   double* p = nullptr;
   double* b = nullptr;
+  // Mixed form: each RK stage's pressure (phi / dt) of the last two steps,
+  // [stage][0 latest, 1 the one before], and how many steps it holds (0..2,
+  // device): the history warm start (nb_tuning.warm_start = 2).
+  double* hist[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  int* d_nhist = nullptr;
   double* staging = nullptr;
   size_t staging_elems = 0;
   BcOp* bc_out = nullptr;  // applyVelocityBC(enforceOutflow = true), phase 1
@@ -300,6 +305,38 @@ void download_lex(nb_case& c, int comp, const double* src, double* host) {
 
 // NSSolver::project (core/src/flow/ns_solver.cpp:475-579) on the current fields.
 // Graph form: the MG-PCG cycle loop is a device-side conditional node.
+// History of the stage pressures (mixed form only; 6 FP64 arrays per case).
+void alloc_history(nb_case& c, size_t ncs) {
+  if (c.precision != NB_PRECISION_MIXED) return;
+  for (int st = 0; st < 3; ++st)
+    for (int k = 0; k < 2; ++k) {
+      c.hist[st][k] = static_cast<double*>(c.alloc(ncs * sizeof(double)));
+      NB_CUDA(cudaMemset(c.hist[st][k], 0, ncs * sizeof(double)));
+    }
+  c.d_nhist = static_cast<int*>(c.alloc(sizeof(int)));
+  NB_CUDA(cudaMemset(c.d_nhist, 0, sizeof(int)));
+}
+
+// A new state makes the history meaningless (set_state, initialize, transfer).
+void reset_history(nb_case& c) {
+  if (c.d_nhist) NB_CUDA(cudaMemsetAsync(c.d_nhist, 0, sizeof(int), c.stream));
+}
+
+bool history_on(const nb_case& c) { return c.d_nhist && c.ctx->tune.warm_start >= 2; }
+
+__global__ void k_history_tick(int* n) {
+  if (*n < 2) *n += 1;
+}
+
+// After the correction of stage `stage` (p = phi / dt): latest -> previous,
+// p -> latest.
+void record_history(nb_case& c, int stage) {
+  if (!history_on(c)) return;
+  const size_t nbytes = static_cast<size_t>(ncell_of(c)) * sizeof(double);
+  NB_CUDA(cudaMemcpyAsync(c.hist[stage][1], c.hist[stage][0], nbytes, cudaMemcpyDeviceToDevice, c.stream));
+  NB_CUDA(cudaMemcpyAsync(c.hist[stage][0], c.p, nbytes, cudaMemcpyDeviceToDevice, c.stream));
+}
+
 // Mixed form with warm_start: the projection of RK stage `stage` starts from
 // the pressure the last projection left (p = phi / dt), scaled to this
 // stage's potential: the stage potentials are about dt P, dt P / 4 and
@@ -307,10 +344,30 @@ void download_lex(nb_case& c, int comp, const double* src, double* host) {
 // dt R, dt R / 4 and 2 dt R / 3), so p holds 2 P / 3 before stage 1 (the last
 // step's stage 3), P before stage 2 and P / 4 before stage 3. The FP64 form
 // starts from 0 as the reference does.
+// With warm_start = 2 the stage's own pressures of the last two steps are
+// extrapolated linearly in time (scaled by this step's dt) once the history
+// holds them; until then the scaled last pressure above.
 const WarmStart* warm_start(const nb_case& c, int stage, WarmStart* ws) {
   if (c.precision != NB_PRECISION_MIXED || !c.ctx->tune.warm_start) return nullptr;
   static constexpr double kAlpha[3] = {1.5, 0.25, 8.0 / 3.0};
   *ws = WarmStart{c.p, &c.d_blk->dt, kAlpha[stage]};
+  if (history_on(c)) {
+    ws->nhist = c.d_nhist;
+    ws->h1 = c.hist[stage][0];
+    if (c.ctx->tune.warm_start == 2) {  // 2 psi_s(n) - psi_s(n-1)
+      ws->h2 = c.hist[stage][1];
+      ws->k2 = -1.0;
+      ws->h1 = c.hist[stage][0];
+      ws->h3 = c.hist[stage][0];
+      ws->k3 = 1.0;
+    } else {  // psi_s(n) + alpha_s (p now - the previous stage's psi one step earlier)
+      const int prev = (stage + 2) % 3;
+      ws->h2 = c.hist[prev][0];
+      ws->k2 = kAlpha[stage];
+      ws->h3 = c.hist[prev][1];
+      ws->k3 = -kAlpha[stage];
+    }
+  }
   return ws;
 }
 
@@ -330,6 +387,7 @@ void project(nb_case& c, double* const* f, int stage, bool direct) {
   }
   flow_launch(c, "correct", ncell_of(c) * 65,
               [&] { launch_correct(c.stream, c.F, c.mg->phi(), &blk->dt, f[0], f[1], f[2], c.p); });
+  record_history(c, stage);
   apply_bc(c, f, false);
 }
 
@@ -385,6 +443,7 @@ void project_amr(nb_case& c, double* const* f, int stage, bool direct) {
   }
   flow_launch(c, "correct", ncell_of(c) * 65,
               [&] { launch_amr_correct(c.stream, c.AF, c.mg->phi(), &blk->dt, f[0], f[1], f[2], c.p); });
+  record_history(c, stage);
   amr_bc(c, f, false);
 }
 
@@ -416,6 +475,10 @@ void issue_step_amr(nb_case& c, int cur, bool cfl_dt, bool direct) {
   });
   NB_CUDA(cudaMemcpyAsync(&blk->execs, c.mg->body_execs(), sizeof(unsigned long long),
                           cudaMemcpyDeviceToDevice, c.stream));
+  if (history_on(c)) {
+    k_history_tick<<<1, 1, 0, c.stream>>>(c.d_nhist);
+    c.ctx->launches++;
+  }
 }
 
 // Issues one SSP-RK3 step (NSSolver::step, core/src/flow/ns_solver.cpp:765-824)
@@ -451,6 +514,10 @@ void issue_step(nb_case& c, int cur, bool cfl_dt, bool direct) {
   });
   NB_CUDA(cudaMemcpyAsync(&blk->execs, c.mg->body_execs(), sizeof(unsigned long long),
                           cudaMemcpyDeviceToDevice, c.stream));
+  if (history_on(c)) {
+    k_history_tick<<<1, 1, 0, c.stream>>>(c.d_nhist);
+    c.ctx->launches++;
+  }
 }
 
 void finish_step(nb_case& c, nb_step_report* rep);
@@ -870,6 +937,7 @@ nb_status nb_case_create(nb_ctx* ctx, const nb_grid_desc* grid, const nb_flow_co
     c->b = static_cast<double*>(c->alloc(ncs * sizeof(double)));
     NB_CUDA(cudaMemset(c->p, 0, ncs * sizeof(double)));
     NB_CUDA(cudaMemset(c->b, 0, ncs * sizeof(double)));
+    alloc_history(*c, ncs);
     c->staging_elems = static_cast<size_t>(std::max({lex_size(F, 0), lex_size(F, 1), lex_size(F, 2)}));
     c->staging = static_cast<double*>(c->alloc(c->staging_elems * sizeof(double)));
     std::vector<BcOp> out_ops, in_ops, solid_ops, dummy;
@@ -978,6 +1046,7 @@ nb_status nb_case_set_state(nb_case* c, const double* u, const double* v, const 
   if (c->amr) return fail(c->ctx, NB_ERR_UNSUPPORTED, "AMR cases take nb_amr_case_set_state");
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
+    reset_history(*c);
     double** f = c->uvw[c->cur];
     upload_lex(*c, 0, u, f[0]);
     upload_lex(*c, 1, v, f[1]);
@@ -1018,6 +1087,7 @@ nb_status nb_case_initialize(nb_case* c) {
   if (!c) return NB_ERR_BAD_ARG;
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
+    reset_history(*c);
     if (c->amr) {  // zero interior, inlet speed on u as the initial guess
       double s = 0.0;
       for (int f = 0; f < 6; ++f)
@@ -1133,6 +1203,7 @@ nb_status nb_amr_case_transfer(nb_case* dst, nb_case* src) {
   std::vector<void*> tmp;
   const nb_status st = guarded(ctx, [&] {
     NB_CUDA(cudaSetDevice(ctx->device));
+    reset_history(*dst);
     NB_CUDA(cudaStreamSynchronize(src->stream));
     const int* dslab[3];
     long long nstore[3];
@@ -1434,6 +1505,7 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     c->b = static_cast<double*>(c->alloc(ncs * sizeof(double)));
     NB_CUDA(cudaMemset(c->p, 0, ncs * sizeof(double)));
     NB_CUDA(cudaMemset(c->b, 0, ncs * sizeof(double)));
+    alloc_history(*c, ncs);
     for (int a = 0; a < 3; ++a) {
       c->nsync[a] = static_cast<int>(c->fm.sync[a].size() / 5);
       if (c->nsync[a])
@@ -1487,6 +1559,7 @@ nb_status nb_amr_case_set_state(nb_case* c, const double* u, const double* v, co
   if (!c || !c->amr || !u || !v || !w || !p) return NB_ERR_BAD_ARG;
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
+    reset_history(*c);
     double** f = c->uvw[c->cur];
     const double* src[3] = {u, v, w};
     for (int a = 0; a < 3; ++a)

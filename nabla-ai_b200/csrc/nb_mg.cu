@@ -1361,22 +1361,38 @@ __global__ void __launch_bounds__(NT) k_pcg_setup(LevelView L, const double* __r
 // Setup from an initial guess: x = fluid ? scale * guess : 0 with scale =
 // alpha * (*dt), r = rhs - A x (rhs as k_pcg_setup forms it), the same |rhs|^2
 // and early exit (the stopping test stays relative to |rhs|).
-struct ScaledFetch {
-  const double* g;
-  double s;
-  __device__ __forceinline__ double operator()(int n, int, int, int) const { return s * g[n]; }
+
+// The initial guess of a warm-started solve: s1 g1 + s2 g2 + s3 g3 (g2, g3 optional).
+struct GuessFetch {
+  const double* g1;
+  const double* g2;
+  const double* g3;
+  double s1, s2, s3;
+  __device__ __forceinline__ double val(int n) const {
+    double v = s1 * g1[n];
+    if (g2) v += s2 * g2[n];
+    if (g3) v += s3 * g3[n];
+    return v;
+  }
+  __device__ __forceinline__ double operator()(int n, int, int, int) const { return val(n); }
   __device__ __forceinline__ bool prolongs() const { return false; }
-  __device__ __forceinline__ double at(int n, int, int, int) const { return s * g[n]; }
+  __device__ __forceinline__ double at(int n, int, int, int) const { return val(n); }
 };
 
 __global__ void __launch_bounds__(NT) k_pcg_setup_warm(LevelView L, const double* __restrict__ b,
                                                        const double* bmean, const double* __restrict__ guess,
                                                        const double* __restrict__ dtp, double alpha,
+                                                       const double* __restrict__ h1, const double* __restrict__ h2,
+                                                       const double* __restrict__ h3, double k2, double k3,
+                                                       const int* nhist,
                                                        double* __restrict__ rhs, double* __restrict__ r,
                                                        double* __restrict__ x, float* __restrict__ r_f, RedBuf rb,
                                                        double* S, SolveFlags* flags, double tol) {
   pdl_wait();
-  const ScaledFetch X{guess, alpha * *dtp};
+  const int nh = nhist ? *nhist : 0;
+  const double dt = *dtp;
+  const GuessFetch X = nh >= 2 ? GuessFetch{h1, h2, h3, dt, k2 * dt, k3 * dt}
+                               : GuessFetch{guess, nullptr, nullptr, alpha * dt, 0.0, 0.0};
   __shared__ double tile[TSN];
   double part[1] = {0.0};
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
@@ -2910,8 +2926,9 @@ void MgSolver::setup(cudaStream_t s, const double* b, double tol, int maxit, con
     lc_.add();
   }
   if (ws)
-    k_pcg_setup_warm<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, ws->guess, ws->dt, ws->alpha, rhs_,
-                                         r_, x_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);
+    k_pcg_setup_warm<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, ws->guess, ws->dt, ws->alpha, ws->h1,
+                                         ws->h2, ws->h3, ws->k2, ws->k3, ws->nhist, rhs_, r_, x_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_,
+                                         tol);
   else
     k_pcg_setup<<<grid, NT, 0, s>>>(L, b, sing ? S_ + S_BSUM : nullptr, rhs_, r_, x_,
                                     mixed ? rnew_f_ : nullptr, rb_, S_, flags_, tol);

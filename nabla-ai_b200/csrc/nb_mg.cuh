@@ -113,6 +113,13 @@ struct WarmStart {
   const double* guess;
   const double* dt;  // device scalar
   double alpha;
+  // History forms (h1, h2, h3 and nhist set): once *nhist >= 2 the guess is
+  // instead dt * (h1 + k2 h2 + k3 h3); before that the form above.
+  const double* h1 = nullptr;
+  const double* h2 = nullptr;
+  const double* h3 = nullptr;
+  double k2 = 0.0, k3 = 0.0;
+  const int* nhist = nullptr;
 };
 
 class MgSolver {

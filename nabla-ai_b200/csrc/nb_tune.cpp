@@ -38,7 +38,7 @@ bool tuning_ok(const nb_tuning& t, std::string& why) {
     why = "threads_per_brick must be 128, 256 or 512";
   else if (t.smoother != 0 && t.smoother != 1) why = "smoother must be 0 or 1";
   else if (t.tail_bricks < 0 || t.tail_bricks > 4096) why = "tail_bricks must be in 0..4096";
-  else if (t.warm_start != 0 && t.warm_start != 1) why = "warm_start must be 0 or 1";
+  else if (t.warm_start < 0 || t.warm_start > 3) why = "warm_start must be in 0..3";
   else if (t.vgrid != 0 && t.vgrid != 1) why = "vgrid must be 0 or 1";
   else if (t.coarse_bf16 != 0 && t.coarse_bf16 != 1) why = "coarse_bf16 must be 0 or 1";
   else return true;
@@ -103,7 +103,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->threads_per_brick = 512;
   t->smoother = 1;
   t->tail_bricks = 8;
-  t->warm_start = 1;
+  t->warm_start = 3;
   t->vgrid = 0;
   t->coarse_bf16 = 0;
 }
@@ -287,7 +287,7 @@ nb_status nb_autotune(nb_ctx* ctx, nb_case* sample, int steps, const char* cache
   if (prec == NB_PRECISION_MIXED) {
     knobs.push_back({&nb_tuning::smoother, {0, 1}});
     knobs.push_back({&nb_tuning::sweeps, {1, 2, 3}});
-    knobs.push_back({&nb_tuning::warm_start, {0, 1}});
+    knobs.push_back({&nb_tuning::warm_start, {0, 1, 2, 3}});
     knobs.push_back({&nb_tuning::coarse_bf16, {0, 1}});
   }
   if (amr && lev > 1) knobs.push_back({&nb_tuning::coarse_direct_max, {0, 256, 512}});

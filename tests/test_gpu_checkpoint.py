@@ -103,6 +103,22 @@ def _clock(ctx, case):
 
 @pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
 def test_octree_restart_is_bit_exact(ctx, tmp_path, precision):
+    """Bit for bit when the initial guesses are functions of the state: the FP64
+    form (zero start) and the mixed form with the scaled-pressure start."""
+    ctx.set_tuning(warm_start=1)
+    try:
+        _octree_restart(ctx, tmp_path, precision, exact=True)
+    finally:
+        ctx.set_tuning(**solver.default_tuning())
+
+
+def test_octree_restart_with_history_start_agrees(ctx, tmp_path):
+    """The mixed form's default history start is not part of the checkpoint: the
+    restarted run agrees with the continuous one to the solver tolerance."""
+    _octree_restart(ctx, tmp_path, abi.PRECISION_MIXED, exact=False)
+
+
+def _octree_restart(ctx, tmp_path, precision, exact):
     mesh, cfg = _amr_channel(ctx, 1)
     gold = _amr_case(mesh, cfg, precision)
     for _ in range(6):
@@ -119,9 +135,15 @@ def test_octree_restart_is_bit_exact(ctx, tmp_path, precision):
     assert _clock(ctx, b) == _clock(ctx, a)
     for _ in range(3):
         b.step()
-    assert _clock(ctx, b) == _clock(ctx, gold)
+    if exact:
+        assert _clock(ctx, b) == _clock(ctx, gold)
+    else:
+        assert _clock(ctx, b)[0] == _clock(ctx, gold)[0]
     for x, y in zip(b.get_state(), gold.get_state()):
-        assert np.array_equal(x, y)
+        if exact:
+            assert np.array_equal(x, y)
+        else:
+            assert np.abs(x - y).max() <= 1e-6 * max(np.abs(y).max(), 1.0)
 
 
 def test_octree_checkpoint_checks_the_mesh(ctx, tmp_path):

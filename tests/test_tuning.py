@@ -14,7 +14,7 @@ def _lib():
 def test_default_tuning():
     assert solver.default_tuning() == {"mg_ctas_per_sm": 4, "rhs_ctas_per_sm": 4, "halo_mode": 0, "sweeps": 2,
                                        "coarse_direct_max": 256, "pdl": 1, "threads_per_brick": 512,
-                                       "smoother": 1, "tail_bricks": 8, "warm_start": 1,
+                                       "smoother": 1, "tail_bricks": 8, "warm_start": 3,
                                        "vgrid": 0, "coarse_bf16": 0}
 
 
@@ -51,7 +51,7 @@ def test_cache_round_trip(tmp_path):
                                          ("halo_mode", 2), ("sweeps", 4), ("coarse_direct_max", 513), ("pdl", 2),
                                          ("threads_per_brick", 64), ("threads_per_brick", 384),
                                          ("smoother", 2), ("tail_bricks", -1), ("tail_bricks", 4097),
-                                         ("warm_start", 2), ("vgrid", 2), ("coarse_bf16", 2)])
+                                         ("warm_start", 4), ("vgrid", 2), ("coarse_bf16", 2)])
 def test_cache_rejects_out_of_range_tuning(tmp_path, field, value):
     path = str(tmp_path / "tune.txt").encode()
     assert _lib().nb_tune_cache_store(path, b"k", C.byref(_tuning(**{field: value})), 1.0) == abi.NB_ERR_BAD_ARG
