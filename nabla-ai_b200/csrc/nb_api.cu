@@ -303,8 +303,6 @@ void download_lex(nb_case& c, int comp, const double* src, double* host) {
   NB_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-// NSSolver::project (core/src/flow/ns_solver.cpp:475-579) on the current fields.
-// Graph form: the MG-PCG cycle loop is a device-side conditional node.
 // History of the stage pressures (mixed form only; 6 FP64 arrays per case).
 void alloc_history(nb_case& c, size_t ncs) {
   if (c.precision != NB_PRECISION_MIXED) return;
@@ -313,8 +311,8 @@ void alloc_history(nb_case& c, size_t ncs) {
       c.hist[st][k] = static_cast<double*>(c.alloc(ncs * sizeof(double)));
       NB_CUDA(cudaMemset(c.hist[st][k], 0, ncs * sizeof(double)));
     }
-  c.d_nhist = static_cast<int*>(c.alloc(sizeof(int)));
-  NB_CUDA(cudaMemset(c.d_nhist, 0, sizeof(int)));
+  c.d_nhist = static_cast<int*>(c.alloc(2 * sizeof(int)));  // [0] steps held, [1] set_state's difference flag
+  NB_CUDA(cudaMemset(c.d_nhist, 0, 2 * sizeof(int)));
 }
 
 // A new state makes the history meaningless (set_state, initialize, transfer).
@@ -323,6 +321,44 @@ void reset_history(nb_case& c) {
 }
 
 bool history_on(const nb_case& c) { return c.d_nhist && c.ctx->tune.warm_start >= 2; }
+
+// Bitwise comparison of an uploaded array with the resident one: any
+// difference (a NaN included) sets *differs.
+__global__ void k_differs(long long n, const unsigned long long* __restrict__ a,
+                          const unsigned long long* __restrict__ b, int* differs) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    if (a[i] != b[i]) {
+      *differs = 1;
+      return;
+    }
+}
+
+__global__ void k_reset_if(const int* differs, int* nhist) {
+  if (*differs) *nhist = 0;
+}
+
+// set_state of a case with a history: the state is uploaded into the scratch
+// parity (and p into the rhs scratch), compared with the resident state, and
+// the history cleared only if they differ; then the scratch becomes the
+// state. A caller that reads the state back and uploads it unchanged (a host
+// round trip every step) keeps the history.
+void compare_and_swap_in(nb_case& c, size_t np) {
+  const int nxt = 1 - c.cur;
+  int* flag = c.d_nhist + 1;
+  NB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), c.stream));
+  for (int a = 0; a < 3; ++a) {
+    const long long n = c.amr ? c.fm.store[a] : store_size(c.F, a);
+    k_differs<<<148, 256, 0, c.stream>>>(n, reinterpret_cast<const unsigned long long*>(c.uvw[nxt][a]),
+                                         reinterpret_cast<const unsigned long long*>(c.uvw[c.cur][a]), flag);
+  }
+  k_differs<<<148, 256, 0, c.stream>>>(static_cast<long long>(np), reinterpret_cast<const unsigned long long*>(c.b),
+                                       reinterpret_cast<const unsigned long long*>(c.p), flag);
+  k_reset_if<<<1, 1, 0, c.stream>>>(flag, c.d_nhist);
+  c.ctx->launches += 5;
+  NB_CUDA(cudaMemcpyAsync(c.p, c.b, np * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+  c.cur = nxt;
+}
 
 __global__ void k_history_tick(int* n) {
   if (*n < 2) *n += 1;
@@ -371,6 +407,8 @@ const WarmStart* warm_start(const nb_case& c, int stage, WarmStart* ws) {
   return ws;
 }
 
+// NSSolver::project (core/src/flow/ns_solver.cpp:475-579) on the current fields.
+// Graph form: the MG-PCG cycle loop is a device-side conditional node.
 void project(nb_case& c, double* const* f, int stage, bool direct) {
   StepBlock* blk = c.d_blk;
   WarmStart wsv;
@@ -1046,12 +1084,13 @@ nb_status nb_case_set_state(nb_case* c, const double* u, const double* v, const 
   if (c->amr) return fail(c->ctx, NB_ERR_UNSUPPORTED, "AMR cases take nb_amr_case_set_state");
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
-    reset_history(*c);
-    double** f = c->uvw[c->cur];
+    const bool keep = c->d_nhist != nullptr;  // stage, compare, then swap in
+    double** f = c->uvw[keep ? 1 - c->cur : c->cur];
     upload_lex(*c, 0, u, f[0]);
     upload_lex(*c, 1, v, f[1]);
     upload_lex(*c, 2, w, f[2]);
-    upload_lex(*c, 3, p, c->p);
+    upload_lex(*c, 3, p, keep ? c->b : c->p);
+    if (keep) compare_and_swap_in(*c, static_cast<size_t>(c->F.nb));
     NB_CUDA(cudaStreamSynchronize(c->stream));
     c->step = step;
     c->t = t;
@@ -1559,15 +1598,16 @@ nb_status nb_amr_case_set_state(nb_case* c, const double* u, const double* v, co
   if (!c || !c->amr || !u || !v || !w || !p) return NB_ERR_BAD_ARG;
   return guarded(c->ctx, [&] {
     NB_CUDA(cudaSetDevice(c->ctx->device));
-    reset_history(*c);
-    double** f = c->uvw[c->cur];
+    const bool keep = c->d_nhist != nullptr;  // stage, compare, then swap in
+    double** f = c->uvw[keep ? 1 - c->cur : c->cur];
     const double* src[3] = {u, v, w};
     for (int a = 0; a < 3; ++a)
       NB_CUDA(cudaMemcpyAsync(f[a], src[a], static_cast<size_t>(c->fm.store[a]) * 8, cudaMemcpyHostToDevice,
                               c->stream));
-    NB_CUDA(cudaMemcpyAsync(c->p, p, static_cast<size_t>(c->fm.nbrick) * BR3 * 8, cudaMemcpyHostToDevice,
-                            c->stream));
+    const size_t np = static_cast<size_t>(c->fm.nbrick) * BR3;
+    NB_CUDA(cudaMemcpyAsync(keep ? c->b : c->p, p, np * 8, cudaMemcpyHostToDevice, c->stream));
     amr_sync(*c, f);
+    if (keep) compare_and_swap_in(*c, np);
     NB_CUDA(cudaStreamSynchronize(c->stream));
     return NB_OK;
   });

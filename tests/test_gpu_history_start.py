@@ -44,14 +44,33 @@ def test_history_start_tracks_fp64_with_fewer_cycles(ctx, mode):
 
 
 def test_new_state_clears_history(ctx):
-    ac, st, _ = _run(ctx, dict(warm_start=2), nsteps=3)
-    ctx.set_tuning(warm_start=2)
-    try:
-        first = [np.array(a, copy=True) for a in st]
-        ac.set_state(*first)
-        a = [ac.step(0.004).poisson_iters for _ in range(3)]
-        ac.set_state(*first)
-        b = [ac.step(0.004).poisson_iters for _ in range(3)]
-        assert a == b
-    finally:
-        ctx.set_tuning(**solver.default_tuning())
+    """A state that differs from the resident one clears the history, so stepping
+    from it repeats exactly."""
+    ac, st, _ = _run(ctx, {}, nsteps=3)
+    first = [np.array(a, copy=True) for a in st]
+    for _ in range(2):
+        ac.step(0.004)
+    ac.set_state(*first)  # differs from the resident state: history cleared
+    a = [ac.step(0.004).poisson_iters for _ in range(4)]
+    sa = [np.array(x, copy=True) for x in ac.get_state()]
+    ac.set_state(*first)
+    b = [ac.step(0.004).poisson_iters for _ in range(4)]
+    assert a == b and a[:2] != [0, 0]
+    for x, y in zip(sa, ac.get_state()):
+        assert np.array_equal(x, y)
+
+
+def test_round_trip_upload_keeps_history(ctx):
+    """Reading the state back and uploading it unchanged every step (a host round
+    trip) keeps the history: the same cycles and bits as stepping on the device."""
+    a, _, ca = _run(ctx, {}, nsteps=6)
+    ctx.set_tuning(**solver.default_tuning())
+    b = _channel(ctx, abi.PRECISION_MIXED)
+    cb = []
+    for _ in range(6):
+        st = [np.array(x, copy=True) for x in b.get_state()]
+        b.set_state(*st)
+        cb.append(b.step(0.004).poisson_iters)
+    assert cb == ca
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(x, y)
