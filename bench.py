@@ -339,6 +339,8 @@ def run_ours(args, rank, world, local_rank):
             out["same_case_as_reference_arm"] = same_case_as_reference(args, ctx, flush, world, device)
         if args.large_steps > 0:
             out["large_case"] = large_case(args, ctx, flush, world, device)
+        if args.batch_steps > 0:
+            out["batch"] = batch_key(args, rank, world, local_rank)
         if args.serve_seconds > 0:
             srv = serve_once(args, ctx, prec, 7 + rank, args.serve_seconds + args.serve_grace)
             out["serving"] = {"workload": serve_config(args), "precision": precision,
@@ -370,6 +372,20 @@ def same_case_as_reference(args, ctx, flush, world, device):
         out[name + "_poisson_cycles_per_step"] = reps[-1].poisson_iters
         ns.close()
     return out
+
+
+def batch_key(args, rank, world, local_rank):
+    """Both forms on the 96-case batch (config 4) with the default tuning: a
+    short run of the batch96 workload, kept as a key of the default line."""
+    import copy
+    a = copy.copy(args)
+    a.steps, a.warmup, a.no_autotune, a.tuning, a.single_form = args.batch_steps, 2, True, None, False
+    a.batch, a.batch_seeds, a.precision = 96, None, "mixed"
+    d = run_batch(a, rank, world, local_rank)
+    return {"workload": d["config"]["workload"], "cells": d["config"]["cells"], "steps": a.steps,
+            "forms": d["forms"], "e2e": d["e2e"]["value"], "roofline": d["roofline"],
+            "divergence_max": d["divergence_max"], "converged": d["converged"],
+            "poisson_iters_mean": d["poisson_iters_mean"], "tuning": "default (no autotune)"}
 
 
 def large_case(args, ctx, flush, world, device):
@@ -907,6 +923,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="form reported as `value` (default: mixed for channel3, fp64 for tgv64)")
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--batch-steps", type=int, default=3,
+                    help="channel3: timed steps of both forms on the 96-case batch (0: skip)")
     ap.add_argument("--large-steps", type=int, default=5,
                     help="channel3: steps of both forms on the 512^3-effective octree (0: skip)")
     ap.add_argument("--same-case-steps", type=int, default=5,

@@ -513,6 +513,34 @@ __global__ void __launch_bounds__(NTH) k_smooth_dots(LevelView L, const T* __res
   grid_reduce<2>(sink.part, rb, [=] __device__(const double* t) { flex_beta(t, S, flags); });
 }
 
+// The first pre-smoothing sweep of a coarse level, from x = 0, at one cell:
+// pointwise in the cell's restricted residual, so the restriction that
+// produces the residual can also write the sweep's result. The same
+// statements as smooth_bricks' sweep from zero (diagonal from the cell's code
+// and coarse-fine couplings, x' = 0 + c2 (b - 0) / D), so the bits agree.
+template <typename T>
+__device__ __forceinline__ T first_sweep(const LevelView& C, int c, T bc, T c2) {
+  const uint32_t code = C.code[c];
+  if (code_type(code) != CELL_FLUID) return T(0);
+  const int lev = C.amr ? C.blevel[c >> 9] : 0;
+  T diag = T(0);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const T h2 = static_cast<T>(C.amr ? C.lh2[lev][f >> 1] : C.h2[f >> 1]);
+    if (code & (1u << f)) diag += h2;
+    else if (code & (1u << (CODE_DIRICHLET + f))) diag += T(2) * h2;
+  }
+  if (C.amr && (code & (1u << CODE_HASCF)))
+    for (int k = C.cf_off[c]; k < C.cf_off[c + 1]; ++k) diag += static_cast<T>(C.cf_coef[k]);
+  const T off = T(0), xc = T(0);
+  const T Ax = diag * xc - off;
+  const T dM = diag > T(0) ? diag : T(1);
+  if constexpr (sizeof(T) == 4)
+    return xc + c2 * __fdividef(bc - Ax, dM);
+  else
+    return xc + c2 * (bc - Ax) / dM;
+}
+
 // ---------------------------------------------------------------------------
 // Residual + full-weighting restriction (multigrid.cpp:116-154): one CTA per
 // fine brick computes r = fluid ? b' - A x' : 0 into shared memory, then each
@@ -523,7 +551,8 @@ template <typename T, int NTH, class ACC, class FX>
 __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, const T* b, const double* bmean,
                                                        const FX& X, const LevelView& C, int fx, int fy, int fz,
                                                        T* rc, int first, int stride, T* tile, T* rs, uint8_t* fl,
-                                                       const ACC& acc, int bio = 0) {
+                                                       const ACC& acc, int bio = 0, T* xf = nullptr,
+                                                       T c2f = T(0)) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   double part = 0.0;
   const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
@@ -564,6 +593,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
         for (int t = threadIdx.x; t < BR3; t += NTH) {
           const T val = fl[t] ? rs[t] : T(0);
           const T sv = (bio & 2) ? st_b16(rc, cb * BR3 + t, val) : (acc.st(rc, cb * BR3 + t, val), val);
+          if (xf) acc.st(xf, cb * BR3 + t, first_sweep(C, cb * BR3 + t, sv, c2f));
           part += wc * static_cast<double>(sv);
         }
       } else {
@@ -584,6 +614,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
           const int ci = (oct & 1) * 4 + lci, cj = ((oct >> 1) & 1) * 4 + lcj, ck = (oct >> 2) * 4 + lck;
           const int at = cb * BR3 + ((ck << 6) | (cj << 3) | ci);
           const T sv = (bio & 2) ? st_b16(rc, at, val) : (acc.st(rc, at, val), val);
+          if (xf) acc.st(xf, at, first_sweep(C, at, sv, c2f));
           part += wc * static_cast<double>(sv);
         }
       }
@@ -608,6 +639,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
           const T val = count > 0 ? sum / static_cast<T>(count) : T(0);
           const int at = cell_index(C, gci, gcj, gck);
           const T sv = (bio & 2) ? st_b16(rc, at, val) : (acc.st(rc, at, val), val);
+          if (xf) acc.st(xf, at, first_sweep(C, at, sv, c2f));
           part += static_cast<double>(sv);
         }
       }
@@ -622,14 +654,15 @@ __global__ void __launch_bounds__(NTH, NTH == 512 ? 4 : 1) k_resid_restrict(Leve
                                                         const double* bmean, XFetch<T> X, LevelView C,
                                                         int fx, int fy, int fz, T* __restrict__ rc,
                                                         RedBuf rb, double* mean_out, double inv_nfluid_c,
-                                                        const SolveFlags* flags, int maxit, int bio) {
+                                                        const SolveFlags* flags, int maxit, int bio, T* xf,
+                                                        T c2f) {
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   __shared__ T rs[BR3];
   __shared__ uint8_t fl[BR3];
   double part[1] = {resid_restrict_bricks<T, NTH>(F, b, bmean, X, C, fx, fy, fz, rc, blockIdx.x, gridDim.x, tile,
-                                                  rs, fl, GAcc{}, bio)};
+                                                  rs, fl, GAcc{}, bio, xf, c2f)};
   if (mean_out) {
     grid_reduce<1>(part, rb, [=] __device__(const double* tt) { *mean_out = tt[0] * inv_nfluid_c; });
   }
@@ -2237,7 +2270,7 @@ void MgSolver::apply_a(cudaStream_t s, const double* x, double* out) {
 // (same arguments) instead of being issued.
 template <typename T>
 void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, void* /*unused*/,
-                      int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog) {
+                      int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog, bool first_done) {
   if (!prog && lvl == tail_lvl_) {
     launch_tail(s);
     *out_x = tail_x_;
@@ -2335,6 +2368,8 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const double bsz = b16 ? 2.0 : tsz;           // bytes of one b value of this level
   const double csz = (bio & 2) ? 2.0 : tsz;     // bytes of one coarse b value
   // pre-smoothing (sweeps_ sweeps; 2 as the reference), the first from x = 0
+  // (already written by the restriction that made b when first_done)
+  if (!first_done)
   MG_EMIT("smooth", ncell * (tsz + bsz + 1), smooth_phase(none, buf[cur], mean[cur], cheb_c2_[0], 0.0, 0, none),
           (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, none, buf[cur], rb_, mean[cur], inv_nf,
                       flags_, maxit_, static_cast<T>(cheb_c2_[0]), T(0), 0, none, b16)));
@@ -2345,7 +2380,9 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
             (launch_pdl(pdl_, ks, dim3(grid), dim3(tpb_), 0, s, L, b, bmean, plain(cur), buf[cur ^ 1], rb_,
                         mean[cur ^ 1], inv_nf, flags_, maxit_, static_cast<T>(cheb_c2_[sw]),
                         static_cast<T>(cheb_c1_[sw]), cheb_ ? (sw == 1 ? 2 : 1) : 0, plain(cur ^ 1), b16)));
-  // residual + restriction
+  // residual + restriction; on non-singular systems (no pending means) it also
+  // writes the coarse level's first sweep when that level smooths by launches
+  const bool fuse_first = !prog && !singular_ && lvl + 1 != tail_lvl_ && lvl + 2 < static_cast<int>(lv_.size());
   const double inv_nfc = Cd.h.nfluid ? 1.0 / Cd.wfluid : 0.0;
   const int cb_slot = lvl_slot(lvl + 1, 2);
   double* cmean = (singular_ && Cd.h.nfluid > 0) ? S_ + cb_slot : nullptr;
@@ -2364,14 +2401,16 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
     ph.fx = Cd.h.fx;
     ph.fy = Cd.h.fy;
     ph.fz = Cd.h.fz;
-    MG_EMIT("resid_restrict", ncell * (tsz + bsz + 1) + ncoarse * csz, ph,
+    MG_EMIT("resid_restrict", ncell * (tsz + bsz + 1) + ncoarse * (csz + (fuse_first ? tsz : 0.0)), ph,
             (launch_pdl(pdl_, kr, dim3(grid), dim3(tpb_), 0, s, L, b, bmean,
                         XFetch<T>{buf[cur], mean[cur], nullptr, nullptr, dummy, 1, 1, 1}, C, Cd.h.fx, Cd.h.fy,
-                        Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_, bio)));
+                        Cd.h.fz, static_cast<T*>(Cd.b), rb_, cmean, inv_nfc, flags_, maxit_, bio,
+                        fuse_first ? static_cast<T*>(Cd.x0) : static_cast<T*>(nullptr),
+                        static_cast<T>(cheb_c2_[0]))));
   }
   void* ec = nullptr;
   int ec_slot = -1;
-  vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec, prog);
+  vcycle<T>(s, lvl + 1, Cd.b, cmean ? cb_slot : -1, nullptr, &ec_slot, &ec, prog, fuse_first);
   const double* ecmean = (singular_ && ec_slot >= 0) ? S_ + ec_slot : nullptr;
   // post-smoothing: the first sweep folds in the prolongation x += P e
   const XFetch<T> prolonged{buf[cur], mean[cur], static_cast<const T*>(ec), ecmean, C, Cd.h.fx, Cd.h.fy,
@@ -2993,8 +3032,8 @@ void MgSolver::solve(cudaStream_t s, const double* b, double tol, int maxit) {
 }
 
 template void MgSolver::vcycle<double>(cudaStream_t, int, const void*, int, void*, int*, void**,
-                                       std::vector<TailPhase>*);
+                                       std::vector<TailPhase>*, bool);
 template void MgSolver::vcycle<float>(cudaStream_t, int, const void*, int, void*, int*, void**,
-                                      std::vector<TailPhase>*);
+                                      std::vector<TailPhase>*, bool);
 
 }  // namespace nb

@@ -177,7 +177,7 @@ class MgSolver {
   // With `prog` the launches are recorded as tail phases instead (no stream).
   template <typename T>
   void vcycle(cudaStream_t s, int lvl, const void* b, int bmean_slot, void* xout_final,
-              int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog = nullptr);
+              int* out_mean_slot, void** out_x, std::vector<TailPhase>* prog = nullptr, bool first_done = false);
   void build_tail();
   void launch_tail(cudaStream_t s);
   void build_grid();
