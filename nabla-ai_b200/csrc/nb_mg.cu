@@ -238,6 +238,54 @@ __device__ __forceinline__ void fill_halo_amr(const LevelView& L, int brick, T* 
   }
 }
 
+// The loads of fill_halo_fast into registers (the brick's own values and its
+// face halo), and their stores into the tile: split so that a CTA can have the
+// next brick's loads in flight while it computes the current one.
+template <typename T, int NTH, class F>
+__device__ __forceinline__ void halo_load(const LevelView& L, int brick, const F& fx, T* own, T* halo, int* hpos) {
+  constexpr int CPT = BR3 / NTH;
+  constexpr int HPT = (384 + NTH - 1) / NTH;
+  const int t = threadIdx.x;
+  const bool pro = fx.prolongs();
+  const int pb = pro ? L.par[brick] : 0, po = pro ? L.poct[brick] : -1;
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) own[q] = fx.at(brick * BR3 + t + q * NTH, pb, po, L.amr);
+#pragma unroll
+  for (int q = 0; q < HPT; ++q) {
+    const int h = t + q * NTH;
+    halo[q] = T(0);
+    hpos[q] = -1;
+    if (h < 384) {
+      // face f = 2a + s, position (u, w) on it: the tile position just outside
+      // the brick and the facing cell of the neighbour brick (the two
+      // tangential axes take u then w, in increasing axis order); selects
+      // rather than arrays indexed by a, which would live in local memory
+      const int f = h >> 6, m = h & 63, u = m & 7, w = m >> 3, a = f >> 1, s = f & 1;
+      const int et = s ? 8 : -1, el = s ? 0 : 7;
+      const int ti = a == 0 ? et : u, tj = a == 1 ? et : (a == 0 ? u : w), tk = a == 2 ? et : w;
+      const int li = a == 0 ? el : u, lj = a == 1 ? el : (a == 0 ? u : w), lk = a == 2 ? el : w;
+      hpos[q] = tpos(ti, tj, tk);
+      const int nb = L.nbr6[brick * 6 + f];
+      if (nb >= 0) {
+        const int npb = pro ? L.npar6[brick * 6 + f] : 0, npo = pro ? L.npoct6[brick * 6 + f] : -1;
+        halo[q] = fx.at(nb * BR3 + ((lk << 6) | (lj << 3) | li), npb, npo, L.amr);
+      }
+    }
+  }
+}
+
+template <typename T, int NTH>
+__device__ __forceinline__ void halo_store(T* tile, const T* own, const T* halo, const int* hpos) {
+  constexpr int CPT = BR3 / NTH;
+  constexpr int HPT = (384 + NTH - 1) / NTH;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) tile[tpos_local(t + q * NTH)] = own[q];
+#pragma unroll
+  for (int q = 0; q < HPT; ++q)
+    if (hpos[q] >= 0) tile[hpos[q]] = halo[q];
+}
+
 // One-round staging (levels with per-brick maps): a CTA of NTH threads loads
 // the brick's 512 cells (512/NTH per thread) and the 384 face-halo cells from
 // the six neighbour bricks (6 faces x 64). Every load is issued before the
@@ -385,14 +433,106 @@ struct SweepOut {
   }
 };
 
+// One cell of a sweep: xout = fluid ? x' + c2 (b' - A x') / D + c1 (x' - x_prev) : 0.
+template <typename T, class ACC, class FX, class FP>
+__device__ __forceinline__ T sweep_cell(const LevelView& L, int brick, int l, uint32_t code, T bc, const double* bmean,
+                                        const FX& X, T c2, T c1, int prev_mode, const FP& P, const T* tile,
+                                        bool staged, bool& fluid) {
+  const int c = brick * BR3 + l;
+  T out = T(0);
+  fluid = code_type(code) == CELL_FLUID;
+  if (fluid) {
+    T diag, off, xc;
+    if (staged) {
+      full_row<T>(L, code, tile, brick, c, X, diag, off);
+      xc = tile[tpos_local(l)];
+    } else {  // first sweep from x = 0: A x = 0
+      const int lev = L.amr ? L.blevel[brick] : 0;
+      diag = T(0);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        const T h2 = static_cast<T>(L.amr ? L.lh2[lev][f >> 1] : L.h2[f >> 1]);
+        if (code & (1u << f)) diag += h2;
+        else if (code & (1u << (CODE_DIRICHLET + f))) diag += T(2) * h2;
+      }
+      if (L.amr && (code & (1u << CODE_HASCF)))
+        for (int k = L.cf_off[c]; k < L.cf_off[c + 1]; ++k) diag += static_cast<T>(L.cf_coef[k]);
+      off = T(0);
+      xc = T(0);
+    }
+    if (bmean) bc = bc - static_cast<T>(ldv<ACC::kCG>(bmean));
+    const T Ax = diag * xc - off;
+    const T dM = diag > T(0) ? diag : T(1);
+    if constexpr (sizeof(T) == 4)  // FP32 smoother (a preconditioner): the fast division
+      out = xc + c2 * __fdividef(bc - Ax, dM);
+    else  // FP64: the reference's omega * r / diag
+      out = xc + c2 * (bc - Ax) / dM;
+    if (prev_mode) {
+      T xp = T(0);
+      if (prev_mode == 1) {
+        int gi, gj, gk;
+        cell_coords(L, c, gi, gj, gk);
+        xp = P(c, gi, gj, gk);
+      }
+      out = out + c1 * (xc - xp);
+    }
+  }
+  return out;
+}
+
 // Bricks first, first + stride, ... of one sweep; every cell's result goes
-// to out(c, weight, value, fluid). `acc` addresses b.
-template <typename T, int NTH, class ACC, class FX, class FP, class OUT>
+// to out(c, weight, value, fluid). `acc` addresses b. With PIPE (levels with
+// per-brick maps and several bricks per CTA) the next brick's code, rhs, own
+// and halo values are loaded while the current brick computes.
+template <typename T, int NTH, class ACC, class FX, class FP, class OUT, bool PIPE = false>
 __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, const double* bmean, const FX& X,
                                              OUT& sink, T c2, T c1, int prev_mode, const FP& P, int first,
                                              int stride, T* tile, const ACC& acc, int b16 = 0) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
+  constexpr int HPT = (384 + NTH - 1) / NTH;
   const bool staged = X.x || X.ec;
+  if constexpr (PIPE) {
+    if (staged && L.fast) {
+      if (first >= L.nbrick) return;
+      uint32_t code[CPT];
+      T bv[CPT], own[CPT], halo[HPT];
+      int hpos[HPT];
+      const auto load = [&](int brick) {
+#pragma unroll
+        for (int q = 0; q < CPT; ++q) {
+          const int c = brick * BR3 + threadIdx.x + q * NTH;
+          code[q] = L.code[c];
+          bv[q] = b16 ? ld_b16(b, c) : acc.ld(b, c);
+        }
+        halo_load<T, NTH>(L, brick, X, own, halo, hpos);
+      };
+      load(first);
+      for (int brick = first;; brick += stride) {
+        halo_store<T, NTH>(tile, own, halo, hpos);
+        uint32_t cc[CPT];
+        T cb[CPT];
+#pragma unroll
+        for (int q = 0; q < CPT; ++q) {
+          cc[q] = code[q];
+          cb[q] = bv[q];
+        }
+        __syncthreads();
+        const bool more = brick + stride < L.nbrick;
+        if (more) load(brick + stride);  // in flight during this brick's arithmetic
+        const double wgt = cell_weight(L, brick);
+#pragma unroll
+        for (int q = 0; q < CPT; ++q) {
+          const int l = threadIdx.x + q * NTH;
+          bool fluid;
+          const T out = sweep_cell<T, ACC>(L, brick, l, cc[q], cb[q], bmean, X, c2, c1, prev_mode, P, tile, true,
+                                           fluid);
+          sink(brick * BR3 + l, wgt, out, fluid);
+        }
+        __syncthreads();
+        if (!more) return;
+      }
+    }
+  }
   for (int brick = first; brick < L.nbrick; brick += stride) {
     uint32_t code[CPT];
     T bv[CPT];
@@ -463,22 +603,45 @@ __device__ __forceinline__ void flex_beta(const double* t, double* S, SolveFlags
   flags->iters += 1;
 }
 
-template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b,
-                                                const double* bmean, XFetch<T> X, T* xout,
-                                                RedBuf rb, double* mean_out, double inv_nfluid,
-                                                const SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
-                                                XFetch<T> P, int b16) {
+template <typename T, int NTH, bool PIPE>
+__device__ __forceinline__ void smooth_launch(const LevelView& L, const T* __restrict__ b, const double* bmean,
+                                              const XFetch<T>& X, T* xout, const RedBuf& rb, double* mean_out,
+                                              double inv_nfluid, const SolveFlags* flags, int maxit, T c2, T c1,
+                                              int prev_mode, const XFetch<T>& P, int b16) {
   pdl_wait();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   const GAcc acc{};
   SweepOut<T, GAcc> sink{xout, acc};
-  smooth_bricks<T, NTH>(L, b, bmean, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, acc, b16);
+  smooth_bricks<T, NTH, GAcc, XFetch<T>, XFetch<T>, SweepOut<T, GAcc>, PIPE>(L, b, bmean, X, sink, c2, c1, prev_mode,
+                                                                            P, blockIdx.x, gridDim.x, tile, acc, b16);
   if (mean_out) {
     double part[1] = {sink.part};
     grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
   }
+}
+
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b, const double* bmean,
+                                                XFetch<T> X, T* xout, RedBuf rb, double* mean_out,
+                                                double inv_nfluid, const SolveFlags* flags, int maxit, T c2, T c1,
+                                                int prev_mode, XFetch<T> P, int b16) {
+  smooth_launch<T, NTH, false>(L, b, bmean, X, xout, rb, mean_out, inv_nfluid, flags, maxit, c2, c1, prev_mode, P,
+                               b16);
+}
+
+// The pipelined sweep (two bricks' loads in registers): 64 registers a thread,
+// 1024 threads an SM. The bound also tells the driver to size the shared
+// memory for that many CTAs; a bound of one CTA an SM would let it choose a
+// carveout that holds one.
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH, 1024 / NTH) k_smooth_pipe(LevelView L, const T* __restrict__ b,
+                                                                 const double* bmean, XFetch<T> X, T* xout,
+                                                                 RedBuf rb, double* mean_out, double inv_nfluid,
+                                                                 const SolveFlags* flags, int maxit, T c2, T c1,
+                                                                 int prev_mode, XFetch<T> P, int b16) {
+  smooth_launch<T, NTH, true>(L, b, bmean, X, xout, rb, mean_out, inv_nfluid, flags, maxit, c2, c1, prev_mode, P,
+                              b16);
 }
 
 // The last post-smoothing sweep of level 0 on a non-singular system, fused
@@ -649,8 +812,11 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
   return part;
 }
 
+// Bounds: 4 CTAs an SM at 512 threads (32 registers), and for the smaller
+// CTAs the count their registers already allow (4 at 128, 2 at 256), so that
+// the driver sizes the shared memory for that many CTAs and not for one.
 template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH, NTH == 512 ? 4 : 1) k_resid_restrict(LevelView F, const T* __restrict__ b,
+__global__ void __launch_bounds__(NTH, NTH == 256 ? 2 : 4) k_resid_restrict(LevelView F, const T* __restrict__ b,
                                                         const double* bmean, XFetch<T> X, LevelView C,
                                                         int fx, int fy, int fz, T* __restrict__ rc,
                                                         RedBuf rb, double* mean_out, double inv_nfluid_c,
@@ -2334,7 +2500,10 @@ void MgSolver::vcycle(cudaStream_t s, int lvl, const void* bv, int bmean_slot, v
   const LevelView& C = Cd.v;
   const double ncoarse = Cd.ncell;
   // kernels for the tuned CTA size (threads per brick)
-  const auto ks = tpb_ == 128 ? k_smooth<T, 128> : (tpb_ == 256 ? k_smooth<T, 256> : k_smooth<T, 512>);
+  // several bricks per CTA: the pipelined smoother (next brick's loads in flight)
+  const bool pipe = sizeof(T) == 8 && L.fast && L.nbrick > grid;
+  const auto ks = pipe ? (tpb_ == 128 ? k_smooth_pipe<T, 128> : (tpb_ == 256 ? k_smooth_pipe<T, 256> : k_smooth_pipe<T, 512>))
+                       : (tpb_ == 128 ? k_smooth<T, 128> : (tpb_ == 256 ? k_smooth<T, 256> : k_smooth<T, 512>));
   const auto kr = tpb_ == 128 ? k_resid_restrict<T, 128>
                               : (tpb_ == 256 ? k_resid_restrict<T, 256> : k_resid_restrict<T, 512>);
   // Ping-pong buffers with their pending means: xa <-> slot 0, xb <-> slot 1.
