@@ -417,7 +417,12 @@ def large_case(args, ctx, flush, world, device):
         out[name + "_ms_per_step"] = round(el / args.large_steps, 3)
         out[name + "_divergence_max"] = max(r.divergence_max for r in reps)
         out[name + "_poisson_cycles_per_step"] = reps[-1].poisson_iters
-        shares = {fam: profile_step(ctx, run, fam) for fam in ("smooth", "resid_restrict", "rhs_rk", "pcg_update")}
+        shares = {fam: profile_step(ctx, run, fam) for fam in FAMILIES}
+        shares = {k: v for k, v in shares.items() if v[1] > 0}
+        total = sum(v[0] for v in shares.values()) or 1.0
+        out[name + "_kernel_shares"] = {k: {"share": round(v[0] / total, 4), "launches": int(v[1]),
+                                            "us_per_launch": round(v[0] * 1e3 / v[1], 2)}
+                                        for k, v in sorted(shares.items(), key=lambda kv: -kv[1][0])}
         top = max(shares, key=lambda k: shares[k][0])
         ms, nl, nb = shares[top]
         ach = nb / (ms * 1e-3) / 1e9 if ms > 0 else 0.0

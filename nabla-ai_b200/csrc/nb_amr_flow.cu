@@ -69,13 +69,125 @@ __device__ __forceinline__ int leaf_of(const LevelView& L, int lev0, const int p
   return r;
 }
 
+// Readers of the ghost walker below. ValRead reads the stored faces. AffRead
+// records instead which stored faces the walker combines and with which
+// weights: every rule of the walker (wrap, reflection, outlet copy, sub-face
+// average, interpolation along the normal) is affine in the stored faces, so
+// a halo point's value is c + sum_k w_k f[idx_k] for fixed (idx_k, w_k) on a
+// given mesh. The ghost map records these forms once per case.
+struct ValRead {
+  using V = double;
+  static constexpr bool kSym = false;
+  __device__ static double rd(const double* __restrict__ f, long long i) { return f[i]; }
+  __device__ static double k(double v) { return v; }
+};
+
+constexpr int AFF_MAX = 8;  // terms of a recorded form; more: the point keeps the walker
+
+struct Aff {
+  double c;  // constant part
+  int n;     // number of terms; -1 when more than AFF_MAX distinct faces (or an index past 2^31)
+  int idx[AFF_MAX];
+  double w[AFF_MAX];
+};
+
+__device__ __forceinline__ void aff_axpy(Aff& r, double s, const Aff& x) {  // r += s x
+  if (r.n < 0 || x.n < 0) {
+    r.n = -1;
+    return;
+  }
+  r.c += s * x.c;
+  for (int q = 0; q < x.n; ++q) {
+    int j = 0;
+    while (j < r.n && r.idx[j] != x.idx[q]) ++j;
+    if (j == r.n) {
+      if (r.n == AFF_MAX) {
+        r.n = -1;
+        return;
+      }
+      r.idx[j] = x.idx[q];
+      r.w[j] = 0.0;
+      ++r.n;
+    }
+    r.w[j] += s * x.w[q];
+  }
+}
+__device__ __forceinline__ Aff operator+(Aff a, const Aff& b) {
+  aff_axpy(a, 1.0, b);
+  return a;
+}
+__device__ __forceinline__ Aff operator-(Aff a, const Aff& b) {
+  aff_axpy(a, -1.0, b);
+  return a;
+}
+__device__ __forceinline__ Aff& operator+=(Aff& a, const Aff& b) {
+  aff_axpy(a, 1.0, b);
+  return a;
+}
+__device__ __forceinline__ Aff operator*(double s, Aff a) {
+  a.c *= s;
+  for (int q = 0; q < a.n; ++q) a.w[q] *= s;
+  return a;
+}
+
+struct AffRead {
+  using V = Aff;
+  static constexpr bool kSym = true;
+  __device__ static Aff rd(const double* __restrict__, long long i) {
+    Aff r;
+    r.c = 0.0;
+    r.n = i < (1LL << 31) ? 1 : -1;
+    r.idx[0] = static_cast<int>(i);
+    r.w[0] = 1.0;
+    return r;
+  }
+  __device__ static Aff k(double v) {
+    Aff r;
+    r.c = v;
+    r.n = 0;
+    return r;
+  }
+};
+
+// The walker's nested boundary constants: value = c_{d-1} - (c_{d-2} - (...
+// - (c_0 - term))), applied innermost-first when reading values (the
+// reference's evaluation order). A recorded form needs no order: it keeps the
+// alternating sum S = c_0 - c_1 + ... and returns (-1)^(d-1) (S - term).
+template <class RD>
+struct Nest {
+  double cst[ACC_MAX];
+  int d = 0;
+  __device__ void push(double v) { cst[d++] = v; }
+  __device__ double finish(double term) const {
+    for (int q = d - 1; q >= 0; --q) term = cst[q] - term;
+    return term;
+  }
+};
+template <>
+struct Nest<AffRead> {
+  Aff S = AffRead::k(0.0);
+  int d = 0;
+  __device__ void push(const Aff& v) {
+    aff_axpy(S, (d & 1) ? -1.0 : 1.0, v);
+    ++d;
+  }
+  __device__ Aff finish(const Aff& term) const {
+    if (d == 0) return term;
+    const Aff r = S - term;
+    return (d & 1) ? r : -1.0 * r;
+  }
+};
+
 // Stored a-face at a face position of level `lev0`: p[a] in [0, N_a], the
 // other coordinates in-domain. Reads the owner: the minus-side cell's slab
 // when that cell is at lev0 and has one (domain high faces, coarse-fine
 // sub-faces owned by the fine side), else the plus-side cell's low face
 // (same level), the average of its four sub-faces (plus side finer), or the
 // coarse face containing it (plus side coarser; p[a] even there).
-__device__ double face_at(const AmrFlowView& F, int a, const double* __restrict__ f, int lev0, const int p0[3]) {
+template <class RD = ValRead>
+__device__ typename RD::V face_at(const AmrFlowView& F, int a, const double* __restrict__ f, int lev0,
+                                 const int p0[3]) {
+  using V = typename RD::V;
   const LevelView& L = F.L;
   const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
   const int N = L.lcells[lev0][a];
@@ -94,16 +206,16 @@ __device__ double face_at(const AmrFlowView& F, int a, const double* __restrict_
     const int rm = leaf_of(L, lev0, m, lm);
     if (rm >= 0 && (m[a] & 7) == 7) {
       const int sid = F.slab_id[3 * rm + a];
-      if (lm == lev0 && sid >= 0) return f[F.nb + sid * 64LL + slab_local(a, m[0] & 7, m[1] & 7, m[2] & 7)];
+      if (lm == lev0 && sid >= 0) return RD::rd(f, F.nb + sid * 64LL + slab_local(a, m[0] & 7, m[1] & 7, m[2] & 7));
       if (!has_plus && lm == lev0 + 1 && sid >= 0) {  // domain high face over finer cells
-        double s = 0.0;
+        V s = RD::k(0.0);
         for (int d2 = 0; d2 < 2; ++d2)
           for (int d1 = 0; d1 < 2; ++d1) {
             int c[3];
             c[a] = 2 * m[a] + 1;
             c[t1] = 2 * m[t1] + d1;
             c[t2] = 2 * m[t2] + d2;
-            s += f[F.nb + sid * 64LL + slab_local(a, c[0] & 7, c[1] & 7, c[2] & 7)];
+            s += RD::rd(f, F.nb + sid * 64LL + slab_local(a, c[0] & 7, c[1] & 7, c[2] & 7));
           }
         return 0.25 * s;
       }
@@ -111,46 +223,49 @@ __device__ double face_at(const AmrFlowView& F, int a, const double* __restrict_
     if (!has_plus && rm >= 0 && lm == lev0 - 1) {  // domain high face over a coarser cell
       const int c[3] = {m[0] >> 1, m[1] >> 1, m[2] >> 1};
       const int sid = F.slab_id[3 * rm + a];
-      if (sid >= 0) return f[F.nb + sid * 64LL + slab_local(a, c[0] & 7, c[1] & 7, c[2] & 7)];
+      if (sid >= 0) return RD::rd(f, F.nb + sid * 64LL + slab_local(a, c[0] & 7, c[1] & 7, c[2] & 7));
     }
   }
-  if (!has_plus) return 0.0;
+  if (!has_plus) return RD::k(0.0);
   int lp;
   const int rp = leaf_of(L, lev0, p, lp);
-  if (rp < 0) return 0.0;
-  if (lp == lev0) return f[rp * static_cast<long long>(BR3) + local_of(p)];
+  if (rp < 0) return RD::k(0.0);
+  if (lp == lev0) return RD::rd(f, rp * static_cast<long long>(BR3) + local_of(p));
   if (lp == lev0 + 1) {
-    double s = 0.0;
+    V s = RD::k(0.0);
     for (int d2 = 0; d2 < 2; ++d2)
       for (int d1 = 0; d1 < 2; ++d1) {
         int c[3];
         c[a] = 2 * p[a];
         c[t1] = 2 * p[t1] + d1;
         c[t2] = 2 * p[t2] + d2;
-        s += f[rp * static_cast<long long>(BR3) + local_of(c)];
+        s += RD::rd(f, rp * static_cast<long long>(BR3) + local_of(c));
       }
     return 0.25 * s;
   }
   const int c[3] = {p[0] >> 1, p[1] >> 1, p[2] >> 1};  // coarser: the coarse cell's low face
-  return f[rp * static_cast<long long>(BR3) + local_of(c)];
+  return RD::rd(f, rp * static_cast<long long>(BR3) + local_of(c));
 }
 
 // a-face value at level `lev0` position p, including the positions that fall
 // mid-cell inside a coarser leaf (linear interpolation along the normal).
-__device__ double face_read(const AmrFlowView& F, int a, const double* __restrict__ f, int lev0, const int p[3]) {
+template <class RD = ValRead>
+__device__ typename RD::V face_read(const AmrFlowView& F, int a, const double* __restrict__ f, int lev0,
+                                   const int p[3]) {
+  using V = typename RD::V;
   const int N = F.L.lcells[lev0][a];
   if ((p[a] & 1) && p[a] < N && lev0 >= 1) {
     int lev;
     const int r = leaf_of(F.L, lev0, p, lev);
     if (r >= 0 && lev == lev0 - 1) {
       int q[3] = {p[0] >> 1, p[1] >> 1, p[2] >> 1};
-      const double lo = face_at(F, a, f, lev0 - 1, q);
+      const V lo = face_at<RD>(F, a, f, lev0 - 1, q);
       q[a] += 1;
-      const double hi = face_at(F, a, f, lev0 - 1, q);
+      const V hi = face_at<RD>(F, a, f, lev0 - 1, q);
       return 0.5 * (lo + hi);
     }
   }
-  return face_at(F, a, f, lev0, p);
+  return face_at<RD>(F, a, f, lev0, p);
 }
 
 __device__ __forceinline__ double inlet_amr(const AmrFlowView& F, int face, int lev, int jidx, int comp) {
@@ -171,25 +286,26 @@ __device__ __forceinline__ double inlet_amr(const AmrFlowView& F, int face, int 
 // about the stored boundary face 2 u_b - u_r, outlet copy, inlet value), then
 // the level-aware face read. The constants of the reference's nested
 // expressions c0 - (c1 - (... - term)) are unwound innermost-first.
-__device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restrict__ f, int lev, int i, int j,
-                          int k) {
+template <class RD = ValRead>
+__device__ __noinline__ typename RD::V amr_acc(const AmrFlowView& F, int comp, const double* __restrict__ f,
+                                              int lev, int i, int j, int k) {
+  using V = typename RD::V;
   const int nx = F.L.lcells[lev][0], ny = F.L.lcells[lev][1], nz = F.L.lcells[lev][2];
-  double cst[ACC_MAX];
-  int d = 0;
-  double term = 0.0;
+  Nest<RD> cst;
+  V term = RD::k(0.0);
   for (int guard = 0; guard < ACC_MAX; ++guard) {
     if (comp == 0) {
       if (k < 0 || k >= nz) {
         if (F.per[2]) { k = wrapi(k, nz); continue; }
         const int face = k < 0 ? 4 : 5;
-        cst[d++] = 2.0 * F.wallv[face][0];
+        cst.push(RD::k(2.0 * F.wallv[face][0]));
         k = k < 0 ? (-1 - k) : (2 * nz - 1 - k);
         continue;
       }
       if (j < 0 || j >= ny) {
         if (F.per[1]) { j = wrapi(j, ny); continue; }
         const int face = j < 0 ? 2 : 3;
-        cst[d++] = 2.0 * F.wallv[face][0];
+        cst.push(RD::k(2.0 * F.wallv[face][0]));
         j = j < 0 ? (-1 - j) : (2 * ny - 1 - j);
         continue;
       }
@@ -197,8 +313,8 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
         if (F.per[0]) { i = wrapi(i, nx); continue; }
         const int ib = i < 0 ? 0 : nx, face = i < 0 ? 0 : 1;
         const int pb[3] = {ib, j, k};
-        if (F.L.bc[face] == NB_BC_OUTLET) { term = face_read(F, 0, f, lev, pb); break; }
-        cst[d++] = 2.0 * face_read(F, 0, f, lev, pb);
+        if (F.L.bc[face] == NB_BC_OUTLET) { term = face_read<RD>(F, 0, f, lev, pb); break; }
+        cst.push(2.0 * face_read<RD>(F, 0, f, lev, pb));
         i = 2 * ib - i;
         continue;
       }
@@ -206,7 +322,7 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
       if (k < 0 || k >= nz) {
         if (F.per[2]) { k = wrapi(k, nz); continue; }
         const int face = k < 0 ? 4 : 5;
-        cst[d++] = 2.0 * F.wallv[face][1];
+        cst.push(RD::k(2.0 * F.wallv[face][1]));
         k = k < 0 ? (-1 - k) : (2 * nz - 1 - k);
         continue;
       }
@@ -214,7 +330,7 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
         if (F.per[0]) { i = wrapi(i, nx); continue; }
         const int im = i < 0 ? (-1 - i) : (2 * nx - 1 - i), face = i < 0 ? 0 : 1;
         if (F.L.bc[face] == NB_BC_INLET) {
-          cst[d++] = 2.0 * inlet_amr(F, face, lev, j, 1);
+          cst.push(RD::k(2.0 * inlet_amr(F, face, lev, j, 1)));
           i = im;
           continue;
         }
@@ -222,10 +338,10 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
           // j is unresolved here; stencil points have it in range, the clamp
           // keeps unused corner points in bounds.
           const int pb[3] = {i < 0 ? 0 : nx - 1, min(max(j, 0), ny), k};
-          term = face_read(F, 1, f, lev, pb);
+          term = face_read<RD>(F, 1, f, lev, pb);
           break;
         }
-        cst[d++] = 2.0 * F.wallv[face][1];
+        cst.push(RD::k(2.0 * F.wallv[face][1]));
         i = im;
         continue;
       }
@@ -233,8 +349,8 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
         if (F.per[1]) { j = wrapi(j, ny); continue; }
         const int jb = j < 0 ? 0 : ny, face = j < 0 ? 2 : 3;
         const int pb[3] = {i, jb, k};
-        if (F.L.bc[face] == NB_BC_OUTLET) { term = face_read(F, 1, f, lev, pb); break; }
-        cst[d++] = 2.0 * face_read(F, 1, f, lev, pb);
+        if (F.L.bc[face] == NB_BC_OUTLET) { term = face_read<RD>(F, 1, f, lev, pb); break; }
+        cst.push(2.0 * face_read<RD>(F, 1, f, lev, pb));
         j = 2 * jb - j;
         continue;
       }
@@ -242,7 +358,7 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
       if (j < 0 || j >= ny) {
         if (F.per[1]) { j = wrapi(j, ny); continue; }
         const int face = j < 0 ? 2 : 3;
-        cst[d++] = 2.0 * F.wallv[face][2];
+        cst.push(RD::k(2.0 * F.wallv[face][2]));
         j = j < 0 ? (-1 - j) : (2 * ny - 1 - j);
         continue;
       }
@@ -251,10 +367,10 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
         const int im = i < 0 ? (-1 - i) : (2 * nx - 1 - i), face = i < 0 ? 0 : 1;
         if (F.L.bc[face] == NB_BC_OUTLET) {
           const int pb[3] = {i < 0 ? 0 : nx - 1, j, min(max(k, 0), nz)};
-          term = face_read(F, 2, f, lev, pb);
+          term = face_read<RD>(F, 2, f, lev, pb);
           break;
         }
-        cst[d++] = 2.0 * F.wallv[face][2];
+        cst.push(RD::k(2.0 * F.wallv[face][2]));
         i = im;
         continue;
       }
@@ -262,17 +378,16 @@ __device__ double amr_acc(const AmrFlowView& F, int comp, const double* __restri
         if (F.per[2]) { k = wrapi(k, nz); continue; }
         const int kb = k < 0 ? 0 : nz;
         const int pb[3] = {i, j, kb};
-        cst[d++] = 2.0 * face_read(F, 2, f, lev, pb);
+        cst.push(2.0 * face_read<RD>(F, 2, f, lev, pb));
         k = 2 * kb - k;
         continue;
       }
     }
     const int pt[3] = {i, j, k};
-    term = face_read(F, comp, f, lev, pt);
+    term = face_read<RD>(F, comp, f, lev, pt);
     break;
   }
-  for (int q = d - 1; q >= 0; --q) term = cst[q] - term;
-  return term;
+  return cst.finish(term);
 }
 
 // Solid flag of the level-`lev0` cell p (outside the domain: not solid).
@@ -303,6 +418,103 @@ struct TileRef {
   __device__ __forceinline__ T operator()(int i, int j, int k) const { return t[tix(i, j, k)]; }
 };
 
+// Same-level leaves of the 27 brick positions around (and at) the brick, -1
+// where the position is outside the mesh or covered at another level.
+__device__ __forceinline__ void fill_nb27(const LevelView& L, int brick, int lev, int* nb27) {
+  if (threadIdx.x < 27) {
+    const int q = threadIdx.x;
+    nb27[q] = lut_at(L, lev, L.bcoord[3 * brick] + q % 3 - 1, L.bcoord[3 * brick + 1] + (q / 3) % 3 - 1,
+                     L.bcoord[3 * brick + 2] + q / 9 - 1);
+  }
+}
+
+// Point p of the momentum kernel's tile (offsets -3..11 around a brick at
+// cell origin o of a level with N cells): never read by a stencil (skip), the
+// brick's own cell, or a halo point at level cell g with, strictly inside the
+// domain, the same-level leaf r that holds it (-1: another level or none).
+struct HaloPt {
+  bool skip, inner;
+  int g[3];
+  int r;
+  long long slot;
+  // A halo point strictly inside the domain whose leaf is at this level is
+  // that leaf's stored cell slot: the ghost walker applies no domain rule
+  // there and its face lookup returns the slot (the minus-side slab is read
+  // only across a periodic low boundary, excluded per component).
+  __device__ bool fast(int a, const int per[3]) const { return r >= 0 && (g[a] >= 1 || !per[a]); }
+};
+
+__device__ __forceinline__ HaloPt halo_pt(const int o[3], const int N[3], const int* nb27, int p) {
+  HaloPt h;
+  const int ti = p % TW - 3, tj = (p / TW) % TW - 3, tk = p / (TW * TW) - 3;
+  h.skip = (ti < -1 || ti > 9) + (tj < -1 || tj > 9) + (tk < -1 || tk > 9) > 1;
+  h.inner = ti >= 0 && ti < 8 && tj >= 0 && tj < 8 && tk >= 0 && tk < 8;
+  h.g[0] = o[0] + ti;
+  h.g[1] = o[1] + tj;
+  h.g[2] = o[2] + tk;
+  h.r = -1;
+  if (!h.skip && !h.inner && h.g[0] >= 0 && h.g[1] >= 0 && h.g[2] >= 0 && h.g[0] < N[0] && h.g[1] < N[1] &&
+      h.g[2] < N[2])
+    h.r = nb27[(ti < 0 ? 0 : (ti < 8 ? 1 : 2)) + 3 * (tj < 0 ? 0 : (tj < 8 ? 1 : 2)) +
+               9 * (tk < 0 ? 0 : (tk < 8 ? 1 : 2))];
+  h.slot = ((tk & 7) << 6) | ((tj & 7) << 3) | (ti & 7);
+  return h;
+}
+
+// Ghost map of the momentum kernel: one entry per (tile point, component) that
+// the same-level fast path does not serve, in the brick's range
+// [gm_off[b], gm_off[b + 1]). Entry .x = p | a << 12 | nt << 14 and .y = the
+// first of its nt terms (index into the component's array, FP32 weight bits):
+// the value is sum_q w_q f[idx_q]. nt = GM_WALK keeps the walker for the
+// point: a form with a constant part (inlet values, moving walls), more than
+// AFF_MAX terms, or a weight that FP32 does not hold exactly.
+constexpr unsigned GM_WALK = 15;
+
+// Pass 1 (ent == nullptr): entries and terms per brick into count[2b],
+// count[2b + 1]. Pass 2: the entries at the host-scanned offsets eoff / toff,
+// in any order within a brick (each entry is read on its own).
+__global__ void __launch_bounds__(RHS_NT) k_ghost_map(AmrFlowView F, int* __restrict__ count,
+                                                      const int* __restrict__ eoff, const int* __restrict__ toff,
+                                                      uint2* __restrict__ ent, int2* __restrict__ term) {
+  const LevelView& L = F.L;
+  __shared__ int nb27[27];
+  __shared__ int ne, nterm;
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int lev = L.blevel[brick];
+    const int o[3] = {L.bcoord[3 * brick] * BR, L.bcoord[3 * brick + 1] * BR, L.bcoord[3 * brick + 2] * BR};
+    const int N[3] = {L.lcells[lev][0], L.lcells[lev][1], L.lcells[lev][2]};
+    fill_nb27(L, brick, lev, nb27);
+    if (threadIdx.x == 0) ne = nterm = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < TN; p += blockDim.x) {
+      const HaloPt h = halo_pt(o, N, nb27, p);
+      if (h.skip || h.inner) continue;
+      for (int a = 0; a < 3; ++a) {
+        if (h.fast(a, F.per)) continue;
+        const Aff A = amr_acc<AffRead>(F, a, nullptr, lev, h.g[0], h.g[1], h.g[2]);
+        bool ok = A.n >= 0 && A.c == 0.0;
+        for (int q = 0; ok && q < A.n; ++q) ok = static_cast<double>(static_cast<float>(A.w[q])) == A.w[q];
+        const int nt = ok ? A.n : 0;
+        const int e = atomicAdd(&ne, 1);
+        const int t = nt ? atomicAdd(&nterm, nt) : 0;
+        if (ent) {
+          const unsigned head = static_cast<unsigned>(p) | (static_cast<unsigned>(a) << 12) |
+                                ((ok ? static_cast<unsigned>(nt) : GM_WALK) << 14);
+          ent[eoff[brick] + e] = make_uint2(head, static_cast<unsigned>(toff[brick] + t));
+          for (int q = 0; q < nt; ++q)
+            term[toff[brick] + t + q] = make_int2(A.idx[q], __float_as_int(static_cast<float>(A.w[q])));
+        }
+      }
+    }
+    __syncthreads();
+    if (!ent && threadIdx.x == 0) {
+      count[2 * brick] = ne;
+      count[2 * brick + 1] = nterm;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Fused momentum RHS + SSP-RK3 combine on AMR bricks (owned faces only).
 // One CTA per brick (grid-stride): stage u, v, w at the brick's level over
@@ -312,13 +524,14 @@ struct TileRef {
 // boundary faces (ns_solver.cpp:325, even when periodic) and on faces touching
 // a solid.
 // ---------------------------------------------------------------------------
+// Bounds: FP32 tiles (40.5 KB) at 4 CTAs an SM, 64 registers; FP64 tiles
+// (81 KB) fit two CTAs an SM.
 template <typename T>
-__global__ void __launch_bounds__(RHS_NT) k_amr_rhs_rk(AmrFlowView F, int stage, const double* __restrict__ dtp,
-                                                       const double* __restrict__ u, const double* __restrict__ v,
-                                                       const double* __restrict__ w, const double* __restrict__ u0,
-                                                       const double* __restrict__ v0, const double* __restrict__ w0,
-                                                       double* __restrict__ uo, double* __restrict__ vo,
-                                                       double* __restrict__ wo) {
+__global__ void __launch_bounds__(RHS_NT, sizeof(T) == 4 ? 4 : 2)
+    k_amr_rhs_rk(AmrFlowView F, int stage, const double* __restrict__ dtp, const double* __restrict__ u,
+                 const double* __restrict__ v, const double* __restrict__ w, const double* __restrict__ u0,
+                 const double* __restrict__ v0, const double* __restrict__ w0, double* __restrict__ uo,
+                 double* __restrict__ vo, double* __restrict__ wo) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* tile[3];
   tile[0] = reinterpret_cast<T*>(smraw);
@@ -335,39 +548,41 @@ __global__ void __launch_bounds__(RHS_NT) k_amr_rhs_rk(AmrFlowView F, int stage,
   const double* in[3] = {u, v, w};
   const double* in0[3] = {u0, v0, w0};
   double* out[3] = {uo, vo, wo};
-  // Same-level leaves of the 27 brick positions around (and at) the brick,
-  // -1 where the position is outside the mesh or covered at another level.
   __shared__ int nb27[27];
   for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
     const int lev = L.blevel[brick];
     const int o[3] = {L.bcoord[3 * brick] * BR, L.bcoord[3 * brick + 1] * BR, L.bcoord[3 * brick + 2] * BR};
     const int N[3] = {L.lcells[lev][0], L.lcells[lev][1], L.lcells[lev][2]};
-    if (threadIdx.x < 27) {
-      const int q = threadIdx.x;
-      nb27[q] = lut_at(L, lev, L.bcoord[3 * brick] + q % 3 - 1, L.bcoord[3 * brick + 1] + (q / 3) % 3 - 1,
-                       L.bcoord[3 * brick + 2] + q / 9 - 1);
-    }
+    fill_nb27(L, brick, lev, nb27);
     __syncthreads();
+    const bool mapped = F.gm_off != nullptr;
     for (int p = threadIdx.x; p < TN; p += blockDim.x) {
-      const int ti = p % TW - 3, tj = (p / TW) % TW - 3, tk = p / (TW * TW) - 3;
-      const int far = (ti < -1 || ti > 9) + (tj < -1 || tj > 9) + (tk < -1 || tk > 9);
-      if (far > 1) continue;  // never read by a stencil
-      const bool inner = ti >= 0 && ti < 8 && tj >= 0 && tj < 8 && tk >= 0 && tk < 8;
-      const int g[3] = {o[0] + ti, o[1] + tj, o[2] + tk};
-      // A halo point strictly inside the domain whose leaf is at this level is
-      // that leaf's stored cell slot: the ghost walker applies no domain rule
-      // there and its face lookup returns the slot (the minus-side slab is
-      // read only across a periodic low boundary, excluded per component).
-      int r = -1;
-      if (!inner && g[0] >= 0 && g[1] >= 0 && g[2] >= 0 && g[0] < N[0] && g[1] < N[1] && g[2] < N[2])
-        r = nb27[(ti < 0 ? 0 : (ti < 8 ? 1 : 2)) + 3 * (tj < 0 ? 0 : (tj < 8 ? 1 : 2)) +
-                 9 * (tk < 0 ? 0 : (tk < 8 ? 1 : 2))];
-      const long long slot = ((tk & 7) << 6) | ((tj & 7) << 3) | (ti & 7);
+      const HaloPt h = halo_pt(o, N, nb27, p);
+      if (h.skip) continue;
       for (int a = 0; a < 3; ++a) {
         double val;
-        if (inner) val = in[a][brick * static_cast<long long>(BR3) + slot];
-        else if (r >= 0 && (g[a] >= 1 || !F.per[a])) val = in[a][r * static_cast<long long>(BR3) + slot];
-        else val = amr_acc(F, a, in[a], lev, g[0], g[1], g[2]);
+        if (h.inner) val = in[a][brick * static_cast<long long>(BR3) + h.slot];
+        else if (h.fast(a, F.per)) val = in[a][h.r * static_cast<long long>(BR3) + h.slot];
+        else if (mapped) continue;  // the brick's ghost map below
+        else val = amr_acc(F, a, in[a], lev, h.g[0], h.g[1], h.g[2]);
+        tile[a][p] = static_cast<T>(val);
+      }
+    }
+    if (mapped) {  // the walker's points: recorded forms, or the walker itself (GM_WALK)
+      const int e1 = F.gm_off[brick + 1];
+      for (int e = F.gm_off[brick] + threadIdx.x; e < e1; e += blockDim.x) {
+        const uint2 E = F.gm_ent[e];
+        const int p = E.x & 4095, a = (E.x >> 12) & 3, nt = static_cast<int>(E.x >> 14);
+        double val;
+        if (nt == static_cast<int>(GM_WALK)) {
+          val = amr_acc(F, a, in[a], lev, o[0] + p % TW - 3, o[1] + (p / TW) % TW - 3, o[2] + p / (TW * TW) - 3);
+        } else {
+          val = 0.0;
+          for (int q = 0; q < nt; ++q) {
+            const int2 t = F.gm_term[E.y + q];
+            val += static_cast<double>(__int_as_float(t.y)) * in[a][t.x];
+          }
+        }
         tile[a][p] = static_cast<T>(val);
       }
     }
@@ -789,6 +1004,17 @@ void amr_flow_setup() {
                                3 * TN * static_cast<int>(sizeof(double))));
   NB_CUDA(cudaFuncSetAttribute(k_amr_rhs_rk<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                3 * TN * static_cast<int>(sizeof(float))));
+}
+
+void launch_ghost_count(cudaStream_t s, const AmrFlowView& F, int* count) {
+  k_ghost_map<<<grid_for(F.L.nbrick), RHS_NT, 0, s>>>(F, count, nullptr, nullptr, nullptr, nullptr);
+  NB_CUDA(cudaGetLastError());
+}
+
+void launch_ghost_fill(cudaStream_t s, const AmrFlowView& F, const int* eoff, const int* toff, uint2* ent,
+                       int2* term) {
+  k_ghost_map<<<grid_for(F.L.nbrick), RHS_NT, 0, s>>>(F, nullptr, eoff, toff, ent, term);
+  NB_CUDA(cudaGetLastError());
 }
 
 void launch_amr_rhs_rk(cudaStream_t s, const AmrFlowView& F, int stage, const double* dtp, const double* u,

@@ -23,6 +23,11 @@ struct AmrFlowView {
   int weno;
   double nu;
   double bf[3];
+  // Ghost map of the momentum kernel (k_ghost_map); null: the walker serves
+  // every halo point that the same-level fast path does not.
+  const int* gm_off;    // [nbrick + 1] entry ranges
+  const uint2* gm_ent;  // entries: point | component | term count, first term
+  const int2* gm_term;  // terms: array index, FP32 weight bits
 };
 
 struct AmrStepScalars {
@@ -33,6 +38,12 @@ void amr_flow_setup();
 void launch_amr_rhs_rk(cudaStream_t s, const AmrFlowView& F, int stage, const double* dtp, const double* u,
                        const double* v, const double* w, const double* u0, const double* v0,
                        const double* w0, double* uo, double* vo, double* wo, int mixed, int grid_cap);
+// Ghost map builder: pass 1 counts entries and terms per brick into count
+// [2 nbrick]; pass 2 writes them at the scanned offsets eoff [nbrick],
+// toff [nbrick].
+void launch_ghost_count(cudaStream_t s, const AmrFlowView& F, int* count);
+void launch_ghost_fill(cudaStream_t s, const AmrFlowView& F, const int* eoff, const int* toff, uint2* ent,
+                       int2* term);
 void launch_amr_sync(cudaStream_t s, const long long* list, int n, double* f);
 void launch_amr_div(cudaStream_t s, const AmrFlowView& F, const double* u, const double* v, const double* w,
                     double* b);

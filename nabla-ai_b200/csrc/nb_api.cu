@@ -1434,6 +1434,42 @@ nb_status nb_apply_laplacian(nb_ctx* ctx, const nb_grid_desc* grid, const double
 // ===========================================================================
 extern "C" {
 
+// The momentum kernel's ghost map: the walker's recorded form for every halo
+// point that the same-level fast path does not serve, built once per case on
+// the case's stream (count, host scan, fill; no device-wide synchronisation,
+// which would break another thread's graph capture). Without it (more than
+// 2^31 entries or terms) the kernel walks those points at every stage.
+static void build_ghost_map(nb_case& c, AmrFlowView& F) {
+  const int nb = F.L.nbrick;
+  int* dcount = static_cast<int*>(c.alloc(2 * static_cast<size_t>(nb) * sizeof(int)));
+  launch_ghost_count(c.stream, F, dcount);
+  NB_CUDA(cudaStreamSynchronize(c.stream));
+  std::vector<int> cnt(2 * static_cast<size_t>(nb));
+  NB_CUDA(cudaMemcpy(cnt.data(), dcount, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<int> eoff(static_cast<size_t>(nb) + 1), toff(static_cast<size_t>(nb));
+  long long ne = 0, nt = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (ne > INT32_MAX || nt > INT32_MAX) return;
+    eoff[b] = static_cast<int>(ne);
+    toff[b] = static_cast<int>(nt);
+    ne += cnt[2 * static_cast<size_t>(b)];
+    nt += cnt[2 * static_cast<size_t>(b) + 1];
+  }
+  if (ne > INT32_MAX || nt > INT32_MAX) return;
+  eoff[nb] = static_cast<int>(ne);
+  int* d_eoff = static_cast<int*>(c.alloc(eoff.size() * sizeof(int)));
+  int* d_toff = static_cast<int*>(c.alloc(toff.size() * sizeof(int)));
+  auto* d_ent = static_cast<uint2*>(c.alloc(static_cast<size_t>(ne) * sizeof(uint2)));
+  auto* d_term = static_cast<int2*>(c.alloc(static_cast<size_t>(nt) * sizeof(int2)));
+  NB_CUDA(cudaMemcpy(d_eoff, eoff.data(), eoff.size() * sizeof(int), cudaMemcpyHostToDevice));
+  NB_CUDA(cudaMemcpy(d_toff, toff.data(), toff.size() * sizeof(int), cudaMemcpyHostToDevice));
+  launch_ghost_fill(c.stream, F, d_eoff, d_toff, d_ent, d_term);
+  NB_CUDA(cudaStreamSynchronize(c.stream));
+  F.gm_off = d_eoff;
+  F.gm_ent = d_ent;
+  F.gm_term = d_term;
+}
+
 nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_config* cfg, int precision,
                              nb_case** out) {
   if (!ctx || !mesh || !cfg || !out) return NB_ERR_BAD_ARG;
@@ -1528,6 +1564,7 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     F.weno = cfg->convection == NB_CONV_WENO5;
     F.nu = c->nu;
     for (int a = 0; a < 3; ++a) F.bf[a] = cfg->body_force[a];
+    build_ghost_map(*c, F);
     for (int h = 0; h < 2; ++h)
       for (int q = 0; q < 3; ++q) {
         const size_t nb = static_cast<size_t>(c->fm.store[q]) * sizeof(double);
