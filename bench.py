@@ -417,6 +417,7 @@ def large_case(args, ctx, flush, world, device):
         out[name + "_ms_per_step"] = round(el / args.large_steps, 3)
         out[name + "_divergence_max"] = max(r.divergence_max for r in reps)
         out[name + "_poisson_cycles_per_step"] = reps[-1].poisson_iters
+        out[name + "_device_bytes"] = int(ctx.lib.nb_case_device_bytes(case.h))
         shares = {fam: profile_step(ctx, run, fam) for fam in FAMILIES}
         shares = {k: v for k, v in shares.items() if v[1] > 0}
         total = sum(v[0] for v in shares.values()) or 1.0
