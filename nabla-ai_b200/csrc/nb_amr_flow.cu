@@ -740,6 +740,11 @@ __global__ void __launch_bounds__(NT) k_amr_correct(AmrFlowView F, const double*
             // outlet ghost -phi (Dirichlet 0), Neumann ghost phi (ns_solver.cpp:508-526)
             const double g = L.bc[2 * a] == NB_BC_OUTLET ? -pc : pc;
             f[a][c] -= (pc - g) / h;
+          } else if (rel == R_SAME) {
+            // the -a cell is the same-level neighbour's (periodic wrap applied)
+            // cell with loc[a] = 7: the cell solid_at and phi_cell resolve
+            const long long cn = F.nbr_lo[3 * brick + a] * static_cast<long long>(BR3) + l + 7 * stride;
+            if (L.type[cn] != CELL_SOLID) f[a][c] -= (pc - phi[cn]) / h;
           } else if (rel != R_FINER) {
             int q[3] = {p[0], p[1], p[2]};
             q[a] -= 1;

@@ -238,6 +238,40 @@ __device__ __forceinline__ void fill_halo_amr(const LevelView& L, int brick, T* 
   }
 }
 
+// Static maps of the brick a CTA stages next, in shared memory: the six face
+// neighbours, for a pending prolongation the parent brick and octant of the
+// brick and of each neighbour, and on a composite restriction the coarse
+// brick, octant and weight its residual goes to. The maps are never written
+// during a solve, so a kernel reads its first brick's before pdl_wait() (a CTA
+// that becomes resident while its predecessor grid drains has them before the
+// wait returns, and its halo loads then depend on no further map load) and
+// each later brick's at the end of the previous one. Two records alternate by
+// iteration parity: a brick's record is read after its first barrier (the
+// restriction's coarse target) while the next brick's is being written.
+struct BrickPre {
+  int pb, po, xcb, xoct;
+  double wc;
+  int nb[6], npb[6], npo[6];
+};
+
+__device__ __forceinline__ void prefetch_brick(const LevelView& L, int brick, bool pro, BrickPre& P,
+                                               const LevelView* C = nullptr) {
+  const int t = threadIdx.x;
+  if (brick >= L.nbrick) return;
+  if (L.fast && t < 6) {
+    P.nb[t] = L.nbr6[brick * 6 + t];
+    P.npb[t] = pro ? L.npar6[brick * 6 + t] : 0;
+    P.npo[t] = pro ? L.npoct6[brick * 6 + t] : -1;
+  } else if (L.fast && t == 6) {
+    P.pb = pro ? L.par[brick] : 0;
+    P.po = pro ? L.poct[brick] : -1;
+  } else if (t == 7 && C && L.amr) {
+    P.xcb = L.xf_brick[brick];
+    P.xoct = L.xf_oct[brick];
+    P.wc = C->amr ? C->bweight[P.xcb] : 1.0;
+  }
+}
+
 // The loads of fill_halo_fast into registers (the brick's own values and its
 // face halo), and their stores into the tile: split so that a CTA can have the
 // next brick's loads in flight while it computes the current one.
@@ -291,12 +325,13 @@ __device__ __forceinline__ void halo_store(T* tile, const T* own, const T* halo,
 // the six neighbour bricks (6 faces x 64). Every load is issued before the
 // first store to shared memory, so all of them are in flight together.
 template <typename T, int NTH, class F>
-__device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T* tile, const F& fx) {
+__device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T* tile, const F& fx,
+                                               const BrickPre* pre = nullptr) {
   constexpr int CPT = BR3 / NTH;
   constexpr int HPT = (384 + NTH - 1) / NTH;
   const int t = threadIdx.x;
   const bool pro = fx.prolongs();
-  const int pb = pro ? L.par[brick] : 0, po = pro ? L.poct[brick] : -1;
+  const int pb = pre ? pre->pb : (pro ? L.par[brick] : 0), po = pre ? pre->po : (pro ? L.poct[brick] : -1);
   T own[CPT];
 #pragma unroll
   for (int q = 0; q < CPT; ++q) own[q] = fx.at(brick * BR3 + t + q * NTH, pb, po, L.amr);
@@ -317,9 +352,10 @@ __device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T*
       const int ti = a == 0 ? et : u, tj = a == 1 ? et : (a == 0 ? u : w), tk = a == 2 ? et : w;
       const int li = a == 0 ? el : u, lj = a == 1 ? el : (a == 0 ? u : w), lk = a == 2 ? el : w;
       hpos[q] = tpos(ti, tj, tk);
-      const int nb = L.nbr6[brick * 6 + f];
+      const int nb = pre ? pre->nb[f] : L.nbr6[brick * 6 + f];
       if (nb >= 0) {
-        const int npb = pro ? L.npar6[brick * 6 + f] : 0, npo = pro ? L.npoct6[brick * 6 + f] : -1;
+        const int npb = pre ? pre->npb[f] : (pro ? L.npar6[brick * 6 + f] : 0);
+        const int npo = pre ? pre->npo[f] : (pro ? L.npoct6[brick * 6 + f] : -1);
         halo[q] = fx.at(nb * BR3 + ((lk << 6) | (lj << 3) | li), npb, npo, L.amr);
       }
     }
@@ -333,9 +369,10 @@ __device__ __forceinline__ void fill_halo_fast(const LevelView& L, int brick, T*
 
 // Stages brick `brick` of L into `tile`; NTH is the CTA's thread count.
 template <typename T, int NTH = NT, class F>
-__device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile, const F& fx) {
+__device__ __forceinline__ void fill_halo(const LevelView& L, int brick, T* tile, const F& fx,
+                                          const BrickPre* pre = nullptr) {
   if (L.fast) {
-    fill_halo_fast<T, NTH>(L, brick, tile, fx);
+    fill_halo_fast<T, NTH>(L, brick, tile, fx, pre);
     return;
   }
   if (L.amr) {
@@ -487,7 +524,8 @@ __device__ __forceinline__ T sweep_cell(const LevelView& L, int brick, int l, ui
 template <typename T, int NTH, class ACC, class FX, class FP, class OUT, bool PIPE = false>
 __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, const double* bmean, const FX& X,
                                              OUT& sink, T c2, T c1, int prev_mode, const FP& P, int first,
-                                             int stride, T* tile, const ACC& acc, int b16 = 0) {
+                                             int stride, T* tile, const ACC& acc, int b16 = 0,
+                                             BrickPre* pre = nullptr) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   constexpr int HPT = (384 + NTH - 1) / NTH;
   const bool staged = X.x || X.ec;
@@ -533,7 +571,7 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
       }
     }
   }
-  for (int brick = first; brick < L.nbrick; brick += stride) {
+  for (int brick = first, it = 0; brick < L.nbrick; brick += stride, ++it) {
     uint32_t code[CPT];
     T bv[CPT];
 #pragma unroll
@@ -542,7 +580,7 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
       code[q] = L.code[c];
       bv[q] = b16 ? ld_b16(b, c) : acc.ld(b, c);
     }
-    if (staged) fill_halo<T, NTH>(L, brick, tile, X);
+    if (staged) fill_halo<T, NTH>(L, brick, tile, X, pre ? pre + (it & 1) : nullptr);
     __syncthreads();
     const double wgt = cell_weight(L, brick);
 #pragma unroll
@@ -590,6 +628,7 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
       }
       sink(c, wgt, out, fluid);
     }
+    if (pre) prefetch_brick(L, brick + stride, X.prolongs(), pre[(it + 1) & 1]);  // read after the next barrier
     __syncthreads();
   }
 }
@@ -608,21 +647,32 @@ __device__ __forceinline__ void smooth_launch(const LevelView& L, const T* __res
                                               const XFetch<T>& X, T* xout, const RedBuf& rb, double* mean_out,
                                               double inv_nfluid, const SolveFlags* flags, int maxit, T c2, T c1,
                                               int prev_mode, const XFetch<T>& P, int b16) {
+  __shared__ BrickPre pre[2];
+  if (!PIPE) prefetch_brick(L, blockIdx.x, X.prolongs(), pre[0]);
   pdl_wait();
+  __syncthreads();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   const GAcc acc{};
   SweepOut<T, GAcc> sink{xout, acc};
-  smooth_bricks<T, NTH, GAcc, XFetch<T>, XFetch<T>, SweepOut<T, GAcc>, PIPE>(L, b, bmean, X, sink, c2, c1, prev_mode,
-                                                                            P, blockIdx.x, gridDim.x, tile, acc, b16);
+  smooth_bricks<T, NTH, GAcc, XFetch<T>, XFetch<T>, SweepOut<T, GAcc>, PIPE>(
+      L, b, bmean, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, acc, b16, PIPE ? nullptr : pre);
   if (mean_out) {
     double part[1] = {sink.part};
     grid_reduce<1>(part, rb, [=] __device__(const double* t) { *mean_out = t[0] * inv_nfluid; });
   }
 }
 
+// CTAs an SM each sweep instantiation is built for, from its register budget
+// (32 registers for FP32 at 512 threads, 40 for FP64): the bound also sizes
+// the driver's shared-memory carveout for that many CTAs.
 template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH) k_smooth(LevelView L, const T* __restrict__ b, const double* bmean,
+constexpr int sweep_ctas() {
+  return NTH == 512 ? (sizeof(T) == 4 ? 4 : 3) : (NTH == 256 ? 5 : 8);
+}
+
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH, sweep_ctas<T, NTH>()) k_smooth(LevelView L, const T* __restrict__ b, const double* bmean,
                                                 XFetch<T> X, T* xout, RedBuf rb, double* mean_out,
                                                 double inv_nfluid, const SolveFlags* flags, int maxit, T c2, T c1,
                                                 int prev_mode, XFetch<T> P, int b16) {
@@ -663,16 +713,19 @@ struct DotsOut {
 };
 
 template <typename T, int NTH>
-__global__ void __launch_bounds__(NTH) k_smooth_dots(LevelView L, const T* __restrict__ b, XFetch<T> X,
+__global__ void __launch_bounds__(NTH, sweep_ctas<T, NTH>()) k_smooth_dots(LevelView L, const T* __restrict__ b, XFetch<T> X,
                                                      double* __restrict__ zo, const double* __restrict__ rnew,
                                                      const double* __restrict__ r, RedBuf rb, double* S,
                                                      SolveFlags* flags, int maxit, T c2, T c1, int prev_mode,
                                                      XFetch<T> P) {
+  __shared__ BrickPre pre[2];
+  prefetch_brick(L, blockIdx.x, X.prolongs(), pre[0]);
   pdl_wait();
+  __syncthreads();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   DotsOut<T> sink{zo, rnew, r};
-  smooth_bricks<T, NTH>(L, b, nullptr, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, GAcc{});
+  smooth_bricks<T, NTH>(L, b, nullptr, X, sink, c2, c1, prev_mode, P, blockIdx.x, gridDim.x, tile, GAcc{}, 0, pre);
   grid_reduce<2>(sink.part, rb, [=] __device__(const double* t) { flex_beta(t, S, flags); });
 }
 
@@ -715,11 +768,12 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
                                                        const FX& X, const LevelView& C, int fx, int fy, int fz,
                                                        T* rc, int first, int stride, T* tile, T* rs, uint8_t* fl,
                                                        const ACC& acc, int bio = 0, T* xf = nullptr,
-                                                       T c2f = T(0)) {
+                                                       T c2f = T(0), BrickPre* pre = nullptr) {
   constexpr int CPT = BR3 / NTH;  // cells per thread
   double part = 0.0;
   const int cx = BR / fx, cy = BR / fy, cz = BR / fz;
-  for (int brick = first; brick < F.nbrick; brick += stride) {
+  for (int brick = first, it = 0; brick < F.nbrick; brick += stride, ++it) {
+    BrickPre* const cur = pre ? pre + (it & 1) : nullptr;
     uint32_t code[CPT];
     T bv[CPT];
 #pragma unroll
@@ -728,7 +782,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
       code[q] = F.code[c];
       bv[q] = (bio & 1) ? ld_b16(b, c) : acc.ld(b, c);
     }
-    fill_halo<T, NTH>(F, brick, tile, X);
+    fill_halo<T, NTH>(F, brick, tile, X, cur);
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < CPT; ++q) {
@@ -750,8 +804,8 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
     if (F.amr) {
       // composite transfer: a kept brick maps cell-for-cell; a merged brick
       // fills one octant (4^3 cells) of its parent with child averages.
-      const int cb = F.xf_brick[brick], oct = F.xf_oct[brick];
-      const double wc = cell_weight(C, cb);
+      const int cb = cur ? cur->xcb : F.xf_brick[brick], oct = cur ? cur->xoct : F.xf_oct[brick];
+      const double wc = cur ? cur->wc : cell_weight(C, cb);
       if (oct < 0) {
         for (int t = threadIdx.x; t < BR3; t += NTH) {
           const T val = fl[t] ? rs[t] : T(0);
@@ -807,6 +861,7 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
         }
       }
     }
+    if (pre) prefetch_brick(F, brick + stride, X.prolongs(), pre[(it + 1) & 1], &C);  // read after the next barrier
     __syncthreads();
   }
   return part;
@@ -822,13 +877,16 @@ __global__ void __launch_bounds__(NTH, NTH == 256 ? 2 : 4) k_resid_restrict(Leve
                                                         RedBuf rb, double* mean_out, double inv_nfluid_c,
                                                         const SolveFlags* flags, int maxit, int bio, T* xf,
                                                         T c2f) {
+  __shared__ BrickPre pre[2];
+  prefetch_brick(F, blockIdx.x, X.prolongs(), pre[0], &C);
   pdl_wait();
+  __syncthreads();
   if (stopped(flags, maxit)) return;
   __shared__ T tile[TSN];
   __shared__ T rs[BR3];
   __shared__ uint8_t fl[BR3];
   double part[1] = {resid_restrict_bricks<T, NTH>(F, b, bmean, X, C, fx, fy, fz, rc, blockIdx.x, gridDim.x, tile,
-                                                  rs, fl, GAcc{}, bio, xf, c2f)};
+                                                  rs, fl, GAcc{}, bio, xf, c2f, pre)};
   if (mean_out) {
     grid_reduce<1>(part, rb, [=] __device__(const double* tt) { *mean_out = tt[0] * inv_nfluid_c; });
   }
