@@ -232,9 +232,18 @@ __global__ void __launch_bounds__(RHS_NT) k_rhs_rk(FlowView F, int stage, const 
       const int far = (ti < 2 || ti > 11) + (tj < 2 || tj > 11) + (tk < 2 || tk > 11);
       if (far > 1) continue;  // never read by any stencil
       const int gi = ox + ti - 3, gj = oy + tj - 3, gk = oz + tk - 3;
-      tu[p] = static_cast<T>(acc_u(F, u, gi, gj, gk));
-      tv[p] = static_cast<T>(acc_v(F, v, gi, gj, gk));
-      tw[p] = static_cast<T>(acc_w(F, w, gi, gj, gk));
+      if (gi >= 0 && gj >= 0 && gk >= 0 && gi < nx && gj < ny && gk < nz) {
+        // strictly inside the domain no ghost rule applies: every accessor
+        // reads the cell's stored low face
+        const long long c = cell_index(L, gi, gj, gk);
+        tu[p] = static_cast<T>(u[c]);
+        tv[p] = static_cast<T>(v[c]);
+        tw[p] = static_cast<T>(w[c]);
+      } else {
+        tu[p] = static_cast<T>(acc_u(F, u, gi, gj, gk));
+        tv[p] = static_cast<T>(acc_v(F, v, gi, gj, gk));
+        tw[p] = static_cast<T>(acc_w(F, w, gi, gj, gk));
+      }
     }
     __syncthreads();
     // Face jobs: component a's low face of every cell (one RHS call site).
