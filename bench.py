@@ -397,13 +397,15 @@ def large_case(args, ctx, flush, world, device):
     import torch
 
     from nabla_b200 import abi, amr, cases, workloads
-    geom, leaves = workloads.tgv_octree(128)
+    base = args.large_base
+    geom, leaves = workloads.tgv_octree(base)
     mesh = amr.AmrMesh(geom, leaves, ctx=ctx)
     cfg = cases.flow_config(reynolds=1600.0, ref_length=1.0, velocity_scale=1.0, cfl=0.4,
                             convection=abi.CONV_WENO5, poisson_tol=1e-10, poisson_max_iters=200)
     hbm, peak_kind = peaks()
-    out = {"workload": "3-level octree of the periodic Taylor-Green box at effective 512^3 (the largest config-3 "
-                       "mesh), nu=1/1600, WENO-5, CFL 0.4, MG-PCG to 1e-10, from the Taylor-Green state",
+    what = "the largest config-3 mesh" if base == 128 else f"base {base}^3"
+    out = {"workload": f"3-level octree of the periodic Taylor-Green box at effective {4 * base}^3 ({what}), "
+                       "nu=1/1600, WENO-5, CFL 0.4, MG-PCG to 1e-10, from the Taylor-Green state",
            "cells": mesh.ncell, "steps": args.large_steps}
     for name, prec in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
         case = amr.AmrCase(mesh, cfg, precision=prec)
@@ -933,6 +935,9 @@ def main():
                     help="channel3: timed steps of both forms on the 96-case batch (0: skip)")
     ap.add_argument("--large-steps", type=int, default=5,
                     help="channel3: steps of both forms on the 512^3-effective octree (0: skip)")
+    ap.add_argument("--large-base", type=int, default=128,
+                    help="base grid of that octree (a multiple of 8; effective 4x): 128 is the largest "
+                         "config-3 mesh, smaller bases are profiling cases")
     ap.add_argument("--same-case-steps", type=int, default=5,
                     help="channel3: steps of both forms on the reference arm's uniform-fine case (0: skip)")
     ap.add_argument("--shares", type=int, default=1,

@@ -582,6 +582,8 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
     }
     if (staged) fill_halo<T, NTH>(L, brick, tile, X, pre ? pre + (it & 1) : nullptr);
     __syncthreads();
+    // the next brick's maps, in flight during this brick's arithmetic (the other record)
+    if (pre) prefetch_brick(L, brick + stride, X.prolongs(), pre[(it + 1) & 1]);
     const double wgt = cell_weight(L, brick);
 #pragma unroll
     for (int q = 0; q < CPT; ++q) {
@@ -628,7 +630,6 @@ __device__ __forceinline__ void smooth_bricks(const LevelView& L, const T* b, co
       }
       sink(c, wgt, out, fluid);
     }
-    if (pre) prefetch_brick(L, brick + stride, X.prolongs(), pre[(it + 1) & 1]);  // read after the next barrier
     __syncthreads();
   }
 }
@@ -784,6 +785,8 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
     }
     fill_halo<T, NTH>(F, brick, tile, X, cur);
     __syncthreads();
+    // the next brick's maps, in flight during this brick's arithmetic (the other record)
+    if (pre) prefetch_brick(F, brick + stride, X.prolongs(), pre[(it + 1) & 1], &C);
 #pragma unroll
     for (int q = 0; q < CPT; ++q) {
       const int l = threadIdx.x + q * NTH;
@@ -861,7 +864,6 @@ __device__ __forceinline__ double resid_restrict_bricks(const LevelView& F, cons
         }
       }
     }
-    if (pre) prefetch_brick(F, brick + stride, X.prolongs(), pre[(it + 1) & 1], &C);  // read after the next barrier
     __syncthreads();
   }
   return part;
