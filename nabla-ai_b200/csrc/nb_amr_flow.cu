@@ -470,12 +470,18 @@ __device__ __forceinline__ HaloPt halo_pt(const int o[3], const int N[3], const 
 // AFF_MAX terms, or a weight that FP32 does not hold exactly.
 constexpr unsigned GM_WALK = 15;
 
-// Pass 1 (ent == nullptr): entries and terms per brick into count[2b],
-// count[2b + 1]. Pass 2: the entries at the host-scanned offsets eoff / toff,
-// in any order within a brick (each entry is read on its own).
-__global__ void __launch_bounds__(RHS_NT) k_ghost_map(AmrFlowView F, int* __restrict__ count,
-                                                      const int* __restrict__ eoff, const int* __restrict__ toff,
-                                                      uint2* __restrict__ ent, int2* __restrict__ term) {
+constexpr unsigned GM_NONE = 0xFF;  // (point, component) served by the fast path: no entry
+
+// The recorded form of halo point h's component a: its term count, or GM_WALK.
+__device__ __forceinline__ unsigned ghost_form(const AmrFlowView& F, int lev, const HaloPt& h, int a, Aff& A) {
+  A = amr_acc<AffRead>(F, a, nullptr, lev, h.g[0], h.g[1], h.g[2]);
+  bool ok = A.n >= 0 && A.c == 0.0;
+  for (int q = 0; ok && q < A.n; ++q) ok = static_cast<double>(static_cast<float>(A.w[q])) == A.w[q];
+  return ok ? static_cast<unsigned>(A.n) : GM_WALK;
+}
+
+// Pass 1: entries and terms per brick into count[2b], count[2b + 1].
+__global__ void __launch_bounds__(RHS_NT) k_ghost_map(AmrFlowView F, int* __restrict__ count) {
   const LevelView& L = F.L;
   __shared__ int nb27[27];
   __shared__ int ne, nterm;
@@ -491,25 +497,105 @@ __global__ void __launch_bounds__(RHS_NT) k_ghost_map(AmrFlowView F, int* __rest
       if (h.skip || h.inner) continue;
       for (int a = 0; a < 3; ++a) {
         if (h.fast(a, F.per)) continue;
-        const Aff A = amr_acc<AffRead>(F, a, nullptr, lev, h.g[0], h.g[1], h.g[2]);
-        bool ok = A.n >= 0 && A.c == 0.0;
-        for (int q = 0; ok && q < A.n; ++q) ok = static_cast<double>(static_cast<float>(A.w[q])) == A.w[q];
-        const int nt = ok ? A.n : 0;
-        const int e = atomicAdd(&ne, 1);
-        const int t = nt ? atomicAdd(&nterm, nt) : 0;
-        if (ent) {
-          const unsigned head = static_cast<unsigned>(p) | (static_cast<unsigned>(a) << 12) |
-                                ((ok ? static_cast<unsigned>(nt) : GM_WALK) << 14);
-          ent[eoff[brick] + e] = make_uint2(head, static_cast<unsigned>(toff[brick] + t));
-          for (int q = 0; q < nt; ++q)
-            term[toff[brick] + t + q] = make_int2(A.idx[q], __float_as_int(static_cast<float>(A.w[q])));
-        }
+        Aff A;
+        const unsigned c = ghost_form(F, lev, h, a, A);
+        atomicAdd(&ne, 1);
+        if (c != GM_WALK && c > 0) atomicAdd(&nterm, static_cast<int>(c));
       }
     }
     __syncthreads();
-    if (!ent && threadIdx.x == 0) {
+    if (threadIdx.x == 0) {
       count[2 * brick] = ne;
       count[2 * brick + 1] = nterm;
+    }
+    __syncthreads();
+  }
+}
+
+// Exclusive prefix sums of (x, y) over the CTA's threads in thread order
+// (RHS_NT threads; ws holds 2 x RHS_NT / 32 ints).
+__device__ __forceinline__ void block_exscan2(int& x, int& y, int* ws) {
+  constexpr int NW = RHS_NT / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int ix = x, iy = y;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int ux = __shfl_up_sync(0xffffffffu, ix, d), uy = __shfl_up_sync(0xffffffffu, iy, d);
+    if (lane >= d) {
+      ix += ux;
+      iy += uy;
+    }
+  }
+  if (lane == 31) {
+    ws[w] = ix;
+    ws[NW + w] = iy;
+  }
+  __syncthreads();
+  int px = 0, py = 0;
+  for (int k = 0; k < w; ++k) {
+    px += ws[k];
+    py += ws[NW + k];
+  }
+  x = px + ix - x;
+  y = py + iy - y;
+  __syncthreads();
+}
+
+// Pass 2: a brick's entries at the host-scanned offsets eoff / toff, sorted by
+// component, then tile position (neighbouring threads of the momentum kernel
+// then gather neighbouring cells). The term codes go to a shared table first,
+// a block scan in that order places every entry, and each entry's form is
+// recorded again where it is written.
+__global__ void __launch_bounds__(RHS_NT) k_ghost_fill(AmrFlowView F, const int* __restrict__ eoff,
+                                                       const int* __restrict__ toff, uint2* __restrict__ ent,
+                                                       int2* __restrict__ term) {
+  constexpr int NE = 3 * TN;                         // (component, tile point) pairs, component-major
+  constexpr int CH = (NE + RHS_NT - 1) / RHS_NT;     // pairs per thread, in order
+  const LevelView& L = F.L;
+  __shared__ int nb27[27];
+  __shared__ uint8_t tcode[NE];
+  __shared__ int ws[2 * (RHS_NT / 32)];
+  for (int brick = blockIdx.x; brick < L.nbrick; brick += gridDim.x) {
+    const int lev = L.blevel[brick];
+    const int o[3] = {L.bcoord[3 * brick] * BR, L.bcoord[3 * brick + 1] * BR, L.bcoord[3 * brick + 2] * BR};
+    const int N[3] = {L.lcells[lev][0], L.lcells[lev][1], L.lcells[lev][2]};
+    fill_nb27(L, brick, lev, nb27);
+    __syncthreads();
+    for (int p = threadIdx.x; p < TN; p += blockDim.x) {
+      const HaloPt h = halo_pt(o, N, nb27, p);
+      for (int a = 0; a < 3; ++a) {
+        unsigned c = GM_NONE;
+        if (!h.skip && !h.inner && !h.fast(a, F.per)) {
+          Aff A;
+          c = ghost_form(F, lev, h, a, A);
+        }
+        tcode[a * TN + p] = static_cast<uint8_t>(c);
+      }
+    }
+    __syncthreads();
+    const int e0 = threadIdx.x * CH, e1 = min(e0 + CH, NE);
+    int ne = 0, nt = 0;
+    for (int e = e0; e < e1; ++e) {
+      const unsigned c = tcode[e];
+      if (c == GM_NONE) continue;
+      ++ne;
+      if (c != GM_WALK) nt += static_cast<int>(c);
+    }
+    block_exscan2(ne, nt, ws);
+    int ei = eoff[brick] + ne, ti = toff[brick] + nt;
+    for (int e = e0; e < e1; ++e) {
+      const unsigned c = tcode[e];
+      if (c == GM_NONE) continue;
+      const int a = e / TN, p = e - a * TN;
+      ent[ei++] = make_uint2(static_cast<unsigned>(p) | (static_cast<unsigned>(a) << 12) | (c << 14),
+                             static_cast<unsigned>(ti));
+      if (c != GM_WALK && c > 0) {
+        Aff A;
+        ghost_form(F, lev, halo_pt(o, N, nb27, p), a, A);
+        for (unsigned q = 0; q < c; ++q)
+          term[ti + q] = make_int2(A.idx[q], __float_as_int(static_cast<float>(A.w[q])));
+        ti += static_cast<int>(c);
+      }
     }
     __syncthreads();
   }
@@ -1012,13 +1098,13 @@ void amr_flow_setup() {
 }
 
 void launch_ghost_count(cudaStream_t s, const AmrFlowView& F, int* count) {
-  k_ghost_map<<<grid_for(F.L.nbrick), RHS_NT, 0, s>>>(F, count, nullptr, nullptr, nullptr, nullptr);
+  k_ghost_map<<<grid_for(F.L.nbrick), RHS_NT, 0, s>>>(F, count);
   NB_CUDA(cudaGetLastError());
 }
 
 void launch_ghost_fill(cudaStream_t s, const AmrFlowView& F, const int* eoff, const int* toff, uint2* ent,
                        int2* term) {
-  k_ghost_map<<<grid_for(F.L.nbrick), RHS_NT, 0, s>>>(F, nullptr, eoff, toff, ent, term);
+  k_ghost_fill<<<grid_for(F.L.nbrick), RHS_NT, 0, s>>>(F, eoff, toff, ent, term);
   NB_CUDA(cudaGetLastError());
 }
 
