@@ -237,6 +237,11 @@ typedef struct nb_tuning {
                                 in BF16 (rounded to nearest; BF16 keeps FP32's exponent
                                 range, so no per-brick scale is needed), 0 (default)
                                 FP32; arithmetic stays FP32 and the PCG FP64 */
+  int32_t ghost_map;         /* octree cases: 1 (default) the momentum kernel replays a
+                                per-case map of the ghost rules' recorded forms for the
+                                halo points that are not same-level cells (built when the
+                                case is created, about 60 B per leaf cell); 0 walks the
+                                ghost rules for those points at every stage (no map) */
 } nb_tuning;
 
 typedef struct nb_tune_report {

@@ -1564,7 +1564,7 @@ nb_status nb_amr_case_create(nb_ctx* ctx, nb_amr_mesh* mesh, const nb_flow_confi
     F.weno = cfg->convection == NB_CONV_WENO5;
     F.nu = c->nu;
     for (int a = 0; a < 3; ++a) F.bf[a] = cfg->body_force[a];
-    build_ghost_map(*c, F);
+    if (ctx->tune.ghost_map) build_ghost_map(*c, F);
     for (int h = 0; h < 2; ++h)
       for (int q = 0; q < 3; ++q) {
         const size_t nb = static_cast<size_t>(c->fm.store[q]) * sizeof(double);

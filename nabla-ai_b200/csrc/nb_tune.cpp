@@ -41,6 +41,7 @@ bool tuning_ok(const nb_tuning& t, std::string& why) {
   else if (t.warm_start < 0 || t.warm_start > 3) why = "warm_start must be in 0..3";
   else if (t.vgrid != 0 && t.vgrid != 1) why = "vgrid must be 0 or 1";
   else if (t.coarse_bf16 != 0 && t.coarse_bf16 != 1) why = "coarse_bf16 must be 0 or 1";
+  else if (t.ghost_map != 0 && t.ghost_map != 1) why = "ghost_map must be 0 or 1";
   else return true;
   return false;
 }
@@ -63,12 +64,12 @@ std::string tune_key(nb_ctx* ctx, const nb_case* c) {
   return s;
 }
 
-// One cache line: key and the twelve fields, then ms per step.
+// One cache line: key and the thirteen fields, then ms per step.
 bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double& ms) {
   std::istringstream in(line);
   if (!(in >> key >> t.mg_ctas_per_sm >> t.rhs_ctas_per_sm >> t.halo_mode >> t.sweeps >> t.coarse_direct_max >>
         t.pdl >> t.threads_per_brick >> t.smoother >> t.tail_bricks >>
-        t.warm_start >> t.vgrid >> t.coarse_bf16 >> ms))
+        t.warm_start >> t.vgrid >> t.coarse_bf16 >> t.ghost_map >> ms))
     return false;
   std::string why;
   return tuning_ok(t, why);
@@ -76,9 +77,9 @@ bool parse_line(const std::string& line, std::string& key, nb_tuning& t, double&
 
 std::string format_line(const std::string& key, const nb_tuning& t, double ms) {
   char buf[320];
-  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
+  std::snprintf(buf, sizeof buf, "%s %d %d %d %d %d %d %d %d %d %d %d %d %d %.6g", key.c_str(), t.mg_ctas_per_sm,
                 t.rhs_ctas_per_sm, t.halo_mode, t.sweeps, t.coarse_direct_max, t.pdl, t.threads_per_brick, t.smoother,
-                t.tail_bricks, t.warm_start, t.vgrid, t.coarse_bf16, ms);
+                t.tail_bricks, t.warm_start, t.vgrid, t.coarse_bf16, t.ghost_map, ms);
   return buf;
 }
 
@@ -106,6 +107,7 @@ void nb_tuning_default(nb_tuning* t) {
   t->warm_start = 3;
   t->vgrid = 0;
   t->coarse_bf16 = 0;
+  t->ghost_map = 1;
 }
 
 nb_status nb_ctx_set_tuning(nb_ctx* ctx, const nb_tuning* t) {

@@ -139,6 +139,7 @@ class Tuning(C.Structure):
         ("warm_start", C.c_int32),
         ("vgrid", C.c_int32),
         ("coarse_bf16", C.c_int32),
+        ("ghost_map", C.c_int32),
     ]
 
     def as_dict(self):
