@@ -1268,8 +1268,6 @@ __device__ __forceinline__ void tail_copy(T* global, char* arena, uintptr_t off,
 
 template <typename T>
 __global__ void __launch_bounds__(NT) k_vtail(const TailProg* __restrict__ prog, const SolveFlags* flags, int maxit) {
-  pdl_wait();
-  if (stopped(flags, maxit)) return;  // the same answer in every CTA: nothing writes the flags meanwhile
   cg::cluster_group cl = cg::this_cluster();
   const int rank = static_cast<int>(cl.block_rank()), cs = static_cast<int>(cl.num_blocks());
   __shared__ LevelView slv[MAX_TAIL_LEV];
@@ -1291,6 +1289,10 @@ __global__ void __launch_bounds__(NT) k_vtail(const TailProg* __restrict__ prog,
     dst = reinterpret_cast<int*>(sph);
     for (int i = threadIdx.x; i < nph * static_cast<int>(sizeof(TailPhase) / 4); i += blockDim.x) dst[i] = src[i];
   }
+  // The program above is written once, when the solve is recorded: it is read
+  // before the wait, while the predecessor grid drains.
+  pdl_wait();
+  if (stopped(flags, maxit)) return;  // the same answer in every CTA: nothing writes the flags meanwhile
   tail_copy<T, true>(static_cast<T*>(prog->b_in), dsm, prog->b_enc, prog->nbrick, rank, lcs);
   cl.sync();
   for (int p = 0; p < nph; ++p) {
