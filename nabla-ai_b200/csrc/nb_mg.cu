@@ -1825,7 +1825,7 @@ __global__ void __launch_bounds__(NT) k_pcg_update(LevelView L, double* __restri
                                                    double* __restrict__ rnew, float* __restrict__ rnew_f,
                                                    int singular, double inv_nfluid, RedBuf rb,
                                                    double* S, SolveFlags* flags, int maxit,
-                                                   double tol) {
+                                                   double tol, void* __restrict__ x0, double c2f) {
   pdl_wait();
   if (stopped(flags, maxit)) return;
   const double alpha = S[S_ALPHA];
@@ -1840,6 +1840,12 @@ __global__ void __launch_bounds__(NT) k_pcg_update(LevelView L, double* __restri
     } else {
       part[0] += cell_weight(L, brick) * (rn * rn);
       if (rnew_f) rnew_f[c] = static_cast<float>(rn);
+      // level 0's first pre-smoothing sweep from x = 0, pointwise in the
+      // residual it smooths (rnew_f in the mixed form, rnew in FP64)
+      if (x0) {
+        if (rnew_f) static_cast<float*>(x0)[c] = first_sweep<float>(L, c, static_cast<float>(rn), static_cast<float>(c2f));
+        else static_cast<double*>(x0)[c] = first_sweep<double>(L, c, rn, c2f);
+      }
     }
   }
   grid_reduce<1>(part, rb, [=] __device__(const double* t) {
@@ -2964,9 +2970,13 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
     // p_ holds the last direction, p2_ receives this cycle's (swapped below)
     NB_LAUNCH(lc_, "pcg_matvec", s, n * 33,
               launch_pdl(pdl_, km, dim3(grid), dim3(tpb_), 0, s, L, z_, p_, p2_, Ap_, rb_, S_, flags_, maxit));
-    NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0)),
-              (launch_pdl(pdl_, k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p2_, r_, Ap_, rnew_, mixed ? rnew_f_ : nullptr,
-                                                sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol)));
+    // non-singular systems whose level 0 smooths by launches: the update also
+    // writes level 0's first sweep (the V-cycle then starts at its second)
+    const bool first0 = !sing && !grid_prog_ && lv_.size() > 1 && tail_lvl_ != 0;
+    NB_LAUNCH(lc_, "pcg_update", s, n * (48 + (sing ? 1 : 0) + (mixed && !sing ? 4 : 0) + (first0 ? zsz + 2 : 0)),
+              (launch_pdl(pdl_, k_pcg_update, dim3(grid), dim3(NT), 0, s, L, x_, p2_, r_, Ap_, rnew_,
+                          mixed ? rnew_f_ : nullptr, sing ? 1 : 0, inv_nf, rb_, S_, flags_, maxit, tol,
+                          first0 ? lv_[0].x0 : nullptr, cheb_c2_[0])));
     if (sing) {
       NB_LAUNCH(lc_, "pcg_center", s, n * (17 + (mixed ? 4 : 0)),
                 (launch_pdl(pdl_, k_pcg_center, dim3(grid), dim3(NT), 0, s, L, rnew_, mixed ? rnew_f_ : nullptr, rb_, S_, flags_, maxit,
@@ -2982,8 +2992,8 @@ void MgSolver::iterate(cudaStream_t s, double tol, int maxit, int count) {
     } else {
       // non-singular: the V-cycle's last sweep also forms z' and the dots
       fuse_dots_ = !sing;
-      if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx);
-      else vcycle<double>(s, 0, rnew_, -1, nullptr, &zslot, &zx);
+      if (mixed) vcycle<float>(s, 0, rnew_f_, -1, nullptr, &zslot, &zx, nullptr, first0);
+      else vcycle<double>(s, 0, rnew_, -1, nullptr, &zslot, &zx, nullptr, first0);
       fuse_dots_ = false;
     }
     std::swap(p_, p2_);
