@@ -77,7 +77,6 @@ __device__ __forceinline__ int leaf_of(const LevelView& L, int lev0, const int p
 // given mesh. The ghost map records these forms once per case.
 struct ValRead {
   using V = double;
-  static constexpr bool kSym = false;
   __device__ static double rd(const double* __restrict__ f, long long i) { return f[i]; }
   __device__ static double k(double v) { return v; }
 };
@@ -132,7 +131,6 @@ __device__ __forceinline__ Aff operator*(double s, Aff a) {
 
 struct AffRead {
   using V = Aff;
-  static constexpr bool kSym = true;
   __device__ static Aff rd(const double* __restrict__, long long i) {
     Aff r;
     r.c = 0.0;
