@@ -245,9 +245,10 @@ __device__ __forceinline__ void fill_halo_amr(const LevelView& L, int brick, T* 
 // during a solve, so a kernel reads its first brick's before pdl_wait() (a CTA
 // that becomes resident while its predecessor grid drains has them before the
 // wait returns, and its halo loads then depend on no further map load) and
-// each later brick's at the end of the previous one. Two records alternate by
-// iteration parity: a brick's record is read after its first barrier (the
-// restriction's coarse target) while the next brick's is being written.
+// each later brick's during the previous brick's arithmetic, right after that
+// brick's staging barrier. Two records alternate by iteration parity: a
+// brick's record is still read after its first barrier (the restriction's
+// coarse target) while the next brick's is being written.
 struct BrickPre {
   int pb, po, xcb, xoct;
   double wc;
